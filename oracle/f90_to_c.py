@@ -1,0 +1,336 @@
+"""Recipe: build the reference's own mechanism arithmetic, run here, into ``oracle/_ref/``.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the product imports, links or runs this file or its
+outputs; only tests, the smoke check and the CPU-baseline leg of the benchmark may.
+
+The reference's chemistry rates live in three self-contained generated Fortran files
+(combustion/HYDROGENF.f90, combustion/grimech30F.f90, combustion/DME39F.f90, each with its
+``*F90.h`` parameter header). No Fortran compiler exists in this image, so this recipe
+transliterates the routines on the path -- ``PRODRATES``, ``GETLINDRATECOEFF``,
+``COMPTHERMODATA`` and ``GETMOLARMASS`` -- statement by statement into C, keeping:
+
+* the statement order and each expression's operator order (C and Fortran both associate
+  ``+ - * /`` left to right; the C file is compiled with ``-ffp-contract=off`` so no FMA is
+  introduced, matching the reference's ``-xAVX`` target, which has no FMA);
+* the Fortran literal kinds of the reference build (Makefile.in:23-24, no default-real
+  promotion): ``D`` exponents and ``_DP`` suffixes stay double, default-real literals become
+  C ``float`` literals that are widened on use, integer literals are exact;
+* the by-reference argument passing (``GETLINDRATECOEFF`` overwrites its ``K0`` argument).
+
+The transliteration is mechanical and shares no code with the product's table generator, so
+it pins that generator and the table-driven oracle independently. Outputs (C sources and the
+shared library) go to ``oracle/_ref/`` only; they are git-ignored and are rebuilt from the
+reference tree by ``python oracle/f90_to_c.py <reference combustion dir>``.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+
+MECHS = {
+    "hydrogen": ("HYDROGENF.f90", "HYDROGENF90.h"),
+    "grimech30": ("grimech30F.f90", "grimech30F90.h"),
+    "dme39": ("DME39F.f90", "DME39F90.h"),
+}
+ROUTINES = ("PRODRATES", "GETLINDRATECOEFF", "COMPTHERMODATA", "GETMOLARMASS")
+INTRINSICS = {"EXP": "exp", "DLOG": "log", "DLOG10": "log10", "MAX": "fmax", "DSQRT": "sqrt", "LOG": "log"}
+
+
+def statements(path):
+    stmts, cur = [], ""
+    for raw in open(path, errors="replace"):
+        line = raw.rstrip("\n")
+        cut = []
+        quote = None
+        for ch in line:
+            if quote:
+                cut.append(ch)
+                quote = None if ch == quote else quote
+            elif ch in "'\"":
+                quote = ch
+                cut.append(ch)
+            elif ch == "!":
+                break
+            else:
+                cut.append(ch)
+        s = "".join(cut).rstrip()
+        if s.endswith("&"):
+            cur += s[:-1] + " "
+            continue
+        cur += s
+        if cur.strip():
+            stmts.append(" ".join(cur.split()))
+        cur = ""
+    return stmts
+
+
+def header_params(path):
+    out = []
+    for st in statements(path):
+        if re.match(r"(?i)integer\s*,\s*parameter", st):
+            for item in st.split("::", 1)[1].split(","):
+                if "=" in item:
+                    n, v = (x.strip() for x in item.split("="))
+                    if re.fullmatch(r"\d+", v):
+                        out.append((n.upper(), int(v)))
+    return out
+
+
+TOK = re.compile(r"\s*((?:\d+\.\d*|\.\d+|\d+)(?:[eEdD][+-]?\d+)?(?:_DP)?|\.[A-Za-z]+\.|[A-Za-z_]\w*|\*\*|'[^']*'|\S)")
+
+
+def tokens(s):
+    pos, out = 0, []
+    while pos < len(s):
+        m = TOK.match(s, pos)
+        if not m:
+            break
+        out.append(m.group(1))
+        pos = m.end()
+    return out
+
+
+def c_literal(t):
+    """Fortran numeric literal -> C literal of the same kind and value."""
+    if t.upper().endswith("_DP"):
+        return t[:-3]
+    if re.search(r"[dD]", t):
+        return t.replace("D", "E").replace("d", "e")
+    if "." in t or "e" in t.lower():
+        return t + "f"  # default real: float32, widened to double where it meets a double
+    return t + ".0"  # integer literal: exact (no integer/integer division occurs in these files)
+
+
+class Routine:
+    def __init__(self, name, args, body, is_func):
+        self.name, self.args, self.body, self.is_func = name, args, body, is_func
+        self.arrays, self.locals, self.consts = set(), [], []
+
+
+def split_routines(stmts):
+    out = {}
+    cur = None
+    for st in stmts:
+        u = st.upper()
+        m = re.match(r"(DOUBLE PRECISION\s+FUNCTION|SUBROUTINE)\s+(\w+)\s*\(([^)]*)\)", u)
+        if m and cur is None:
+            args = [a.strip() for a in m.group(3).split(",") if a.strip()]
+            cur = Routine(m.group(2), args, [], m.group(1) != "SUBROUTINE")
+            continue
+        if cur is not None:
+            if u == "END":
+                out[cur.name] = cur
+                cur = None
+            else:
+                cur.body.append(st)
+    return out
+
+
+def translate_expr(toks, r, mech):
+    """Token list -> C expression string for routine r."""
+    out = []
+    i = 0
+    while i < len(toks):
+        t = toks[i]
+        u = t.upper()
+        nxt = toks[i + 1] if i + 1 < len(toks) else None
+        if re.match(r"^(\d|\.\d)", t):
+            out.append(c_literal(t))
+        elif u in (".GT.", ".LT.", ".GE.", ".LE.", ".EQ.", ".NE."):
+            out.append({".GT.": ">", ".LT.": "<", ".GE.": ">=", ".LE.": "<=", ".EQ.": "==", ".NE.": "!="}[u])
+        elif re.match(r"[A-Za-z_]", t):
+            if nxt == "(" and u in INTRINSICS:
+                out.append(INTRINSICS[u])
+            elif nxt == "(" and u == "GETLINDRATECOEFF":
+                # by-reference call: collect the argument groups
+                depth, j, args, cur = 0, i + 1, [], []
+                while True:
+                    tk = toks[j]
+                    if tk == "(":
+                        depth += 1
+                        if depth > 1:
+                            cur.append(tk)
+                    elif tk == ")":
+                        depth -= 1
+                        if depth == 0:
+                            args.append(cur)
+                            break
+                        cur.append(tk)
+                    elif tk == "," and depth == 1:
+                        args.append(cur)
+                        cur = []
+                    else:
+                        cur.append(tk)
+                    j += 1
+                cargs = []
+                for a in args:
+                    ca = translate_expr(a, r, mech)
+                    if len(a) == 1 and a[0].upper() in r.args:
+                        cargs.append("p_" + a[0].upper())
+                    else:
+                        cargs.append("&" + ca)
+                out.append(f"ref_{mech}_getlindratecoeff(" + ", ".join(cargs) + ")")
+                i = j + 1
+                continue
+            elif u in r.args and nxt == "(":
+                # array dummy: A(i) -> p_A[(i)-1]
+                depth, j, inner = 0, i + 1, []
+                while True:
+                    tk = toks[j]
+                    if tk == "(":
+                        depth += 1
+                        if depth > 1:
+                            inner.append(tk)
+                    elif tk == ")":
+                        depth -= 1
+                        if depth == 0:
+                            break
+                        inner.append(tk)
+                    else:
+                        inner.append(tk)
+                    j += 1
+                out.append(f"p_{u}[({translate_expr(inner, r, mech)})-1]")
+                i = j + 1
+                continue
+            elif u in r.args:
+                out.append(f"(*p_{u})")
+            elif u == r.name and r.is_func:
+                out.append("result")
+            else:
+                out.append(u)
+        elif t == "**":
+            # base ** (group): rewrite the previous operand and the following group as pow()
+            base = out.pop()
+            depth, j, inner = 0, i + 1, []
+            assert toks[j] == "(", "exponent must be parenthesised"
+            while True:
+                tk = toks[j]
+                if tk == "(":
+                    depth += 1
+                elif tk == ")":
+                    depth -= 1
+                inner.append(tk)
+                if depth == 0:
+                    break
+                j += 1
+            out.append(f"pow({base}, {translate_expr(inner, r, mech)})")
+            i = j + 1
+            continue
+        else:
+            out.append(t)
+        i += 1
+    return " ".join(out)
+
+
+def translate_routine(r, mech):
+    lines = []
+    decl = []
+    body = []
+    pnames = set()
+    for st in r.body:
+        m = re.match(r"^PARAMETER\s*\((\w+)\s*=", st.upper())
+        if m:
+            pnames.add(m.group(1))
+    for st in r.body:
+        u = st.upper()
+        if re.match(r"^(IMPLICIT|INCLUDE)\b", u):
+            continue
+        m = re.match(r"^(REAL\(DP\)|DOUBLE PRECISION|INTEGER|CHARACTER[^:]*)\s*(,\s*PARAMETER)?\s*(::)?\s*(.*)$", u)
+        if m and not re.match(r"^(REAL|DOUBLE|INTEGER)\w*\s*=", u):
+            ctype = "int" if m.group(1).startswith("INTEGER") else "double"
+            items = re.split(r",(?![^(]*\))", m.group(4))
+            for it in items:
+                it = it.strip()
+                if not it:
+                    continue
+                if "=" in it:
+                    n, v = (x.strip() for x in it.split("=", 1))
+                    decl.append(f"  const {ctype} {n} = {translate_expr(tokens(v), r, mech)};")
+                    continue
+                n = re.match(r"(\w+)", it).group(1)
+                if n in r.args or n == r.name or n in pnames:
+                    continue
+                decl.append(f"  {ctype} {n};")
+            continue
+        m = re.match(r"^PARAMETER\s*\((\w+)\s*=\s*(.*)\)$", u)
+        if m:
+            decl.append(f"  const double {m.group(1)} = {translate_expr(tokens(m.group(2)), r, mech)};")
+            continue
+        m = re.match(r"^IF\s*\((.*)\)\s*THEN$", st, re.I)
+        if m:
+            body.append(f"  if ({translate_expr(tokens(m.group(1)), r, mech)}) {{")
+            continue
+        if u == "ELSE":
+            body.append("  } else {")
+            continue
+        if u in ("END IF", "ENDIF"):
+            body.append("  }")
+            continue
+        if "=" in st:
+            toks = tokens(st)
+            depth = 0
+            for k, t in enumerate(toks):
+                depth += t == "("
+                depth -= t == ")"
+                if t == "=" and depth == 0:
+                    break
+            lhs = translate_expr(toks[:k], r, mech)
+            rhs = translate_expr(toks[k + 1:], r, mech)
+            body.append(f"  {lhs} = {rhs};")
+            continue
+        raise ValueError(f"untranslated statement in {r.name}: {st}")
+    cname = f"ref_{mech}_{r.name.lower()}"
+    params = ", ".join(f"double *p_{a}" for a in r.args)
+    if r.is_func:
+        lines.append(f"double {cname}({params}) {{")
+        lines.append("  double result;")
+    else:
+        lines.append(f"void {cname}({params}) {{")
+    lines += decl + body
+    if r.is_func:
+        lines.append("  return result;")
+    lines.append("}")
+    return "\n".join(lines)
+
+
+def transliterate(src_dir, mech):
+    f90, h = MECHS[mech]
+    params = header_params(os.path.join(src_dir, h))
+    routines = split_routines(statements(os.path.join(src_dir, f90)))
+    out = [f"/* Generated by oracle/f90_to_c.py from combustion/{f90} (+ {h}). Not committed. */",
+           "#include <math.h>", f"enum {{"]
+    out += [f"  {n} = {v}," for n, v in params]
+    out.append("};")
+    out.append(f"double ref_{mech}_getlindratecoeff(double*, double*, double*, double*, double*, double*);")
+    for name in ROUTINES:
+        out.append(translate_routine(routines[name], mech))
+    nspec = dict(params)["SEND"] - 1
+    nslot = dict(params)["REND"] - 1
+    nm = dict(params)["MEND"] - 1
+    out.append(f"int ref_{mech}_sizes(int *ns, int *nr, int *nm) {{ *ns = {nspec}; *nr = {nslot}; *nm = {nm}; return 0; }}")
+    # the variable names (SN2, R1F, ...) collide between mechanisms, so each goes to its own file
+    return "\n".join(out) + "\n"
+
+
+def build(src_dir, out_dir=OUT, cc="gcc"):
+    os.makedirs(out_dir, exist_ok=True)
+    cfiles = []
+    for mech in MECHS:
+        path = os.path.join(out_dir, f"ref_{mech}.c")
+        with open(path, "w") as fh:
+            fh.write(transliterate(src_dir, mech))
+        cfiles.append(path)
+    so = os.path.join(out_dir, "libref_mech.so")
+    cmd = [cc, "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-o", so] + cfiles + ["-lm"]
+    subprocess.check_call(cmd)
+    return so
+
+
+if __name__ == "__main__":
+    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/combustion"
+    print(build(src))

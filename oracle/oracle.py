@@ -1,0 +1,282 @@
+"""Python side of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may import this
+module, and only as the checker or the timed CPU baseline. The product never imports it.
+
+* :class:`Oracle` loads a mechanism table (the JSON under ``tiger_nga_b200/mechanisms``),
+  turns every literal into the double the reference binary would use (default-real literals
+  rounded to float32, Makefile.in:23-24), and drives ``chem_oracle.c`` -- the table-driven
+  restatement of PRODRATES / GETLINDRATECOEFF / COMPTHERMODATA / finitechem_compute_rhs.
+* :class:`Reference` drives ``oracle/_ref/libref_mech.so``, the reference's own Fortran
+  mechanism routines transliterated statement by statement to C by ``oracle/f90_to_c.py``.
+  It exists only where that library was built (it needs the reference tree to build).
+
+The literal-kind rule and table flattening are written here independently of the product's
+loader on purpose.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import struct
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+MECH_DIR = os.path.join(REPO, "tiger_nga_b200", "mechanisms")
+LIB = os.path.join(HERE, "_build", "libchem_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_mech.so")
+
+
+def build_oracle(force: bool = False) -> str:
+    """Compile chem_oracle.c (and solver_oracle.c when present) with gcc + OpenMP."""
+    srcs = [os.path.join(HERE, f) for f in ("chem_oracle.c", "solver_oracle.c") if os.path.exists(os.path.join(HERE, f))]
+    newest = max(os.path.getmtime(s) for s in srcs)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
+        os.makedirs(os.path.dirname(LIB), exist_ok=True)
+        tmp = LIB + f".{os.getpid()}.tmp"
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+                               "-o", tmp] + srcs + ["-lm"])
+        os.replace(tmp, LIB)
+    return LIB
+
+
+def _lit(text, mode="f32"):
+    t = text.strip()
+    neg = t.startswith("-")
+    body = t[1:] if neg else t
+    if body.upper().endswith("_DP"):
+        v = float(body[:-3].replace("D", "E").replace("d", "e"))
+    elif "d" in body.lower():
+        v = float(body.replace("D", "E").replace("d", "e"))
+    elif "." in body or "e" in body.lower():
+        v = float(body)
+        if mode == "f32":
+            v = struct.unpack("<f", struct.pack("<f", v))[0]
+    else:
+        v = float(int(body))
+    return -v if neg else v
+
+
+class _Mech(ctypes.Structure):
+    _fields_ = [
+        ("ns", ctypes.c_int), ("nslot", ctypes.c_int), ("nm", ctypes.c_int), ("nfo", ctypes.c_int),
+        ("rgas", ctypes.c_double), ("troe", ctypes.c_double * 7),
+        ("tb_ptr", ctypes.c_void_p), ("tb_sp", ctypes.c_void_p), ("tb_coef", ctypes.c_void_p),
+        ("k_flags", ctypes.c_void_p), ("kA", ctypes.c_void_p), ("kn", ctypes.c_void_p), ("kE", ctypes.c_void_p),
+        ("k_fo", ctypes.c_void_p),
+        ("f0_flags", ctypes.c_void_p), ("fi_flags", ctypes.c_void_p),
+        ("f0A", ctypes.c_void_p), ("f0n", ctypes.c_void_p), ("f0E", ctypes.c_void_p),
+        ("fiA", ctypes.c_void_p), ("fin", ctypes.c_void_p), ("fiE", ctypes.c_void_p),
+        ("fc_ptr", ctypes.c_void_p), ("fc_form", ctypes.c_void_p), ("fc_a", ctypes.c_void_p),
+        ("fc_x", ctypes.c_void_p), ("fo_M", ctypes.c_void_p),
+        ("w_ptr", ctypes.c_void_p), ("w_sp", ctypes.c_void_p), ("w_M", ctypes.c_void_p),
+        ("cd_ptr", ctypes.c_void_p), ("cd_sign", ctypes.c_void_p), ("cd_slot", ctypes.c_void_p),
+        ("cd_coef", ctypes.c_void_p),
+        ("tmid", ctypes.c_double), ("th_hi", ctypes.c_void_p), ("th_lo", ctypes.c_void_p), ("wmol", ctypes.c_void_p),
+    ]
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Oracle:
+    """Table-driven FP64 restatement of the reference chemistry, one mechanism."""
+
+    def __init__(self, name: str, literal_mode: str = "f32"):
+        self.name = name
+        self.mode = literal_mode
+        with open(os.path.join(MECH_DIR, name + ".json")) as fh:
+            tab = json.load(fh)
+        self.tab = tab
+        L = lambda t: _lit(t, literal_mode)  # noqa: E731
+        ns, nslot, nm = tab["n_species"], tab["n_slots"], tab["n_thirdbody"]
+        self.ns, self.nslot, self.nm = ns, nslot, nm
+        keep = []
+
+        def I(x):  # noqa: E743
+            a = np.ascontiguousarray(np.asarray(x, dtype=np.int32))
+            keep.append(a)
+            return a
+
+        def D(x):
+            a = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+            keep.append(a)
+            return a
+
+        tb_ptr, tb_sp, tb_coef = [0], [], []
+        for terms in tab["third_body"]:
+            for s, c in terms:
+                tb_sp.append(s)
+                tb_coef.append(L(c))
+            tb_ptr.append(len(tb_sp))
+
+        def arr_flags(d):
+            return (2 if d["n"] is not None else 0) | (4 if d["E"] is not None else 0)
+
+        kfl, kA, kn, kE, kfo = [], [], [], [], []
+        f0fl, fifl, f0A, f0n, f0E, fiA, fin, fiE, fcp, fcf, fca, fcx, foM = ([] for _ in range(13))
+        fcp.append(0)
+        for k in tab["k"]:
+            if k["type"] == "falloff":
+                kfl.append(1)
+                kA.append(0.0), kn.append(0.0), kE.append(0.0)
+                kfo.append(len(foM))
+                for d, fl, A, n, E in ((k["k0"], f0fl, f0A, f0n, f0E), (k["kinf"], fifl, fiA, fin, fiE)):
+                    fl.append(arr_flags(d))
+                    A.append(L(d["A"]))
+                    n.append(L(d["n"]) if d["n"] is not None else 0.0)
+                    E.append(L(d["E"]) if d["E"] is not None else 0.0)
+                for t in k["fc"]:
+                    fcf.append(0 if t["form"] == "T_over" else 1)
+                    fca.append(L(t["a"]))
+                    fcx.append(L(t["x"]))
+                fcp.append(len(fca))
+                foM.append(k["M"])
+            else:
+                kfl.append(arr_flags(k))
+                kA.append(L(k["A"]))
+                kn.append(L(k["n"]) if k["n"] is not None else 0.0)
+                kE.append(L(k["E"]) if k["E"] is not None else 0.0)
+                kfo.append(-1)
+        w_ptr, w_sp, w_M = [0], [], []
+        for w in tab["w"]:
+            w_sp += w["C"]
+            w_ptr.append(len(w_sp))
+            w_M.append(w["M"])
+        cd_ptr, cd_sign, cd_slot, cd_coef = [0], [], [], []
+        for terms in tab["cdot"]:
+            for sgn, c, r in terms:
+                cd_sign.append(sgn)
+                cd_coef.append(L(c))
+                cd_slot.append(r)
+            cd_ptr.append(len(cd_slot))
+
+        def thermo(rng):
+            out = []
+            for e in tab["thermo"][rng]:
+                out += [L(e["c0"])] + [L(a) for a in e["a"]] + [L(e["a6"])] + [L(b) for b in e["b"]]
+            return out
+
+        self.wmol = D([L(x) for x in tab["molar_mass"]])
+        m = _Mech()
+        m.ns, m.nslot, m.nm, m.nfo = ns, nslot, nm, len(foM)
+        m.rgas = L(tab["rgas"])
+        m.troe[:] = [L("0.75"), L("1.27"), L("0.4"), L("0.67"), L("0.14"), L("1.0D-60"), L("1.0")]
+        for fname, val in (("tb_ptr", I(tb_ptr)), ("tb_sp", I(tb_sp)), ("tb_coef", D(tb_coef)),
+                           ("k_flags", I(kfl)), ("kA", D(kA)), ("kn", D(kn)), ("kE", D(kE)), ("k_fo", I(kfo)),
+                           ("f0_flags", I(f0fl + [0])), ("fi_flags", I(fifl + [0])),
+                           ("f0A", D(f0A + [0])), ("f0n", D(f0n + [0])), ("f0E", D(f0E + [0])),
+                           ("fiA", D(fiA + [0])), ("fin", D(fin + [0])), ("fiE", D(fiE + [0])),
+                           ("fc_ptr", I(fcp)), ("fc_form", I(fcf + [0])), ("fc_a", D(fca + [0])),
+                           ("fc_x", D(fcx + [0])), ("fo_M", I(foM + [0])),
+                           ("w_ptr", I(w_ptr)), ("w_sp", I(w_sp + [0])), ("w_M", I(w_M)),
+                           ("cd_ptr", I(cd_ptr)), ("cd_sign", I(cd_sign + [0])), ("cd_slot", I(cd_slot + [0])),
+                           ("cd_coef", D(cd_coef + [0])),
+                           ("th_hi", D(thermo("hi"))), ("th_lo", D(thermo("lo"))), ("wmol", self.wmol)):
+            setattr(m, fname, _p(val))
+        m.tmid = L(tab["thermo"]["tmid"])
+        self._keep = keep
+        self.m = m
+        self.lib = ctypes.CDLL(build_oracle())
+        self.lib.orc_prodrates.argtypes = [ctypes.POINTER(_Mech)] + [ctypes.c_void_p] * 5 + [ctypes.c_double] * 2
+        self.lib.orc_thermo.argtypes = [ctypes.POINTER(_Mech), ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+        self.lib.orc_rhs.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]
+        self.lib.orc_rhs_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                           ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
+        self.lib.orc_max_threads.restype = ctypes.c_int
+
+    # ---- single cell --------------------------------------------------------------------
+    def prodrates(self, C, T, P):
+        """(cdot, W, K, M) for concentrations C [kmol/m^3], T [K], P [Pa]."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        cd = np.zeros(self.ns)
+        W = np.zeros(self.nslot)
+        K = np.zeros(self.nslot)
+        M = np.zeros(max(self.nm, 1))
+        self.lib.orc_prodrates(ctypes.byref(self.m), _p(cd), _p(W), _p(K), _p(C), _p(M), float(T), float(P))
+        return cd, W, K, M
+
+    def thermo(self, T):
+        h = np.zeros(self.ns)
+        cp = np.zeros(self.ns)
+        self.lib.orc_thermo(ctypes.byref(self.m), float(T), _p(h), _p(cp))
+        return h, cp
+
+    def rhs(self, sol, p):
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        out = np.zeros(self.ns + 1)
+        self.lib.orc_rhs(ctypes.byref(self.m), _p(sol), float(p), _p(out))
+        return out
+
+    # ---- batch (species-major) ------------------------------------------------------------
+    def rhs_batch(self, sol, p, nthreads=0):
+        """sol: (N+1, ncells) float64 C-contiguous, species-major. Returns rhs of the same shape."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        out = np.empty_like(sol)
+        self.lib.orc_rhs_batch(ctypes.byref(self.m), _p(sol), float(p), _p(out), sol.shape[1], sol.shape[1],
+                               int(nthreads))
+        return out
+
+    def max_threads(self):
+        return self.lib.orc_max_threads()
+
+
+class Reference:
+    """The reference's own mechanism routines, transliterated to C (oracle/_ref)."""
+
+    def __init__(self, name: str):
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(REF_LIB)
+        self.lib = ctypes.CDLL(REF_LIB)
+        ns, nr, nm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        getattr(self.lib, f"ref_{name}_sizes")(ctypes.byref(ns), ctypes.byref(nr), ctypes.byref(nm))
+        self.ns, self.nslot, self.nm = ns.value, nr.value, nm.value
+        self._pr = getattr(self.lib, f"ref_{name}_prodrates")
+        self._th = getattr(self.lib, f"ref_{name}_compthermodata")
+        self._mm = getattr(self.lib, f"ref_{name}_getmolarmass")
+        for f in (self._pr, self._th, self._mm):
+            f.restype = None
+        mm = np.zeros(self.ns)
+        self._mm(_p(mm))
+        self.wmol = mm
+
+    def prodrates(self, C, T, P):
+        C = np.array(C, dtype=np.float64)
+        cd, W, K, M = np.zeros(self.ns), np.zeros(self.nslot), np.zeros(self.nslot), np.zeros(self.nm)
+        t, p = ctypes.c_double(T), ctypes.c_double(P)
+        self._pr(_p(cd), _p(W), _p(K), _p(C), _p(M), ctypes.byref(t), ctypes.byref(p))
+        return cd, W, K, M
+
+    def thermo(self, T):
+        h, cp = np.zeros(self.ns), np.zeros(self.ns)
+        t = ctypes.c_double(T)
+        self._th(_p(h), _p(cp), ctypes.byref(t))
+        return h, cp
+
+    def rhs(self, sol, p):
+        """finitechem_compute_rhs (finitechem.f90:93-175) over the transliterated routines."""
+        N = self.ns
+        sol = np.asarray(sol, dtype=np.float64)
+        rho = 0.0
+        for k in range(N):
+            rho = rho + sol[k]
+        Y = sol[:N] / rho
+        T = sol[N] / rho
+        h, cp = self.thermo(T)
+        cpmix = 0.0
+        for k in range(N):
+            cpmix = cpmix + Y[k] * cp[k]
+        conc = sol[:N] / self.wmol
+        cd, _, _, _ = self.prodrates(conc, T, p)
+        out = np.zeros(N + 1)
+        out[:N] = cd * self.wmol
+        tmp = 0.0
+        for k in range(N):
+            tmp = tmp - h[k] * out[k]
+        out[N] = tmp / cpmix
+        return out
