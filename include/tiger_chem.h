@@ -1,0 +1,105 @@
+/* tiger_chem.h -- C-ABI of the B200 finite-rate chemistry path (sm_100a).
+ *
+ * A drop-in for the finite-rate chemistry substep of the NGA/ARTS low-Mach solver. The
+ * reference exposes two Fortran ABIs on this path (external linkage, arguments by
+ * reference):
+ *   - the substep  finitechem_source_chemistry(RHO_, SC_)    combustion/finitechem.f90:962-1071
+ *   - the mechanism plugin  PRODRATES / COMPTHERMODATA / GETMOLARMASS / GETSPECIESNAMES /
+ *     GETNSPECIES / GETNREACTIONS                            combustion/mechanism.f90:17-108
+ * Every entry point here takes plain pointers and sizes, returns an int status (0 = OK,
+ * negative = error; tng_last_error() gives the message) and is callable from Fortran through
+ * ISO_C_BINDING (see fortran/tiger_chem_gpu.f90).
+ *
+ * Threading: one handle per host thread; a handle owns one CUDA stream on its device.
+ * No entry point falls back to the CPU: without a usable sm_100 device tng_chem_create fails.
+ */
+#ifndef TIGER_CHEM_H
+#define TIGER_CHEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TNG_OK 0
+#define TNG_ERR_ARG (-1)
+#define TNG_ERR_CUDA (-2)
+#define TNG_ERR_MECH (-3)
+#define TNG_ERR_STATE (-4)
+
+/* Precision of the rate evaluation. */
+#define TNG_FP64 0  /* everything FP64 (agrees with the reference within 1e-10 relative) */
+#define TNG_MIXED 1 /* FP32 rate products in log2 space, FP64 reverse exponents/sums/thermo */
+
+/* Literal kinds of the mechanism constants. */
+#define TNG_LIT_REF 0 /* as the reference build: default-real literals rounded to float32 */
+#define TNG_LIT_F64 1 /* every literal read as a double */
+
+/* Pointer location flags for batch calls. */
+#define TNG_DEVICE_PTRS 0 /* arrays live in device memory (the fast path) */
+#define TNG_HOST_PTRS 1   /* arrays live in host memory; copied through pinned staging */
+
+typedef struct tng_cfg {
+  int precision;    /* TNG_FP64 | TNG_MIXED */
+  int literal_mode; /* TNG_LIT_REF | TNG_LIT_F64 */
+  int device;       /* CUDA device ordinal */
+  double rtol;      /* relative tolerance ('Finitechem rel. tol.', finitechem.f90:266, default 1e-6) */
+  double atol;      /* absolute tolerance ('Finitechem abs. tol.', finitechem.f90:267, default 1e-12) */
+  int max_steps;    /* internal steps per cell and substep (MAX_NSTEPS, finitechem.f90:1025) */
+  int max_newton;   /* Newton iterations per internal step before the step is retried */
+  int block_size;   /* threads per block of the rate kernel, 0 = tuned default */
+  int reserved[8];
+} tng_cfg;
+
+typedef struct tng_chem tng_chem;
+
+/* Fill cfg with the reference defaults. */
+void tng_default_cfg(tng_cfg* cfg);
+
+/* Last error message of the calling thread (copied, NUL-terminated). Returns its length. */
+int tng_last_error(char* buf, int len);
+
+/* Create a handle for a built-in mechanism ("hydrogen", "grimech30", "dme39").
+ * Replaces the link-time choice of mechanism (combustion/Makefile:3-5) and finitechem_init's
+ * mechanism queries (finitechem.f90:184-213). */
+int tng_chem_create(const char* mechanism, const tng_cfg* cfg, tng_chem** out);
+int tng_chem_destroy(tng_chem* h);
+
+/* GETNSPECIES / GETNSPECS / GETNREACTIONS (HYDROGENF.f90:412-450) and the third-body count. */
+int tng_chem_sizes(const tng_chem* h, int* nspecies, int* nslots, int* nthirdbody);
+/* GETMOLARMASS (HYDROGENF.f90:366-386): W_k in kg/kmol, with the handle's literal kinds. */
+int tng_chem_molar_mass(const tng_chem* h, double* wmol);
+/* GETSPECIESNAMES (HYDROGENF.f90:389-409): name of species k (0-based), NUL-terminated. */
+int tng_chem_species_name(const tng_chem* h, int k, char* buf, int len);
+/* The handle's CUDA stream (cudaStream_t) for callers that enqueue around it. */
+void* tng_chem_stream(tng_chem* h);
+
+/* Batched finitechem_compute_rhs (finitechem.f90:93-175, low-Mach branch) with PRODRATES,
+ * GETLINDRATECOEFF and COMPTHERMODATA inside: for each of ncells cells,
+ *   sol = (rho*Y_1..rho*Y_N, rho*T)  ->  rhs = (d(rho*Y_k)/dt, d(rho*T)/dt)
+ * Arrays are species-major: variable v of cell i at [v*ld + i], v = 0..N, ld >= ncells.
+ * p is the thermodynamic pressure in Pa (the reference uses 0.5*(P_thermo+P_thermo_old)).
+ * flags: TNG_DEVICE_PTRS or TNG_HOST_PTRS. Device calls are asynchronous on the handle's
+ * stream; host calls return after the results are in rhs. */
+int tng_prodrates_batch(tng_chem* h, const double* sol, double* rhs, int64_t ncells, int64_t ld, double p,
+                        int flags);
+
+/* Debug variant of tng_prodrates_batch that also stores every slot's rate W_r
+ * (the W(r) work array of PRODRATES) at rates[r*ld + i]; device pointers only. */
+int tng_prodrates_batch_rates(tng_chem* h, const double* sol, double* rhs, double* rates, int64_t ncells, int64_t ld,
+                              double p);
+
+/* Wait for the handle's stream; returns the first asynchronous error, if any. */
+int tng_chem_sync(tng_chem* h);
+
+/* Measurement helper (no reference counterpart): sustained FP64 FMA throughput of a device in
+ * TFLOP/s (FMA = 2 flops), the denominator of the FP64-pipe roofline of the rate kernels. */
+int tng_bench_fp64_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TIGER_CHEM_H */

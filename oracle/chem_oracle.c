@@ -182,3 +182,61 @@ int orc_max_threads(void) {
   return 1;
 #endif
 }
+
+/* Gross (cancellation-free) magnitude of every rhs entry, the denominator of the normwise
+ * parity test: gross_k = W_k * sum over the CDOT terms of |coef * W_r|, and
+ * gross_T = sum_k |h_k| gross_k / cp_mix. */
+void orc_rhs_gross(const orc_mech *m, const double *sol, double p, double *gross) {
+  int N = m->ns;
+  double h[ORC_MAXS], cp[ORC_MAXS], conc[ORC_MAXS], cd[ORC_MAXS], M[ORC_MAXS];
+  double K[ORC_MAXR], W[ORC_MAXR];
+  double rho = 0.0;
+  for (int k = 0; k < N; ++k) rho = rho + sol[k];
+  double T = sol[N] / rho;
+  orc_thermo(m, T, h, cp);
+  double cpmix = 0.0;
+  for (int k = 0; k < N; ++k) cpmix = cpmix + (sol[k] / rho) * cp[k];
+  for (int k = 0; k < N; ++k) conc[k] = sol[k] / m->wmol[k];
+  orc_prodrates(m, cd, W, K, conc, M, T, p);
+  double gt = 0.0;
+  for (int k = 0; k < N; ++k) {
+    double g = 0.0;
+    for (int i = m->cd_ptr[k]; i < m->cd_ptr[k + 1]; ++i) g += fabs(m->cd_coef[i] * W[m->cd_slot[i]]);
+    gross[k] = g * m->wmol[k];
+    gt += fabs(h[k]) * gross[k];
+  }
+  gross[N] = gt / cpmix;
+}
+
+void orc_rhs_gross_batch(const orc_mech *m, const double *sol, double p, double *gross, int64_t ncells, int64_t ld,
+                         int nthreads) {
+  int N = m->ns;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t i = 0; i < ncells; ++i) {
+    double s[ORC_MAXS], r[ORC_MAXS];
+    for (int v = 0; v <= N; ++v) s[v] = sol[v * ld + i];
+    orc_rhs_gross(m, s, p, r);
+    for (int v = 0; v <= N; ++v) gross[v * ld + i] = r[v];
+  }
+}
+
+/* Rates W_r of every slot for a species-major batch (slot-major output rates[r*ld + i]). */
+void orc_rates_batch(const orc_mech *m, const double *sol, double p, double *rates, int64_t ncells, int64_t ld,
+                     int64_t ldr, int nthreads) {
+  int N = m->ns;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t i = 0; i < ncells; ++i) {
+    double conc[ORC_MAXS], cd[ORC_MAXS], M[ORC_MAXS], K[ORC_MAXR], W[ORC_MAXR];
+    double rho = 0.0;
+    for (int k = 0; k < N; ++k) rho = rho + sol[k * ld + i];
+    for (int k = 0; k < N; ++k) conc[k] = sol[k * ld + i] / m->wmol[k];
+    orc_prodrates(m, cd, W, K, conc, M, sol[N * ld + i] / rho, p);
+    for (int r = 0; r < m->nslot; ++r) rates[r * ldr + i] = W[r];
+  }
+}

@@ -313,6 +313,41 @@ def transliterate(src_dir, mech):
     nslot = dict(params)["REND"] - 1
     nm = dict(params)["MEND"] - 1
     out.append(f"int ref_{mech}_sizes(int *ns, int *nr, int *nm) {{ *ns = {nspec}; *nr = {nslot}; *nm = {nm}; return 0; }}")
+    # finitechem_compute_rhs (finitechem.f90:93-175, low-Mach branch) over a species-major batch,
+    # OpenMP over cells like one MPI rank per core; the mechanism routines are the transliterated ones.
+    out.append(f"""
+#include <stdint.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+void ref_{mech}_rhs_batch(const double *sol, double p, double *rhs, int64_t ncells, int64_t ld, int nthreads) {{
+  double W_sp[{nspec}];
+  ref_{mech}_getmolarmass(W_sp);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t i = 0; i < ncells; ++i) {{
+    double s[{nspec + 1}], h[{nspec}], cp[{nspec}], conc[{nspec}], cd[{nspec}], K[{nslot}], W[{nslot}], M[{max(nm, 1)}];
+    for (int v = 0; v <= {nspec}; ++v) s[v] = sol[v * ld + i];
+    double rho = 0.0;
+    for (int k = 0; k < {nspec}; ++k) rho = rho + s[k];
+    double T = s[{nspec}] / rho, P = p;
+    ref_{mech}_compthermodata(h, cp, &T);
+    double cpmix = 0.0;
+    for (int k = 0; k < {nspec}; ++k) cpmix = cpmix + (s[k] / rho) * cp[k];
+    for (int k = 0; k < {nspec}; ++k) conc[k] = s[k] / W_sp[k];
+    ref_{mech}_prodrates(cd, W, K, conc, M, &T, &P);
+    double tmp = 0.0;
+    for (int k = 0; k < {nspec}; ++k) {{
+      double r = cd[k] * W_sp[k];
+      rhs[k * ld + i] = r;
+      tmp = tmp - h[k] * r;
+    }}
+    rhs[{nspec} * ld + i] = tmp / cpmix;
+  }}
+}}
+""")
     # the variable names (SN2, R1F, ...) collide between mechanisms, so each goes to its own file
     return "\n".join(out) + "\n"
 
@@ -326,7 +361,7 @@ def build(src_dir, out_dir=OUT, cc="gcc"):
             fh.write(transliterate(src_dir, mech))
         cfiles.append(path)
     so = os.path.join(out_dir, "libref_mech.so")
-    cmd = [cc, "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-o", so] + cfiles + ["-lm"]
+    cmd = [cc, "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-o", so] + cfiles + ["-lm"]
     subprocess.check_call(cmd)
     return so
 

@@ -189,6 +189,10 @@ class Oracle:
         self.lib.orc_rhs_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         self.lib.orc_max_threads.restype = ctypes.c_int
+        self.lib.orc_rhs_gross_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double,
+                                                 ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
+        self.lib.orc_rates_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                             ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
 
     # ---- single cell --------------------------------------------------------------------
     def prodrates(self, C, T, P):
@@ -222,6 +226,22 @@ class Oracle:
                                int(nthreads))
         return out
 
+    def rhs_gross_batch(self, sol, p, nthreads=0):
+        """Cancellation-free magnitude of each rhs entry (denominator of the normwise test)."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        out = np.empty_like(sol)
+        self.lib.orc_rhs_gross_batch(ctypes.byref(self.m), _p(sol), float(p), _p(out), sol.shape[1], sol.shape[1],
+                                     int(nthreads))
+        return out
+
+    def rates_batch(self, sol, p, nthreads=0):
+        """Every slot's rate W_r, shape (nslot, ncells)."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        out = np.empty((self.nslot, sol.shape[1]))
+        self.lib.orc_rates_batch(ctypes.byref(self.m), _p(sol), float(p), _p(out), sol.shape[1], sol.shape[1],
+                                 sol.shape[1], int(nthreads))
+        return out
+
     def max_threads(self):
         return self.lib.orc_max_threads()
 
@@ -239,11 +259,21 @@ class Reference:
         self._pr = getattr(self.lib, f"ref_{name}_prodrates")
         self._th = getattr(self.lib, f"ref_{name}_compthermodata")
         self._mm = getattr(self.lib, f"ref_{name}_getmolarmass")
-        for f in (self._pr, self._th, self._mm):
+        self._rb = getattr(self.lib, f"ref_{name}_rhs_batch")
+        for f in (self._pr, self._th, self._mm, self._rb):
             f.restype = None
         mm = np.zeros(self.ns)
         self._mm(_p(mm))
         self.wmol = mm
+
+    def rhs_batch(self, sol, p, nthreads=0):
+        """finitechem_compute_rhs over a species-major batch, OpenMP over cells."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        out = np.empty_like(sol)
+        f = self._rb
+        f(_p(sol), ctypes.c_double(p), _p(out), ctypes.c_int64(sol.shape[1]), ctypes.c_int64(sol.shape[1]),
+          ctypes.c_int(int(nthreads)))
+        return out
 
     def prodrates(self, C, T, P):
         C = np.array(C, dtype=np.float64)

@@ -1,0 +1,217 @@
+"""Python binding of the C-ABI (``include/tiger_chem.h``) over ctypes.
+
+Mirrors the reference's finite-rate chemistry interface for this path:
+
+* :meth:`FiniteChem.compute_rhs` -- batched ``finitechem_compute_rhs``
+  (combustion/finitechem.f90:93-175) with ``PRODRATES`` inside;
+* :meth:`FiniteChem.molar_mass`, :attr:`FiniteChem.species`, :attr:`FiniteChem.nspecies`,
+  :attr:`FiniteChem.nreactions` -- ``GETMOLARMASS`` / ``GETSPECIESNAMES`` / ``GETNSPECIES`` /
+  ``GETNREACTIONS`` (combustion/HYDROGENF.f90:366-450).
+
+The library is the in-tree ``libtiger_chem.so`` built by :mod:`tiger_nga_b200.build`. There is
+no CPU fallback: if the library or a CUDA device is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libtiger_chem.so")
+
+TNG_FP64, TNG_MIXED = 0, 1
+TNG_LIT_REF, TNG_LIT_F64 = 0, 1
+TNG_DEVICE_PTRS, TNG_HOST_PTRS = 0, 1
+
+
+class TngCfg(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("literal_mode", ctypes.c_int), ("device", ctypes.c_int),
+                ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_steps", ctypes.c_int),
+                ("max_newton", ctypes.c_int), ("block_size", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
+
+
+class ChemError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> ctypes.CDLL:
+    """Load ``libtiger_chem.so`` (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ChemError(f"{p} is missing: build it with `python -m tiger_nga_b200.build` (needs nvcc)")
+    lib = ctypes.CDLL(p)
+    V, I, D, L = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int64
+    sig = {
+        "tng_default_cfg": (None, [ctypes.POINTER(TngCfg)]),
+        "tng_last_error": (I, [ctypes.c_char_p, I]),
+        "tng_chem_create": (I, [ctypes.c_char_p, ctypes.POINTER(TngCfg), ctypes.POINTER(V)]),
+        "tng_chem_destroy": (I, [V]),
+        "tng_chem_sizes": (I, [V, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I)]),
+        "tng_chem_molar_mass": (I, [V, V]),
+        "tng_chem_species_name": (I, [V, I, ctypes.c_char_p, I]),
+        "tng_chem_stream": (V, [V]),
+        "tng_chem_sync": (I, [V]),
+        "tng_prodrates_batch": (I, [V, V, V, L, L, D, I]),
+        "tng_prodrates_batch_rates": (I, [V, V, V, V, L, L, D]),
+        "tng_bench_fp64_peak": (I, [I, ctypes.POINTER(D)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error(lib=None) -> str:
+    lib = lib or load_library()
+    buf = ctypes.create_string_buffer(2048)
+    lib.tng_last_error(buf, 2048)
+    return buf.value.decode()
+
+
+def _check(rc: int, what: str) -> None:
+    if rc != 0:
+        raise ChemError(f"{what} failed ({rc}): {last_error()}")
+
+
+def default_cfg() -> TngCfg:
+    cfg = TngCfg()
+    load_library().tng_default_cfg(ctypes.byref(cfg))
+    return cfg
+
+
+def fp64_peak_tflops(device: int = 0) -> float:
+    """Measured FP64 FMA throughput of a device (TFLOP/s)."""
+    v = ctypes.c_double()
+    _check(load_library().tng_bench_fp64_peak(device, ctypes.byref(v)), "tng_bench_fp64_peak")
+    return v.value
+
+
+class FiniteChem:
+    """One mechanism on one GPU (a ``tng_chem`` handle and its stream)."""
+
+    def __init__(self, mechanism: str, precision: str = "fp64", literal_mode: str = "ref", device: int = 0,
+                 **cfg_fields):
+        self.lib = load_library()
+        cfg = default_cfg()
+        cfg.precision = {"fp64": TNG_FP64, "mixed": TNG_MIXED}[precision]
+        cfg.literal_mode = {"ref": TNG_LIT_REF, "f64": TNG_LIT_F64}[literal_mode]
+        cfg.device = device
+        for k, v in cfg_fields.items():
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        _check(self.lib.tng_chem_create(mechanism.encode(), ctypes.byref(cfg), ctypes.byref(h)), "tng_chem_create")
+        self.h = h
+        self.mechanism = mechanism
+        self.device = device
+        ns, nr, nm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.tng_chem_sizes(h, ctypes.byref(ns), ctypes.byref(nr), ctypes.byref(nm)), "tng_chem_sizes")
+        self.nspecies, self.nreactions, self.nthirdbody = ns.value, nr.value, nm.value
+        self._torch_stream = None
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.tng_chem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- mechanism getters -----------------------------------------------------------------
+    def molar_mass(self) -> np.ndarray:
+        w = np.zeros(self.nspecies)
+        _check(self.lib.tng_chem_molar_mass(self.h, w.ctypes.data), "tng_chem_molar_mass")
+        return w
+
+    @property
+    def species(self) -> list[str]:
+        out = []
+        buf = ctypes.create_string_buffer(64)
+        for k in range(self.nspecies):
+            _check(self.lib.tng_chem_species_name(self.h, k, buf, 64), "tng_chem_species_name")
+            out.append(buf.value.decode())
+        return out
+
+    # ---- streams ---------------------------------------------------------------------------
+    def torch_stream(self):
+        import torch
+
+        if self._torch_stream is None:
+            self._torch_stream = torch.cuda.ExternalStream(self.lib.tng_chem_stream(self.h), device=self.device)
+        return self._torch_stream
+
+    def sync(self) -> None:
+        _check(self.lib.tng_chem_sync(self.h), "tng_chem_sync")
+
+    # ---- R7: batched right-hand side ------------------------------------------------------
+    def compute_rhs(self, sol, p: float, out=None):
+        """d(sol)/dt for a species-major batch ``sol`` of shape (N+1, ncells).
+
+        ``sol`` may be a CUDA tensor (device path, asynchronous, ordered with torch's current
+        stream) or a NumPy array (host path; copies pipelined through the device).
+        """
+        nv = self.nspecies + 1
+        if isinstance(sol, np.ndarray):
+            if sol.dtype != np.float64 or sol.ndim != 2 or sol.shape[0] != nv or not sol.flags.c_contiguous:
+                raise ValueError(f"sol must be a C-contiguous float64 array of shape ({nv}, ncells)")
+            if out is None:
+                out = np.empty_like(sol)
+            n = sol.shape[1]
+            _check(self.lib.tng_prodrates_batch(self.h, sol.ctypes.data, out.ctypes.data, n, n, float(p),
+                                                TNG_HOST_PTRS), "tng_prodrates_batch")
+            return out
+        import torch
+
+        if not (sol.is_cuda and sol.dtype == torch.float64 and sol.dim() == 2 and sol.shape[0] == nv):
+            raise ValueError(f"sol must be a CUDA float64 tensor of shape ({nv}, ncells)")
+        if sol.stride(1) != 1:
+            raise ValueError("sol must be species-major with unit stride along cells")
+        ld = sol.stride(0)
+        if out is None:
+            out = torch.empty_like(sol)
+        if out.stride() != sol.stride():
+            raise ValueError("out must have the same strides as sol")
+        st = self.torch_stream()
+        st.wait_stream(torch.cuda.current_stream(sol.device))
+        _check(self.lib.tng_prodrates_batch(self.h, sol.data_ptr(), out.data_ptr(), sol.shape[1], ld, float(p),
+                                            TNG_DEVICE_PTRS), "tng_prodrates_batch")
+        torch.cuda.current_stream(sol.device).wait_stream(st)
+        return out
+
+    def launch_rhs(self, sol_ptr: int, out_ptr: int, ncells: int, ld: int, p: float) -> None:
+        """Raw asynchronous launch on the handle's stream (device pointers, no stream joins)."""
+        _check(self.lib.tng_prodrates_batch(self.h, sol_ptr, out_ptr, ncells, ld, float(p), TNG_DEVICE_PTRS),
+               "tng_prodrates_batch")
+
+    def compute_rhs_rates(self, sol, p: float):
+        """compute_rhs plus every slot's rate W_r (device tensors; reference literal kinds only)."""
+        import torch
+
+        nv = self.nspecies + 1
+        n = sol.shape[1]
+        if sol.stride(1) != 1 or sol.shape[0] != nv:
+            raise ValueError("sol must be species-major (N+1, ncells)")
+        out = torch.empty_like(sol)
+        rates = torch.empty((self.nreactions, n), dtype=torch.float64, device=sol.device)
+        if sol.stride(0) != n:
+            raise ValueError("compute_rhs_rates needs a dense batch (ld == ncells)")
+        st = self.torch_stream()
+        st.wait_stream(torch.cuda.current_stream(sol.device))
+        _check(self.lib.tng_prodrates_batch_rates(self.h, sol.data_ptr(), out.data_ptr(), rates.data_ptr(), n, n,
+                                                  float(p)), "tng_prodrates_batch_rates")
+        torch.cuda.current_stream(sol.device).wait_stream(st)
+        return out, rates

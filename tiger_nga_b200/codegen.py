@@ -1,0 +1,367 @@
+"""CUDA code generator: mechanism table -> straight-line sm_100a device code.
+
+The reference's mechanism files are straight-line generated Fortran (``PRODRATES``,
+combustion/grimech30F.f90:4-2580). The GPU path keeps that shape -- one cell per thread,
+every rate constant, rate and production rate in registers, every coefficient an immediate --
+but generates it from the mechanism table and restructures the arithmetic for the GPU:
+
+* ``K = exp(lnA + n*LT + E*invRT)``: ``ln A`` folded into the exponent (one FMA pair per slot,
+  no separate multiply), ``1/(R T)`` formed once per cell instead of one division per slot;
+* Troe falloff (GETLINDRATECOEFF, grimech30F.f90:2583-2619) evaluated from the logarithms of
+  k0 and kinf directly -- ``log10(Pr) = (ln k0 + ln[M] - ln max(kinf,1e-60))/ln 10`` -- so the
+  k0/kinf exponentials and the ``log10`` of the reference collapse into one ``exp`` for Pr; the
+  centring factor F_cent and its logarithm are computed once per distinct F_cent expression
+  (a forward/reverse pair shares one);
+* production rates accumulated by scatter right after each rate ``W_r`` is formed (net
+  stoichiometric coefficient per species and slot), so W never has to be stored;
+* thermodynamics (COMPTHERMODATA, grimech30F.f90:2925-3516) evaluated after the rates for the
+  enthalpy term of the temperature equation (finitechem.f90:160-173).
+
+Two precision modes are emitted per mechanism:
+
+``rhs_fp64`` -- everything in FP64; agrees with the reference arithmetic to ~1e-14 relative.
+
+``rhs_mixed`` -- every rate is formed in base-2 log space and exponentiated with the FP32
+``ex2.approx`` unit: forward (and irreversible) slots assemble their exponent in FP32; the
+fitted reverse slots -- whose ``ln A_b - E_b/RT`` carries the large cancellations the
+equilibrium constant was folded into -- assemble it in FP64 and round only the final exponent.
+Third-body sums, production-rate accumulation and thermodynamics stay FP64.
+
+Both take ``LM`` (literal mode) as a template argument: 0 = reference literal kinds, 1 = all
+literals double. Generated files go to ``tiger_nga_b200/_build/gen``; they are rebuilt from the
+committed tables by :mod:`tiger_nga_b200.build`.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+from .mechanism import Mechanism
+
+LOG2E = 1.0 / math.log(2.0)
+INV_LN10 = 1.0 / math.log(10.0)
+LOG10_2 = math.log10(2.0)
+
+
+def _d(x: float) -> str:
+    if x == 0.0:
+        return "0.0"
+    return float(x).hex()
+
+
+def _f(x: float) -> str:
+    v = float(np.float32(x))
+    if v == 0.0:
+        return "0.0f"
+    return v.hex() + "f"
+
+
+def _lm(a: float, b: float, fmt=_d) -> str:
+    """Literal-mode select between the reference-kind value a and the all-double value b."""
+    sa, sb = fmt(a), fmt(b)
+    return sa if sa == sb else f"TNG_LM({sa}, {sb})"
+
+
+class _Gen:
+    def __init__(self, name: str):
+        self.name = name
+        self.m32 = Mechanism(name, "f32")
+        self.m64 = Mechanism(name, "f64")
+        m = self.m32
+        self.ns, self.nslot, self.nm = m.ns, m.nslot, m.nm
+        # first slot that needs each third-body set (as W factor or as falloff [M])
+        self.fc_keys32: dict[tuple, int] = {}
+
+    # ---------------------------------------------------------------- helpers
+    def arr_terms(self, a32, a64, log2: bool):
+        """(lnA, n, E) constant strings; log2=True scales to base-2 units."""
+        s = LOG2E if log2 else 1.0
+        lnA = _lm(math.log(a32.A) * s, math.log(a64.A) * s)
+        n = _lm(a32.n, a64.n) if a32.n is not None else None
+        E = _lm(a32.E * s, a64.E * s) if a32.E is not None else None
+        return lnA, n, E
+
+    def fc_code(self, idx: int, fc32, fc64, out: list[str], prec: str):
+        """Emit F_cent for one distinct expression; returns the names of log10(fc), log2(fc)."""
+        terms = []
+        for (a, form, x), (a6, _, x6) in zip(fc32, fc64):
+            # exact shortcuts: exp(-T/1e30) == 1.0 and exp(-T/1e-30) == 0.0 in double for any T in range
+            if form == 0 and x <= 1e-20:
+                continue
+            if form == 1 and x >= 1e20:
+                continue
+            if (form == 0 and x >= 1e20) or (form == 1 and x == 0.0):
+                terms.append(_lm(a, a6))
+                continue
+            if form == 0:
+                terms.append(f"{_lm(a, a6)} * exp(-T * {_lm(1.0 / x, 1.0 / x6)})")
+            else:
+                terms.append(f"{_lm(a, a6)} * exp(-{_lm(x, x6)} * invT)")
+        if not terms:
+            raise ValueError("F_cent is identically zero")
+        out.append(f"  const double fc{idx} = {' + '.join(terms)};")
+        out.append(f"  const double lfc{idx} = log(fc{idx});")
+        out.append(f"  const double l10fc{idx} = lfc{idx} * {_d(INV_LN10)};")
+        out.append(f"  const double ntmp{idx} = {_lm(self.m32.troe['c_n0'], self.m64.troe['c_n0'])} - "
+                   f"{_lm(self.m32.troe['c_n1'], self.m64.troe['c_n1'])} * l10fc{idx};")
+        out.append(f"  const double cc{idx} = -{_lm(self.m32.troe['c_c0'], self.m64.troe['c_c0'])} - "
+                   f"{_lm(self.m32.troe['c_c1'], self.m64.troe['c_c1'])} * l10fc{idx};")
+        if prec == "mixed":
+            out.append(f"  const float l2fcf{idx} = (float)(lfc{idx} * {_d(LOG2E)});")
+            out.append(f"  const float ntmpf{idx} = (float)ntmp{idx};")
+            out.append(f"  const float ccf{idx} = (float)cc{idx};")
+
+    # ---------------------------------------------------------------- one rhs function
+    def rhs(self, prec: str, dump: bool = False) -> str:
+        m32, m64 = self.m32, self.m64
+        ns = self.ns
+        o: list[str] = []
+        fn = f"rhs_{prec}"
+        o.append(f"template <int LM, bool DUMP>")
+        o.append(f"__device__ static __forceinline__ void {fn}(const double* __restrict__ s, double p, double* __restrict__ r,"
+                 f" double* __restrict__ dump, long long dld) {{")
+        o.append("  (void)dump; (void)dld;")
+        # rho and T
+        o.append("  double rho = s[0];")
+        for k in range(1, ns):
+            o.append(f"  rho = rho + s[{k}];")
+        o.append("  const double irho = 1.0 / rho;")
+        o.append(f"  const double T = s[{ns}] * irho;")
+        o.append("  const double LT = log(T);")
+        o.append(f"  const double invRT = 1.0 / ({_lm(m32.rgas, m64.rgas)} * T);")
+        o.append(f"  const double invT = {_lm(m32.rgas, m64.rgas)} * invRT;")
+        for k in range(ns):
+            o.append(f"  const double c{k} = s[{k}] * {_lm(1.0 / m32.wmol[k], 1.0 / m64.wmol[k])};")
+            o.append(f"  double cd{k} = 0.0;")
+        if prec == "mixed":
+            o.append("  const float LT2f = (float)(LT * %s);" % _d(LOG2E))
+            o.append("  const double LT2 = LT * %s;" % _d(LOG2E))
+            o.append("  const float invRTf = (float)invRT;")
+            for k in range(ns):
+                o.append(f"  const float lc{k} = tng_lg2f(fabsf((float)c{k}));")
+                o.append(f"  const float sg{k} = c{k} < 0.0 ? -1.0f : 1.0f;")
+        have_m: set[int] = set()
+        have_lc: set[int] = set()
+        have_fc: dict[tuple, int] = {}
+        lnprt_done = False
+
+        def need_m(j):
+            if j in have_m:
+                return
+            terms = m32.third_body[j]
+            terms64 = m64.third_body[j]
+            parts = []
+            for (s_, c), (_, c6) in zip(terms, terms64):
+                parts.append(f"c{s_}" if c == 1.0 and c6 == 1.0 else f"{_lm(c, c6)} * c{s_}")
+            o.append(f"  const double m{j} = {' + '.join(parts)};")
+            if prec == "mixed":
+                o.append(f"  const float lm{j} = tng_lg2f(fabsf((float)m{j}));")
+                o.append(f"  const float sm{j} = m{j} < 0.0 ? -1.0f : 1.0f;")
+            have_m.add(j)
+
+        for s32, s64 in zip(m32.slots, m64.slots):
+            r = s32.index
+            o.append(f"  // slot {r}: {s32.name}")
+            reverse = s32.reverse
+            if s32.kind == "falloff":
+                need_m(s32.M_fall)
+                if s32.M >= 0:
+                    need_m(s32.M)
+                if not lnprt_done:
+                    o.append("  const double lnprt = log(p * invRT);")
+                    lnprt_done = True
+                j = s32.M_fall
+                if j not in have_lc:
+                    o.append(f"  const double lcm{j} = m{j} > 0.0 ? log(m{j}) : lnprt;")
+                    have_lc.add(j)
+                key = s32.fc_key
+                lind = key == ((1.0, 1, 0.0),)  # F_cent == 1: plain Lindemann
+                if not lind and key not in have_fc:
+                    have_fc[key] = len(have_fc)
+                    self.fc_code(have_fc[key], s32.fc, s64.fc, o, prec)
+                lnA0, n0, E0 = self.arr_terms(s32.k0, s64.k0, False)
+                lnAi, ni, Ei = self.arr_terms(s32.kinf, s64.kinf, False)
+
+                def expo(lnA, n, E):
+                    e = lnA
+                    if E is not None:
+                        e = f"fma({E}, invRT, {e})"
+                    if n is not None:
+                        e = f"fma({n}, LT, {e})"
+                    return e
+
+                kmin = math.log(m32.troe["kmin"])
+                o.append(f"  {{ const double lk0 = {expo(lnA0, n0, E0)};")
+                o.append(f"    const double lki = {expo(lnAi, ni, Ei)};")
+                o.append(f"    const double lpr = lk0 + lcm{j} - fmax(lki, {_d(kmin)});")
+                if prec == "fp64":
+                    o.append("    const double pr = exp(lpr);")
+                    if lind:
+                        o.append("    double w = exp(lki) * pr / (1.0 + pr);")
+                    else:
+                        u = have_fc[key]
+                        o.append(f"    const double lg = lpr * {_d(INV_LN10)} + cc{u};")
+                        o.append(f"    const double f = lg / (ntmp{u} - {_lm(m32.troe['c_d'], m64.troe['c_d'])} * lg);")
+                        o.append(f"    double w = exp(lki + lfc{u} / (f * f + 1.0)) * pr / (1.0 + pr);")
+                    for c in s32.C:
+                        o.append(f"    w = w * c{c};")
+                    if s32.M >= 0:
+                        need_m(s32.M)
+                        o.append(f"    w = w * m{s32.M};")
+                else:
+                    # FP64 exponents of k0/kinf, Troe blending in FP32 base-2 logs
+                    o.append("    const float lpr2 = (float)(lpr * %s);" % _d(LOG2E))
+                    o.append("    const float lki2 = (float)(lki * %s);" % _d(LOG2E))
+                    if lind:
+                        o.append("    const float lk2 = lki2 + lpr2 - tng_softplus2f(lpr2);")
+                    else:
+                        u = have_fc[key]
+                        o.append(f"    const float lg = lpr2 * {_f(LOG10_2)} + ccf{u};")
+                        o.append(f"    const float f = __fdividef(lg, ntmpf{u} - {_f(m32.troe['c_d'])} * lg);")
+                        o.append(f"    const float lk2 = lki2 + __fdividef(l2fcf{u}, f * f + 1.0f) + lpr2 - tng_softplus2f(lpr2);")
+                    if s32.M >= 0:
+                        need_m(s32.M)
+                    tail = "".join(f" + lc{c}" for c in s32.C) + (f" + lm{s32.M}" if s32.M >= 0 else "")
+                    sg = "".join(f" * sg{c}" for c in s32.C) + (f" * sm{s32.M}" if s32.M >= 0 else "")
+                    o.append(f"    const double w = (double)(tng_ex2f(lk2{tail}){sg});")
+                if dump:
+                    o.append(f"    if (DUMP) dump[{r}LL * dld] = w;")
+                self.scatter(r, o, "    ")
+                o.append("  }")
+                continue
+
+            a32, a64 = s32.arr, s64.arr
+            if s32.M >= 0:
+                need_m(s32.M)
+            if prec == "fp64":
+                if a32.n is None and a32.E is None:
+                    o.append(f"  {{ double w = {_lm(a32.A, a64.A)};")
+                else:
+                    lnA, n, E = self.arr_terms(a32, a64, False)
+                    e = lnA
+                    if E is not None:
+                        e = f"fma({E}, invRT, {e})"
+                    if n is not None:
+                        e = f"fma({n}, LT, {e})"
+                    o.append(f"  {{ double w = exp({e});")
+                for c in s32.C:
+                    o.append(f"    w = w * c{c};")
+                if s32.M >= 0:
+                    o.append(f"    w = w * m{s32.M};")
+            else:
+                lnA, n, E = self.arr_terms(a32, a64, True)
+                if reverse:
+                    e = lnA
+                    if E is not None:
+                        e = f"fma({E}, invRT, {e})"
+                    if n is not None:
+                        e = f"fma({n}, LT2, {e})"
+                    head = f"(float)({e})"
+                else:
+                    lnAf = _lm(math.log(a32.A) * LOG2E, math.log(a64.A) * LOG2E, _f)
+                    e = lnAf
+                    if E is not None:
+                        e = f"fmaf({_lm(a32.E * LOG2E, a64.E * LOG2E, _f)}, invRTf, {e})"
+                    if n is not None:
+                        e = f"fmaf({_lm(a32.n, a64.n, _f)}, LT2f, {e})"
+                    head = e
+                tail = "".join(f" + lc{c}" for c in s32.C) + (f" + lm{s32.M}" if s32.M >= 0 else "")
+                sg = "".join(f" * sg{c}" for c in s32.C) + (f" * sm{s32.M}" if s32.M >= 0 else "")
+                o.append(f"  {{ const double w = (double)(tng_ex2f({head}{tail}){sg});")
+            if dump:
+                o.append(f"    if (DUMP) dump[{r}LL * dld] = w;")
+            self.scatter(r, o, "    ")
+            o.append("  }")
+
+        # epilogue: production rates -> mass rates, temperature equation
+        o.append("  double cpm = 0.0, tmp = 0.0;")
+        o.append(f"  if (T > {_lm(m32.tmid, m64.tmid)}) {{")
+        self.thermo_block(m32.th_hi, m64.th_hi, o)
+        o.append("  } else {")
+        self.thermo_block(m32.th_lo, m64.th_lo, o)
+        o.append("  }")
+        o.append(f"  r[{ns}] = tmp / cpm;")
+        o.append("}")
+        return "\n".join(o)
+
+    def scatter(self, r: int, o: list[str], ind: str):
+        col = self.m32.nu[:, r]
+        col64 = self.m64.nu[:, r]
+        for k in range(self.ns):
+            v, v6 = col[k], col64[k]
+            if v == 0.0 and v6 == 0.0:
+                continue
+            if v == 1.0 and v6 == 1.0:
+                o.append(f"{ind}cd{k} += w;")
+            elif v == -1.0 and v6 == -1.0:
+                o.append(f"{ind}cd{k} -= w;")
+            else:
+                o.append(f"{ind}cd{k} = fma({_lm(v, v6)}, w, cd{k});")
+
+    def thermo_block(self, t32, t64, o):
+        m32, m64 = self.m32, self.m64
+        for k in range(self.ns):
+            a, b = t32[k], t64[k]
+            L = lambda i: _lm(a[i], b[i])  # noqa: E731
+            o.append(f"    {{ const double y = c{k} * ({_lm(m32.wmol[k], m64.wmol[k])} * irho);")
+            o.append(f"      const double cpk = {L(0)} * ({L(7)} + T * ({L(8)} + T * ({L(9)} + T * ({L(10)} + T * {L(11)}))));")
+            o.append(f"      const double hk = {L(0)} * (T * ({L(1)} + T * ({L(2)} + T * ({L(3)} + T * ({L(4)} + T * {L(5)})))) + {L(6)});")
+            o.append(f"      const double rk = cd{k} * {_lm(m32.wmol[k], m64.wmol[k])};")
+            o.append(f"      r[{k}] = rk;")
+            o.append(f"      cpm = fma(y, cpk, cpm);")
+            o.append(f"      tmp = fma(-hk, rk, tmp); }}")
+
+    def header(self) -> str:
+        m32, m64 = self.m32, self.m64
+        cls = f"Mech_{self.name}"
+        out = [f"// Generated from tiger_nga_b200/mechanisms/{self.name}.json by tiger_nga_b200/codegen.py.",
+               "// Do not edit: regenerate with tiger_nga_b200.build.",
+               "#pragma once",
+               '#include "tng_device.cuh"',
+               "namespace tng {",
+               f"struct {cls} {{",
+               f"  static constexpr int NS = {self.ns};",
+               f"  static constexpr int NSLOT = {self.nslot};",
+               f"  static constexpr int NM = {self.nm};",
+               f'  static constexpr const char* NAME = "{self.name}";']
+        out.append(self.rhs("fp64", dump=True))
+        out.append(self.rhs("mixed", dump=True))
+        out.append("};")
+        # host-side info
+        names = ", ".join(f'"{s}"' for s in m32.species)
+        out.append(f"static const char* const {self.name}_species[{self.ns}] = {{{names}}};")
+        out.append(f"static const double {self.name}_wmol[2][{self.ns}] = {{{{{', '.join(_d(x) for x in m32.wmol)}}}, "
+                   f"{{{', '.join(_d(x) for x in m64.wmol)}}}}};")
+        el = m32.elem
+        out.append(f"static const int {self.name}_nelem = {el.shape[0]};")
+        out.append(f'static const char* const {self.name}_elements[{el.shape[0]}] = {{{", ".join(chr(34) + e + chr(34) for e in m32.elements)}}};')
+        out.append(f"static const double {self.name}_elem[{el.shape[0]}][{self.ns}] = {{"
+                   + ", ".join("{" + ", ".join(_d(x) for x in row) + "}" for row in el) + "};")
+        out.append("}  // namespace tng")
+        return "\n".join(out) + "\n"
+
+
+def generate(name: str) -> str:
+    return _Gen(name).header()
+
+
+def write_all(out_dir: str, names=("hydrogen", "grimech30", "dme39")) -> list[str]:
+    os.makedirs(out_dir, exist_ok=True)
+    paths = []
+    for n in names:
+        src = generate(n)
+        path = os.path.join(out_dir, f"mech_{n}.cuh")
+        old = open(path).read() if os.path.exists(path) else None
+        if old != src:
+            with open(path, "w") as fh:
+                fh.write(src)
+        paths.append(path)
+    return paths
+
+
+if __name__ == "__main__":
+    for p in write_all(sys.argv[1] if len(sys.argv) > 1 else "tiger_nga_b200/_build/gen"):
+        print(p)

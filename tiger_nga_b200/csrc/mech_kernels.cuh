@@ -1,0 +1,25 @@
+// Builds the operation table of one generated mechanism.
+#pragma once
+#include "kernels.cuh"
+
+namespace tng {
+
+template <class Mech>
+MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int nelem, const char* const* elements,
+                 const double* elem) {
+  MechOps o{};
+  o.name = Mech::NAME;
+  o.ns = Mech::NS;
+  o.nslot = Mech::NSLOT;
+  o.nm = Mech::NM;
+  o.nelem = nelem;
+  o.species = species;
+  o.wmol[0] = wmol[0];
+  o.wmol[1] = wmol[1];
+  o.elements = elements;
+  o.elem = elem;
+  o.rhs = &launch_rhs<Mech>;
+  return o;
+}
+
+}  // namespace tng
