@@ -50,7 +50,8 @@ typedef struct tng_cfg {
   int max_steps;    /* internal steps per cell and substep (MAX_NSTEPS, finitechem.f90:1025) */
   int max_newton;   /* Newton iterations per internal step before the step is retried */
   int block_size;   /* threads per block of the rate kernel, 0 = tuned default */
-  int reserved[8];
+  int rate_variant; /* rate-kernel variant (0 plain, 1 block-synchronised, 2 + register cap), -1 = tuned */
+  int reserved[7];
 } tng_cfg;
 
 typedef struct tng_chem tng_chem;

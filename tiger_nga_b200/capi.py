@@ -29,7 +29,8 @@ TNG_DEVICE_PTRS, TNG_HOST_PTRS = 0, 1
 class TngCfg(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("literal_mode", ctypes.c_int), ("device", ctypes.c_int),
                 ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_steps", ctypes.c_int),
-                ("max_newton", ctypes.c_int), ("block_size", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
+                ("max_newton", ctypes.c_int), ("block_size", ctypes.c_int), ("rate_variant", ctypes.c_int),
+                ("reserved", ctypes.c_int * 7)]
 
 
 class ChemError(RuntimeError):
@@ -178,12 +179,12 @@ class FiniteChem:
 
         if not (sol.is_cuda and sol.dtype == torch.float64 and sol.dim() == 2 and sol.shape[0] == nv):
             raise ValueError(f"sol must be a CUDA float64 tensor of shape ({nv}, ncells)")
-        if sol.stride(1) != 1:
+        if sol.shape[1] > 1 and sol.stride(1) != 1:
             raise ValueError("sol must be species-major with unit stride along cells")
-        ld = sol.stride(0)
+        ld = max(sol.stride(0), sol.shape[1])
         if out is None:
             out = torch.empty_like(sol)
-        if out.stride() != sol.stride():
+        if sol.shape[1] > 1 and out.stride() != sol.stride():
             raise ValueError("out must have the same strides as sol")
         st = self.torch_stream()
         st.wait_stream(torch.cuda.current_stream(sol.device))

@@ -120,7 +120,7 @@ class _Gen:
         ns = self.ns
         o: list[str] = []
         fn = f"rhs_{prec}"
-        o.append(f"template <int LM, bool DUMP>")
+        o.append(f"template <int LM, bool DUMP, int SYNC>")
         o.append(f"__device__ static __forceinline__ void {fn}(const double* __restrict__ s, double p, double* __restrict__ r,"
                  f" double* __restrict__ dump, long long dld) {{")
         o.append("  (void)dump; (void)dld;")
@@ -164,6 +164,8 @@ class _Gen:
 
         for s32, s64 in zip(m32.slots, m64.slots):
             r = s32.index
+            if r > 0 and r % 48 == 0:
+                o.append("  if constexpr (SYNC != 0) __syncthreads();  // keep the block's warps on the same code lines")
             o.append(f"  // slot {r}: {s32.name}")
             reverse = s32.reverse
             if s32.kind == "falloff":

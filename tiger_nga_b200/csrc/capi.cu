@@ -56,6 +56,7 @@ void tng_default_cfg(tng_cfg* cfg) {
   cfg->max_steps = 10000;
   cfg->max_newton = 4;
   cfg->block_size = 0;
+  cfg->rate_variant = -1;
 }
 
 int tng_last_error(char* buf, int len) {
@@ -169,7 +170,7 @@ int tng_prodrates_batch(tng_chem* h, const double* sol, double* rhs, int64_t nce
   const int prec = h->cfg.precision, lm = h->cfg.literal_mode, blk = h->cfg.block_size;
   cudaError_t e;
   if (flags == TNG_DEVICE_PTRS) {
-    e = h->ops->rhs(prec, lm, sol, rhs, nullptr, ncells, ld, p, blk, h->stream);
+    e = h->ops->rhs(prec, lm, h->cfg.rate_variant, sol, rhs, nullptr, ncells, ld, p, blk, h->stream);
     if (e != cudaSuccess) return cuda_error(e, "rate kernel launch");
     return TNG_OK;
   }
@@ -202,7 +203,7 @@ int tng_prodrates_batch(tng_chem* h, const double* sol, double* rhs, int64_t nce
     }
     cudaEventRecord(ev_in[b], cs);
     cudaStreamWaitEvent(h->stream, ev_in[b], 0);
-    if ((e = h->ops->rhs(prec, lm, din, dout, nullptr, n, n, p, blk, h->stream)) != cudaSuccess) {
+    if ((e = h->ops->rhs(prec, lm, h->cfg.rate_variant, din, dout, nullptr, n, n, p, blk, h->stream)) != cudaSuccess) {
       rc = cuda_error(e, "rate kernel launch");
       break;
     }
@@ -230,7 +231,7 @@ int tng_prodrates_batch_rates(tng_chem* h, const double* sol, double* rhs, doubl
   if (h->cfg.literal_mode != TNG_LIT_REF)
     return set_error(TNG_ERR_ARG, "tng_prodrates_batch_rates: only built for TNG_LIT_REF");
   DeviceGuard g(h->cfg.device);
-  cudaError_t e = h->ops->rhs(h->cfg.precision, 0, sol, rhs, rates, ncells, ld, p, h->cfg.block_size, h->stream);
+  cudaError_t e = h->ops->rhs(h->cfg.precision, 0, 0, sol, rhs, rates, ncells, ld, p, h->cfg.block_size, h->stream);
   if (e != cudaSuccess) return cuda_error(e, "rate kernel launch");
   return TNG_OK;
 }

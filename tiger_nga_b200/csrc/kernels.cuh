@@ -14,21 +14,30 @@ namespace tng {
 
 constexpr int kRhsMaxBlock = 256;
 
-template <class Mech, int LM, int PREC, bool DUMP>
-__global__ void __launch_bounds__(kRhsMaxBlock) k_rhs(const double* __restrict__ sol, double* __restrict__ out,
-                                                      double* __restrict__ dump, long long n, long long ld, double p) {
+// SYNC != 0 inserts block barriers every 48 slots inside the generated code so that the warps
+// of a block stay on the same instruction lines (the straight-line code is far larger than the
+// instruction cache); the loop below is block-uniform so every thread reaches every barrier.
+template <class Mech, int LM, int PREC, bool DUMP, int SYNC, int MINB>
+__global__ void __launch_bounds__(kRhsMaxBlock, MINB)
+    k_rhs(const double* __restrict__ sol, double* __restrict__ out, double* __restrict__ dump, long long n,
+          long long ld, double p) {
   constexpr int NV = Mech::NS + 1;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const long long i = base + threadIdx.x;
+    const bool live = i < n;
+    const long long ii = live ? i : n - 1;
     double s[NV], r[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) s[v] = __ldcs(sol + v * ld + i);
+    for (int v = 0; v < NV; ++v) s[v] = __ldcs(sol + v * ld + ii);
     if constexpr (PREC == 0)
-      Mech::template rhs_fp64<LM, DUMP>(s, p, r, DUMP ? dump + i : nullptr, ld);
+      Mech::template rhs_fp64<LM, DUMP, SYNC>(s, p, r, DUMP && live ? dump + i : nullptr, ld);
     else
-      Mech::template rhs_mixed<LM, DUMP>(s, p, r, DUMP ? dump + i : nullptr, ld);
+      Mech::template rhs_mixed<LM, DUMP, SYNC>(s, p, r, DUMP && live ? dump + i : nullptr, ld);
+    if (live) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) __stcs(out + v * ld + i, r[v]);
+      for (int v = 0; v < NV; ++v) __stcs(out + v * ld + i, r[v]);
+    }
   }
 }
 
@@ -48,39 +57,47 @@ struct MechOps {
   const char* const* elements;
   const double* elem;  // nelem x ns, row-major
   // rate evaluation: prec 0/1, lm 0/1; dump may be null
-  cudaError_t (*rhs)(int prec, int lm, const double* sol, double* out, double* dump, long long n, long long ld,
-                     double p, int block, cudaStream_t st);
+  cudaError_t (*rhs)(int prec, int lm, int variant, const double* sol, double* out, double* dump, long long n,
+                     long long ld, double p, int block, cudaStream_t st);
 };
 
-template <class Mech>
-cudaError_t launch_rhs(int prec, int lm, const double* sol, double* out, double* dump, long long n, long long ld,
-                       double p, int block, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  if (block <= 0 || block > kRhsMaxBlock) block = 128;
+// Kernel variants of the rate evaluation (the autotuner's choices): 0 = plain, 1 = block
+// barriers every 48 slots, 2 = barriers + a 2-blocks-per-SM register cap.
+constexpr int kRhsVariants = 3;
+
+template <class Mech, int LM, int PREC>
+cudaError_t launch_rhs_v(int variant, const double* sol, double* out, double* dump, long long n, long long ld,
+                         double p, int block, cudaStream_t st) {
   const unsigned grid = rhs_grid(n, block);
-  const bool d = dump != nullptr;
-  if (prec == 0) {
-    if (lm == 0) {
-      if (d)
-        k_rhs<Mech, 0, 0, true><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-      else
-        k_rhs<Mech, 0, 0, false><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-    } else {
-      if (d) return cudaErrorInvalidValue;
-      k_rhs<Mech, 1, 0, false><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-    }
-  } else {
-    if (lm == 0) {
-      if (d)
-        k_rhs<Mech, 0, 1, true><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-      else
-        k_rhs<Mech, 0, 1, false><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-    } else {
-      if (d) return cudaErrorInvalidValue;
-      k_rhs<Mech, 1, 1, false><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
-    }
+  if (dump) {
+    k_rhs<Mech, LM, PREC, true, 0, 1><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
+    return cudaGetLastError();
+  }
+  if (variant < 0) variant = 1;  // tuned default (see profiles/)
+  switch (variant) {
+    case 1:
+      k_rhs<Mech, LM, PREC, false, 1, 1><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
+      break;
+    case 2:
+      k_rhs<Mech, LM, PREC, false, 1, 2><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
+      break;
+    default:
+      k_rhs<Mech, LM, PREC, false, 0, 1><<<grid, block, 0, st>>>(sol, out, dump, n, ld, p);
   }
   return cudaGetLastError();
+}
+
+template <class Mech>
+cudaError_t launch_rhs(int prec, int lm, int variant, const double* sol, double* out, double* dump, long long n,
+                       long long ld, double p, int block, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  if (block <= 0 || block > kRhsMaxBlock) block = 128;
+  if (dump && lm != 0) return cudaErrorInvalidValue;
+  if (prec == 0)
+    return lm == 0 ? launch_rhs_v<Mech, 0, 0>(variant, sol, out, dump, n, ld, p, block, st)
+                   : launch_rhs_v<Mech, 1, 0>(0, sol, out, nullptr, n, ld, p, block, st);
+  return lm == 0 ? launch_rhs_v<Mech, 0, 1>(variant, sol, out, dump, n, ld, p, block, st)
+                 : launch_rhs_v<Mech, 1, 1>(0, sol, out, nullptr, n, ld, p, block, st);
 }
 
 }  // namespace tng
