@@ -51,7 +51,10 @@ typedef struct tng_cfg {
   int max_newton;   /* Newton iterations per internal step before the step is retried */
   int block_size;   /* threads per block of the rate kernel, 0 = tuned default */
   int rate_variant; /* rate-kernel variant (0 plain, 1 block-synchronised, 2 + register cap), -1 = tuned */
-  int reserved[7];
+  int solver_warps; /* cells (warps) per block of the implicit solver: 2, 4 or 8; 0 = tuned */
+  int pass_budget;  /* internal steps per cell and solver pass before the cell is re-queued; 0 = no limit */
+  int max_passes;   /* passes captured in the solver's CUDA graph (the last one has no budget) */
+  int reserved[4];
 } tng_cfg;
 
 typedef struct tng_chem tng_chem;
@@ -94,6 +97,39 @@ int tng_prodrates_batch_rates(tng_chem* h, const double* sol, double* rhs, doubl
 
 /* Wait for the handle's stream; returns the first asynchronous error, if any. */
 int tng_chem_sync(tng_chem* h);
+
+/* Statistics of one implicit substep. */
+typedef struct tng_substep_stats {
+  int64_t cells;         /* cells integrated */
+  int64_t cells_failed;  /* cells whose integration stopped with a non-zero status */
+  int64_t steps;         /* internal BDF steps, all cells */
+  int64_t newton_iters;  /* Newton iterations, all cells */
+  int64_t jacobians;     /* Jacobian evaluations + LU factorisations, all cells */
+  int max_steps_cell;    /* largest per-cell step count */
+  int max_newton_cell;   /* largest per-cell Newton iteration count */
+  int passes;            /* solver passes that found work */
+  int newton_hist[16];   /* cells by Newton iterations: [0], [1], [2,3], [4,7], ..., [2^14, inf) */
+  double ms;             /* device time of the substep (CUDA events), host copies excluded */
+} tng_substep_stats;
+
+/* The implicit chemistry substep over a batch: the per-cell CVODE integration of
+ * finitechem_source_chemistry (finitechem.f90:962-1071, CVODE calls :987-1068) on the GPU.
+ * state (species-major, variable v of cell i at [v*ld + i], v = 0..N: rho*Y_k then rho*T) is
+ * advanced in place over dt (dts[i] per cell when dts is non-null, else the scalar dt) at
+ * pressure p with the handle's rtol/atol/max_steps. Cells are integrated by a persistent
+ * work-stealing kernel; the pass loop runs as one CUDA graph. cell_nst / cell_nni / cell_status
+ * (device int arrays of ncells, nullable) receive per-cell step and Newton counts and status
+ * (0 ok, 1 max steps, 2 convergence failures, 3 error-test failures, 4 non-finite, 5 step too
+ * small). flags: TNG_DEVICE_PTRS (state, dts and cell arrays on the device) or TNG_HOST_PTRS
+ * (state and dts on the host; cell arrays must then be null). stats may be null; when given the
+ * call waits for the device. */
+int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
+                      int flags, int* cell_nst, int* cell_nni, int* cell_status, tng_substep_stats* stats);
+
+/* Parity helper: the solver's own (table-driven, warp-cooperative) right-hand side and, when
+ * jac is non-null, its Jacobian (cell-major, (N+1)^2 row-major per cell), device pointers. */
+int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,
+                       double* jac);
 
 /* Measurement helper (no reference counterpart): sustained FP64 FMA throughput of a device in
  * TFLOP/s (FMA = 2 flops), the denominator of the FP64-pipe roofline of the rate kernels. */

@@ -34,7 +34,7 @@ REF_LIB = os.path.join(HERE, "_ref", "libref_mech.so")
 def build_oracle(force: bool = False) -> str:
     """Compile chem_oracle.c (and solver_oracle.c when present) with gcc + OpenMP."""
     srcs = [os.path.join(HERE, f) for f in ("chem_oracle.c", "solver_oracle.c") if os.path.exists(os.path.join(HERE, f))]
-    newest = max(os.path.getmtime(s) for s in srcs)
+    newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(HERE, "orc_mech.h")])
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         os.makedirs(os.path.dirname(LIB), exist_ok=True)
         tmp = LIB + f".{os.getpid()}.tmp"
@@ -77,6 +77,7 @@ class _Mech(ctypes.Structure):
         ("cd_ptr", ctypes.c_void_p), ("cd_sign", ctypes.c_void_p), ("cd_slot", ctypes.c_void_p),
         ("cd_coef", ctypes.c_void_p),
         ("tmid", ctypes.c_double), ("th_hi", ctypes.c_void_p), ("th_lo", ctypes.c_void_p), ("wmol", ctypes.c_void_p),
+        ("nu", ctypes.c_void_p), ("eff", ctypes.c_void_p),
     ]
 
 
@@ -163,6 +164,15 @@ class Oracle:
             return out
 
         self.wmol = D([L(x) for x in tab["molar_mass"]])
+        nu = np.zeros((ns, nslot))
+        for k, terms in enumerate(tab["cdot"]):
+            for sgn, c, r in terms:
+                nu[k, r] += sgn * L(c)
+        eff = np.zeros((max(nm, 1), ns))
+        for j, terms in enumerate(tab["third_body"]):
+            for s_, c in terms:
+                eff[j, s_] += L(c)
+        self.nu_dense, self.eff_dense = D(nu), D(eff)
         m = _Mech()
         m.ns, m.nslot, m.nm, m.nfo = ns, nslot, nm, len(foM)
         m.rgas = L(tab["rgas"])
@@ -177,7 +187,8 @@ class Oracle:
                            ("w_ptr", I(w_ptr)), ("w_sp", I(w_sp + [0])), ("w_M", I(w_M)),
                            ("cd_ptr", I(cd_ptr)), ("cd_sign", I(cd_sign + [0])), ("cd_slot", I(cd_slot + [0])),
                            ("cd_coef", D(cd_coef + [0])),
-                           ("th_hi", D(thermo("hi"))), ("th_lo", D(thermo("lo"))), ("wmol", self.wmol)):
+                           ("th_hi", D(thermo("hi"))), ("th_lo", D(thermo("lo"))), ("wmol", self.wmol),
+                           ("nu", self.nu_dense), ("eff", self.eff_dense)):
             setattr(m, fname, _p(val))
         m.tmid = L(tab["thermo"]["tmid"])
         self._keep = keep
@@ -189,6 +200,7 @@ class Oracle:
         self.lib.orc_rhs_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
                                            ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         self.lib.orc_max_threads.restype = ctypes.c_int
+        _solver_protos(self.lib)
         self.lib.orc_rhs_gross_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double,
                                                  ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         self.lib.orc_rates_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
@@ -244,6 +256,73 @@ class Oracle:
 
     def max_threads(self):
         return self.lib.orc_max_threads()
+
+
+class SolverCfg(ctypes.Structure):
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_steps", ctypes.c_int),
+                ("maxcor", ctypes.c_int), ("msbp", ctypes.c_int), ("dgmax", ctypes.c_double)]
+
+
+class CellStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("nst", ctypes.c_int), ("nni", ctypes.c_int), ("nje", ctypes.c_int),
+                ("nef", ctypes.c_int), ("ncf", ctypes.c_int), ("nrhs", ctypes.c_int), ("q", ctypes.c_int),
+                ("h", ctypes.c_double)]
+
+
+def _solver_protos(lib):
+    lib.orc_jacobian.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                 ctypes.c_void_p]
+    lib.orc_bdf_cell.argtypes = [ctypes.POINTER(_Mech), ctypes.POINTER(SolverCfg), ctypes.c_void_p, ctypes.c_double,
+                                 ctypes.c_double, ctypes.POINTER(CellStats)]
+    lib.orc_bdf_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.POINTER(SolverCfg), ctypes.c_void_p, ctypes.c_int64,
+                                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    lib.orc_lu.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    lib.orc_lu.restype = ctypes.c_int
+    lib.orc_lu_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+
+
+def solver_cfg(rtol=1e-6, atol=1e-12, max_steps=10000, maxcor=3, msbp=20, dgmax=0.3):
+    return SolverCfg(rtol, atol, max_steps, maxcor, msbp, dgmax)
+
+
+def _oracle_jacobian(self, u, p):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    f0 = self.rhs(u, p)
+    J = np.zeros((self.ns + 1, self.ns + 1))
+    self.lib.orc_jacobian(ctypes.byref(self.m), _p(u), float(p), _p(f0), _p(J))
+    return J
+
+
+def _oracle_substep_cell(self, u, dt, p, cfg=None):
+    u = np.array(u, dtype=np.float64)
+    st = CellStats()
+    cfg = cfg or solver_cfg()
+    self.lib.orc_bdf_cell(ctypes.byref(self.m), ctypes.byref(cfg), _p(u), float(dt), float(p), ctypes.byref(st))
+    return u, {k: getattr(st, k) for k, _ in CellStats._fields_}
+
+
+def _oracle_substep_batch(self, state, dt, p, cfg=None, nthreads=0):
+    """Integrate a species-major batch (N+1, ncells) over dt (scalar or per cell)."""
+    out = np.array(state, dtype=np.float64, order="C", copy=True)
+    n = out.shape[1]
+    cfg = cfg or solver_cfg()
+    nst = np.zeros(n, dtype=np.int32)
+    nni = np.zeros(n, dtype=np.int32)
+    status = np.zeros(n, dtype=np.int32)
+    if np.ndim(dt) == 0:
+        dts, dts_p, dts_s = None, None, float(dt)
+    else:
+        dts = np.ascontiguousarray(dt, dtype=np.float64)
+        dts_p, dts_s = _p(dts), 0.0
+    self.lib.orc_bdf_batch(ctypes.byref(self.m), ctypes.byref(cfg), _p(out), n, n, dts_p, dts_s, float(p), _p(nst),
+                           _p(nni), _p(status), int(nthreads))
+    return out, {"nst": nst, "nni": nni, "status": status}
+
+
+Oracle.jacobian = _oracle_jacobian
+Oracle.substep_cell = _oracle_substep_cell
+Oracle.substep_batch = _oracle_substep_batch
 
 
 class Reference:

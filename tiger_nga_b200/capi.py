@@ -30,7 +30,20 @@ class TngCfg(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("literal_mode", ctypes.c_int), ("device", ctypes.c_int),
                 ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_steps", ctypes.c_int),
                 ("max_newton", ctypes.c_int), ("block_size", ctypes.c_int), ("rate_variant", ctypes.c_int),
-                ("reserved", ctypes.c_int * 7)]
+                ("solver_warps", ctypes.c_int), ("pass_budget", ctypes.c_int), ("max_passes", ctypes.c_int),
+                ("reserved", ctypes.c_int * 4)]
+
+
+class SubstepStats(ctypes.Structure):
+    _fields_ = [("cells", ctypes.c_int64), ("cells_failed", ctypes.c_int64), ("steps", ctypes.c_int64),
+                ("newton_iters", ctypes.c_int64), ("jacobians", ctypes.c_int64), ("max_steps_cell", ctypes.c_int),
+                ("max_newton_cell", ctypes.c_int), ("passes", ctypes.c_int), ("newton_hist", ctypes.c_int * 16),
+                ("ms", ctypes.c_double)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "newton_hist"}
+        d["newton_hist"] = list(self.newton_hist)
+        return d
 
 
 class ChemError(RuntimeError):
@@ -63,6 +76,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_prodrates_batch": (I, [V, V, V, L, L, D, I]),
         "tng_prodrates_batch_rates": (I, [V, V, V, V, L, L, D]),
         "tng_bench_fp64_peak": (I, [I, ctypes.POINTER(D)]),
+        "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
+        "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -216,3 +231,81 @@ class FiniteChem:
                                                   float(p)), "tng_prodrates_batch_rates")
         torch.cuda.current_stream(sol.device).wait_stream(st)
         return out, rates
+
+
+def _substep(self, state, dt, p: float, cell_counts: bool = False, stats: bool = True):
+    """The implicit chemistry substep (finitechem_source_chemistry's per-cell integration).
+
+    ``state`` is a species-major (N+1, ncells) batch of (rho*Y_k, rho*T), advanced in place over
+    ``dt`` (a scalar or a per-cell array/tensor). CUDA tensors stay on the device; NumPy arrays
+    go through the host-pointer path. Returns the statistics dict (and per-cell counters when
+    ``cell_counts``).
+    """
+    nv = self.nspecies + 1
+    st = SubstepStats()
+    stp = ctypes.byref(st) if stats else None
+    if isinstance(state, np.ndarray):
+        if state.dtype != np.float64 or state.ndim != 2 or state.shape[0] != nv or not state.flags.c_contiguous:
+            raise ValueError(f"state must be a C-contiguous float64 array of shape ({nv}, ncells)")
+        n = state.shape[1]
+        dts = None
+        if np.ndim(dt):
+            dts = np.ascontiguousarray(dt, dtype=np.float64)
+            if dts.shape != (n,):
+                raise ValueError("per-cell dt must have shape (ncells,)")
+        _check(self.lib.tng_substep_batch(self.h, state.ctypes.data, n, n, dts.ctypes.data if dts is not None else None,
+                                          0.0 if dts is not None else float(dt), float(p), TNG_HOST_PTRS, None, None,
+                                          None, stp), "tng_substep_batch")
+        return st.as_dict() if stats else None
+    import torch
+
+    if not (state.is_cuda and state.dtype == torch.float64 and state.dim() == 2 and state.shape[0] == nv):
+        raise ValueError(f"state must be a CUDA float64 tensor of shape ({nv}, ncells)")
+    n = state.shape[1]
+    if n > 1 and state.stride(1) != 1:
+        raise ValueError("state must be species-major with unit stride along cells")
+    ld = max(state.stride(0), n)
+    dts = None
+    if not isinstance(dt, (float, int)):
+        dts = torch.as_tensor(dt, dtype=torch.float64, device=state.device).contiguous()
+        if dts.shape != (n,):
+            raise ValueError("per-cell dt must have shape (ncells,)")
+    cnt = None
+    if cell_counts:
+        cnt = torch.zeros((3, n), dtype=torch.int32, device=state.device)
+    sst = self.torch_stream()
+    sst.wait_stream(torch.cuda.current_stream(state.device))
+    _check(self.lib.tng_substep_batch(self.h, state.data_ptr(), n, ld, dts.data_ptr() if dts is not None else None,
+                                      0.0 if dts is not None else float(dt), float(p), TNG_DEVICE_PTRS,
+                                      cnt[0].data_ptr() if cnt is not None else None,
+                                      cnt[1].data_ptr() if cnt is not None else None,
+                                      cnt[2].data_ptr() if cnt is not None else None, stp), "tng_substep_batch")
+    torch.cuda.current_stream(state.device).wait_stream(sst)
+    out = st.as_dict() if stats else None
+    if cell_counts:
+        return out, {"nst": cnt[0], "nni": cnt[1], "status": cnt[2]}
+    return out
+
+
+def _solver_rhs_jac(self, state, p: float, jacobian: bool = True):
+    """The solver's own right-hand side and Jacobian (parity helper), CUDA tensors."""
+    import torch
+
+    nv = self.nspecies + 1
+    n = state.shape[1]
+    if state.stride(1) != 1 and n > 1:
+        raise ValueError("state must be species-major")
+    rhs = torch.empty((nv, n), dtype=torch.float64, device=state.device)
+    jac = torch.empty((n, nv, nv), dtype=torch.float64, device=state.device) if jacobian else None
+    if state.stride(0) != n:
+        state = state.contiguous()
+    sst = self.torch_stream()
+    sst.wait_stream(torch.cuda.current_stream(state.device))
+    _check(self.lib.tng_solver_rhs_jac(self.h, state.data_ptr(), n, n, float(p), rhs.data_ptr(),
+                                       jac.data_ptr() if jac is not None else None), "tng_solver_rhs_jac")
+    torch.cuda.current_stream(state.device).wait_stream(sst)
+    return rhs, jac
+
+
+FiniteChem.substep = _substep
+FiniteChem.solver_rhs_jac = _solver_rhs_jac

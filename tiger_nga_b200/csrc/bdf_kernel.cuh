@@ -1,0 +1,458 @@
+// The per-cell BDF integration (warp-cooperative) and the persistent work-stealing kernel.
+// Same algorithm and constants as oracle/solver_oracle.c (orc_bdf_cell).
+#pragma once
+#include "solver.cuh"
+
+namespace tng {
+
+struct BdfCoef {
+  double L[kQmax + 2][kQmax + 2];
+  double errc[kQmax + 2], dnc[kQmax + 2], upc[kQmax + 2];
+};
+
+struct BdfLaunch {
+  BdfArgs a;
+  BdfCoef c;
+  const int* n_in_dev;  // when non-null, the number of queued cells is read from device memory
+};
+
+// two-entry-per-lane vector helpers
+__device__ __forceinline__ double wrms2(const double v0, const double v1, const double w0, const double w1,
+                                        const int nv, const int lane) {
+  const double a = lane < nv ? v0 * w0 : 0.0;
+  const double b = lane + 32 < nv ? v1 * w1 : 0.0;
+  return sqrt(warp_sum(a * a + b * b) / nv);
+}
+
+__device__ __forceinline__ bool warp_all_finite(const double v0, const double v1, const int nv, const int lane) {
+  const bool ok = (lane >= nv || isfinite(v0)) && (lane + 32 >= nv || isfinite(v1));
+  return __all_sync(kFull, ok);
+}
+
+#define TNG_ZLOOP(j) _Pragma("unroll") for (int j = 0; j <= kQmax + 1; ++j)
+
+__device__ __forceinline__ void z_predict(double (&z)[kQmax + 2][2], const int q) {
+#pragma unroll
+  for (int k = 0; k < kQmax; ++k) {
+    if (k < q) {
+#pragma unroll
+      for (int j = kQmax; j > 0; --j)
+        if (j > k && j <= q) {
+          z[j - 1][0] += z[j][0];
+          z[j - 1][1] += z[j][1];
+        }
+    }
+  }
+}
+
+__device__ __forceinline__ void z_retract(double (&z)[kQmax + 2][2], const int q) {
+#pragma unroll
+  for (int k = kQmax - 1; k >= 0; --k) {
+    if (k < q) {
+#pragma unroll
+      for (int j = 1; j <= kQmax; ++j)
+        if (j > k && j <= q) {
+          z[j - 1][0] -= z[j][0];
+          z[j - 1][1] -= z[j][1];
+        }
+    }
+  }
+}
+
+__device__ __forceinline__ void z_rescale(double (&z)[kQmax + 2][2], const int q, const double eta) {
+  double f = 1.0;
+#pragma unroll
+  for (int j = 1; j <= kQmax + 1; ++j) {
+    f *= eta;
+    if (j <= q) {
+      z[j][0] *= f;
+      z[j][1] *= f;
+    }
+  }
+}
+
+__device__ __forceinline__ double zget(const double (&z)[kQmax + 2][2], const int j, const int h) {
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k <= kQmax + 1; ++k)
+    if (k == j) v = z[k][h];
+  return v;
+}
+
+__device__ __forceinline__ void zset(double (&z)[kQmax + 2][2], const int j, const int h, const double v) {
+#pragma unroll
+  for (int k = 0; k <= kQmax + 1; ++k)
+    if (k == j) z[k][h] = v;
+}
+
+// Integrate one cell (warp-cooperative). Returns true when the cell is finished (any status),
+// false when it used up the pass budget and was saved for the next pass.
+__device__ bool bdf_cell(const BdfLaunch& P, const WarpMem& w, const int cell, const int lane) {
+  const BdfArgs& a = P.a;
+  const BdfCoef& C = P.c;
+  const SvDev& t = a.tab;
+  const int ns = t.L.size[SZ_NS], nv = ns + 1, rs = a.rs;
+  const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
+  const double p = a.p, rtol = a.rtol, atol = a.atol;
+  const bool h0 = lane < nv, h1 = lane + 32 < nv;
+  double z[kQmax + 2][2];
+  double acorp[2] = {0.0, 0.0}, ewt[2] = {0.0, 0.0}, acor[2], y[2], f[2], x[2];
+  TNG_ZLOOP(j) { z[j][0] = 0.0; z[j][1] = 0.0; }
+  double tcur = 0.0, h = 0.0, hprev = 0.0, crate = 1.0, etamax = 1e4, gamma_lu = 0.0;
+  int q = 1, qwait = 2, qprev = 0, need_j = 1, nst_lu = 0, nst = 0, nni = 0, nje = 0, status = ST_OK;
+  double* sv = a.save ? a.save + (long long)cell * a.save_stride : nullptr;
+  const bool resume = a.resume && a.resume[cell];
+  if (resume) {
+    TNG_ZLOOP(j) {
+      if (j <= kQmax) {
+        z[j][0] = h0 ? sv[j * nv + lane] : 0.0;
+        z[j][1] = h1 ? sv[j * nv + lane + 32] : 0.0;
+      }
+    }
+    acorp[0] = h0 ? sv[(kQmax + 1) * nv + lane] : 0.0;
+    acorp[1] = h1 ? sv[(kQmax + 1) * nv + lane + 32] : 0.0;
+    const double* s = sv + (kQmax + 2) * nv;
+    tcur = s[0], h = s[1], hprev = s[2], crate = s[3], etamax = s[4];
+    q = (int)s[5], qwait = (int)s[6], qprev = (int)s[7], nst = (int)s[8], nni = (int)s[9], nje = (int)s[10];
+    need_j = 1;
+    nst_lu = nst;
+    ewt[0] = h0 ? 1.0 / (rtol * fabs(z[0][0]) + atol) : 0.0;
+    ewt[1] = h1 ? 1.0 / (rtol * fabs(z[0][1]) + atol) : 0.0;
+  } else {
+    const long long ld = a.ld;
+    const double u0 = h0 ? a.state[(long long)lane * ld + cell] : 0.0;
+    const double u1 = h1 ? a.state[(long long)(lane + 32) * ld + cell] : 0.0;
+    z[0][0] = u0;
+    z[0][1] = u1;
+    if (!(dt > 0.0)) goto finish;
+    ewt[0] = h0 ? 1.0 / (rtol * fabs(u0) + atol) : 0.0;
+    ewt[1] = h1 ? 1.0 / (rtol * fabs(u1) + atol) : 0.0;
+    rhs_warp(t, w, u0, u1, p, f[0], f[1], lane);
+    if (!warp_all_finite(f[0], f[1], nv, lane)) {
+      status = ST_NONFINITE;
+      goto finish;
+    }
+    // initial step from an estimate of ||y''||
+    {
+      const double hlb = 100.0 * 2.220446049250313e-16 * dt;
+      double hub = 0.1 * dt;
+      double r = 0.0;
+      if (h0) r = fabs(f[0]) / (0.1 * fabs(u0) + atol);
+      if (h1) r = fmax(r, fabs(f[1]) / (0.1 * fabs(u1) + atol));
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(kFull, r, off));
+      if (hub * r > 1.0) hub = 1.0 / r;
+      double hg = sqrt(hlb * hub), hnew = hg;
+      if (hub < hlb) {
+        hnew = hlb;
+      } else {
+        for (int it = 0; it < 4; ++it) {
+          double g0, g1;
+          rhs_warp(t, w, u0 + hg * f[0], u1 + hg * f[1], p, g0, g1, lane);
+          const double ydd = wrms2((g0 - f[0]) / hg, (g1 - f[1]) / hg, ewt[0], ewt[1], nv, lane);
+          hnew = (ydd * hub * hub > 2.0) ? sqrt(2.0 / ydd) : sqrt(hg * hub);
+          if (!isfinite(hnew)) hnew = hg;
+          const double hrat = hnew / hg;
+          if (it == 3 || (hrat > 0.5 && hrat < 2.0)) break;
+          hg = hnew;
+        }
+        hnew *= 0.5;
+        if (hnew < hlb) hnew = hlb;
+        if (hnew > hub) hnew = hub;
+      }
+      h = hnew < dt ? hnew : dt;
+    }
+    z[1][0] = h * f[0];
+    z[1][1] = h * f[1];
+    hprev = h;
+  }
+  {
+    const double hlb = 100.0 * 2.220446049250313e-16 * dt;
+    const int maxcor = a.maxcor > 0 ? a.maxcor : 3;
+    const int msbp = a.msbp > 0 ? a.msbp : 20;
+    const double dgmax = a.dgmax > 0.0 ? a.dgmax : 0.3;
+    int pass_steps = 0;
+    while (tcur < dt) {
+      if (nst >= a.max_steps) {
+        status = ST_MAXSTEPS;
+        break;
+      }
+      if (pass_steps >= a.budget) {
+        // save the history for the next pass and queue the cell again
+        TNG_ZLOOP(j) {
+          if (j <= kQmax) {
+            if (h0) sv[j * nv + lane] = z[j][0];
+            if (h1) sv[j * nv + lane + 32] = z[j][1];
+          }
+        }
+        if (h0) sv[(kQmax + 1) * nv + lane] = acorp[0];
+        if (h1) sv[(kQmax + 1) * nv + lane + 32] = acorp[1];
+        if (lane == 0) {
+          double* s = sv + (kQmax + 2) * nv;
+          s[0] = tcur, s[1] = h, s[2] = hprev, s[3] = crate, s[4] = etamax;
+          s[5] = q, s[6] = qwait, s[7] = qprev, s[8] = nst, s[9] = nni, s[10] = nje;
+          a.resume[cell] = 1;
+          const int slot = atomicAdd(a.n_out, 1);
+          a.queue_out[slot] = cell;
+        }
+        __syncwarp();
+        return false;
+      }
+      if (tcur + h > dt) {
+        const double eta = (dt - tcur) / h;
+        z_rescale(z, q, eta);
+        h = dt - tcur;
+      }
+      int ncf = 0, nef = 0;
+      double dsm = 0.0;
+      bool fail = false;
+      for (;;) {  // attempt the step
+        if (h < hlb * 1e-3 || !isfinite(h)) {
+          status = ST_HMIN;
+          fail = true;
+          break;
+        }
+        z_predict(z, q);
+        const double l0 = C.L[q][0];
+        const double gamma = h * l0;
+        bool conv_fail = false;
+        bool jcur = false;
+        if (need_j || nst >= nst_lu + msbp || fabs(gamma / gamma_lu - 1.0) > dgmax) {
+          rhs_warp(t, w, z[0][0], z[0][1], p, f[0], f[1], lane);
+          jac_warp(t, w, rs, z[0][0], z[0][1], f[0], f[1], p, lane);
+          ++nje;
+          for (int e = lane; e < nv * rs; e += 32) w.mat[e] = -gamma * w.mat[e];
+          __syncwarp();
+          for (int i = lane; i < nv; i += 32) w.mat[i * rs + i] += 1.0;
+          __syncwarp();
+          const int sing = lu_warp(w.mat, nv, rs, w.piv, lane);
+          gamma_lu = gamma;
+          nst_lu = nst;
+          jcur = true;
+          need_j = 0;
+          crate = 1.0;
+          if (sing) conv_fail = true;
+        }
+        if (!conv_fail) {
+          double delp = 0.0;
+          acor[0] = acor[1] = 0.0;
+          y[0] = z[0][0];
+          y[1] = z[0][1];
+          conv_fail = true;
+          for (int it = 0; it < maxcor; ++it) {
+            rhs_warp(t, w, y[0], y[1], p, f[0], f[1], lane);
+            ++nni;
+            x[0] = h * f[0] - z[1][0] - acor[0];
+            x[1] = h * f[1] - z[1][1] - acor[1];
+            if (h0) w.vb[lane] = x[0];
+            if (h1) w.vb[lane + 32] = x[1];
+            __syncwarp();
+            lu_solve_warp(w.mat, nv, rs, w.piv, w.vb, lane);
+            x[0] = h0 ? w.vb[lane] : 0.0;
+            x[1] = h1 ? w.vb[lane + 32] : 0.0;
+            __syncwarp();
+            if (gamma != gamma_lu) {
+              const double cf = 2.0 / (1.0 + gamma / gamma_lu);
+              x[0] *= cf;
+              x[1] *= cf;
+            }
+            acor[0] += x[0];
+            acor[1] += x[1];
+            y[0] = z[0][0] + l0 * acor[0];
+            y[1] = z[0][1] + l0 * acor[1];
+            const double del = wrms2(x[0], x[1], ewt[0], ewt[1], nv, lane);
+            if (!isfinite(del)) break;
+            if (it > 0) crate = fmax(0.3 * crate, del / delp);
+            const double dcon = del * fmin(1.0, crate) * C.errc[q] / 0.1;
+            if (dcon <= 1.0) {
+              conv_fail = false;
+              break;
+            }
+            if (it > 0 && del > 2.0 * delp) break;
+            delp = del;
+          }
+        }
+        if (conv_fail) {
+          z_retract(z, q);
+          ++ncf;
+          if (ncf >= 10) {
+            status = ST_CONVFAIL;
+            fail = true;
+            break;
+          }
+          if (!jcur) {
+            need_j = 1;
+            continue;
+          }
+          z_rescale(z, q, 0.25);
+          h *= 0.25;
+          need_j = 1;
+          continue;
+        }
+        dsm = C.errc[q] * wrms2(acor[0], acor[1], ewt[0], ewt[1], nv, lane);
+        if (dsm > 1.0) {
+          z_retract(z, q);
+          ++nef;
+          if (nef >= 7) {
+            status = ST_ERRFAIL;
+            fail = true;
+            break;
+          }
+          if (nef >= 3 && q > 1) {
+            h *= 0.1;
+            q = 1;
+            rhs_warp(t, w, z[0][0], z[0][1], p, f[0], f[1], lane);
+            z[1][0] = h * f[0];
+            z[1][1] = h * f[1];
+            qwait = 2;
+            qprev = 0;
+            continue;
+          }
+          double eta = 1.0 / (pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+          eta = fmax(0.1, fmin(0.9, eta));
+          if (nef >= 2) eta = fmin(eta, 0.2);
+          z_rescale(z, q, eta);
+          h *= eta;
+          continue;
+        }
+        break;
+      }
+      if (fail) break;
+      // accept
+      tcur += h;
+      ++nst;
+      ++pass_steps;
+#pragma unroll
+      for (int j = 0; j <= kQmax; ++j)
+        if (j <= q) {
+          z[j][0] += C.L[q][j] * acor[0];
+          z[j][1] += C.L[q][j] * acor[1];
+        }
+      if (!warp_all_finite(z[0][0], z[0][1], nv, lane)) {
+        status = ST_NONFINITE;
+        break;
+      }
+      ewt[0] = h0 ? 1.0 / (rtol * fabs(z[0][0]) + atol) : 0.0;
+      ewt[1] = h1 ? 1.0 / (rtol * fabs(z[0][1]) + atol) : 0.0;
+      if (tcur >= dt) break;
+      --qwait;
+      const double eta_q = 1.0 / (pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+      double eta_m = 0.0, eta_p = 0.0;
+      if (qwait <= 0) {
+        if (q > 1) {
+          const double ddn = C.dnc[q] * wrms2(zget(z, q, 0), zget(z, q, 1), ewt[0], ewt[1], nv, lane);
+          eta_m = 1.0 / (pow(6.0 * ddn, 1.0 / q) + 1e-6);
+        }
+        if (q < kQmax && qprev == q) {
+          const double r = pow(h / hprev, q + 1);
+          const double dup =
+              C.upc[q] * wrms2(acor[0] - r * acorp[0], acor[1] - r * acorp[1], ewt[0], ewt[1], nv, lane);
+          eta_p = 1.0 / (pow(10.0 * dup, 1.0 / (q + 2)) + 1e-6);
+        }
+      }
+      double eta = eta_q;
+      int newq = q;
+      if (eta_m > eta) {
+        eta = eta_m;
+        newq = q - 1;
+      }
+      if (eta_p > eta) {
+        eta = eta_p;
+        newq = q + 1;
+      }
+      if (eta < 1.5) {
+        eta = 1.0;
+        newq = q;
+      } else if (eta > etamax) {
+        eta = etamax;
+      }
+      etamax = 10.0;
+      acorp[0] = acor[0];
+      acorp[1] = acor[1];
+      qprev = q;
+      hprev = h;
+      if (newq == q + 1) {
+        const double c = C.L[q][q] / (q + 1);
+        zset(z, q + 1, 0, c * acor[0]);
+        zset(z, q + 1, 1, c * acor[1]);
+        q = q + 1;
+        qprev = 0;
+      } else if (newq == q - 1) {
+        q = q - 1;
+        qprev = 0;
+      }
+      if (eta != 1.0 || qprev == 0)
+        qwait = q + 1;
+      else if (qwait <= 0)
+        qwait = 2;
+      if (eta != 1.0) {
+        z_rescale(z, q, eta);
+        h *= eta;
+      }
+    }
+  }
+finish:
+  {
+    const long long ld = a.ld;
+    if (h0) a.state[(long long)lane * ld + cell] = z[0][0];
+    if (h1) a.state[(long long)(lane + 32) * ld + cell] = z[0][1];
+    if (lane == 0) {
+      if (a.nst) a.nst[cell] = nst;
+      if (a.nni) a.nni[cell] = nni;
+      if (a.nje) a.nje[cell] = nje;
+      if (a.status) a.status[cell] = status;
+      if (a.resume) a.resume[cell] = 0;
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_bdf(const BdfLaunch P) {
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpMem w = warp_mem(smem + (size_t)warp * P.a.smem_warp, P.a.tab.L, P.a.rs);
+  const int n_in = P.n_in_dev ? *P.n_in_dev : P.a.n_in;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(P.a.head, 1);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= n_in) break;
+    const int cell = P.a.queue_in ? P.a.queue_in[idx] : idx;
+    bdf_cell(P, w, cell, lane);
+  }
+}
+
+// Standalone right-hand side / Jacobian of the table-driven warp path (parity checks).
+template <int WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
+    k_warp_rhs_jac(SvDev t, const double* __restrict__ state, long long ld, int n, double p, double* __restrict__ rhs,
+                   double* __restrict__ jac, int rs, int smem_warp) {
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const WarpMem w = warp_mem(smem + (size_t)warp * smem_warp, t.L, rs);
+  const int nv = t.L.size[SZ_NV];
+  for (int cell = blockIdx.x * WARPS + warp; cell < n; cell += gridDim.x * WARPS) {
+    const double y0 = lane < nv ? state[(long long)lane * ld + cell] : 0.0;
+    const double y1 = lane + 32 < nv ? state[(long long)(lane + 32) * ld + cell] : 0.0;
+    double f0, f1;
+    rhs_warp(t, w, y0, y1, p, f0, f1, lane);
+    if (lane < nv) rhs[(long long)lane * ld + cell] = f0;
+    if (lane + 32 < nv) rhs[(long long)(lane + 32) * ld + cell] = f1;
+    if (jac) {
+      jac_warp(t, w, rs, y0, y1, f0, f1, p, lane);
+      for (int e = lane; e < nv * nv; e += 32) jac[(long long)cell * nv * nv + e] = w.mat[(e / nv) * rs + e % nv];
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void k_reset_counters(int* a, int* b) {
+  if (threadIdx.x == 0) {
+    *a = 0;
+    if (b) *b = 0;
+  }
+}
+
+}  // namespace tng

@@ -57,6 +57,9 @@ void tng_default_cfg(tng_cfg* cfg) {
   cfg->max_newton = 4;
   cfg->block_size = 0;
   cfg->rate_variant = -1;
+  cfg->solver_warps = 0;
+  cfg->pass_budget = 0;
+  cfg->max_passes = 8;
 }
 
 int tng_last_error(char* buf, int len) {
@@ -118,6 +121,7 @@ int tng_chem_destroy(tng_chem* h) {
   {
     DeviceGuard g(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    solver_release(h);
     for (auto& b : h->bufs) b.release();
     for (int i = 0; i < 2; ++i)
       if (h->copy_stream[i]) cudaStreamDestroy(h->copy_stream[i]);

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "solver_layout.h"
 #include "tng_device.cuh"
 
 namespace tng {
@@ -59,6 +60,10 @@ struct MechOps {
   // rate evaluation: prec 0/1, lm 0/1; dump may be null
   cudaError_t (*rhs)(int prec, int lm, int variant, const double* sol, double* out, double* dump, long long n,
                      long long ld, double p, int block, cudaStream_t st);
+  // tables of the implicit solver
+  const SvLayout* sv_layout;
+  const int* sv_int;
+  const double* sv_dbl[2];
 };
 
 // Kernel variants of the rate evaluation (the autotuner's choices): 0 = plain, 1 = block

@@ -6,7 +6,7 @@ namespace tng {
 
 template <class Mech>
 MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int nelem, const char* const* elements,
-                 const double* elem) {
+                 const double* elem, const SvLayout* svl, const int* svi, const double* svd0, const double* svd1) {
   MechOps o{};
   o.name = Mech::NAME;
   o.ns = Mech::NS;
@@ -19,6 +19,10 @@ MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int
   o.elements = elements;
   o.elem = elem;
   o.rhs = &launch_rhs<Mech>;
+  o.sv_layout = svl;
+  o.sv_int = svi;
+  o.sv_dbl[0] = svd0;
+  o.sv_dbl[1] = svd1;
   return o;
 }
 

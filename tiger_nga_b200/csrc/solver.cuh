@@ -1,0 +1,495 @@
+// K3: the implicit chemistry substep on sm_100a, one cell per warp.
+//
+// Replaces finitechem_source_chemistry's per-cell CVODE call (combustion/finitechem.f90:
+// 962-1071): variable-order (1..5), variable-step BDF in Nordsieck form with modified Newton on
+// M = I - gamma J and a dense FP64 LU with partial pivoting, stopping exactly at dt. The
+// algorithm is restated in oracle/solver_oracle.c (the CPU twin used by the tests).
+//
+// Execution model (B200):
+//  * a warp owns one cell; every vector of length NV = N+1 lives in registers, two entries per
+//    lane (index lane and lane+32), so predictor, corrector update and WRMS norms are register
+//    work plus one warp reduction;
+//  * the right-hand side is table-driven and lane-parallel over the mechanism's reaction slots
+//    (rates W_r into shared memory), production rates gathered from balanced per-lane chunk
+//    lists (no atomics: results are deterministic);
+//  * the Jacobian is assembled in shared memory (analytic mass-action and third-body/falloff-[M]
+//    columns, forward-difference temperature column, temperature row from the species rows);
+//    M = I - gamma J is factored in place by the warp (shuffle arg-max pivoting, 4x8 lane tiles
+//    for the trailing update);
+//  * a persistent grid steals cells from a queue; a cell that exhausts the pass's step budget
+//    saves its Nordsieck history and goes to the next pass's queue (recompaction), so a pass
+//    never runs longer than the budget allows and the host loop over passes is a CUDA graph.
+// No wait in this kernel depends on another warp or block: work is claimed with atomics only.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "solver_layout.h"
+
+namespace tng {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kQmax = 5;
+
+struct SvDev {
+  const int* __restrict__ I;
+  const double* __restrict__ D;
+  SvLayout L;
+  __device__ __forceinline__ const int* ip(int k) const { return I + L.ioff[k]; }
+  __device__ __forceinline__ const double* dp(int k) const { return D + L.doff[k]; }
+};
+
+// status codes per cell
+enum { ST_OK = 0, ST_MAXSTEPS = 1, ST_CONVFAIL = 2, ST_ERRFAIL = 3, ST_NONFINITE = 4, ST_HMIN = 5, ST_PENDING = 9 };
+
+struct BdfArgs {
+  SvDev tab;
+  double* state;     // species-major [v*ld + cell], in/out
+  long long ld;
+  const double* dts;  // per-cell dt or null
+  double dt_scalar;
+  double p;
+  const int* queue_in;  // cells of this pass (null: 0..n_in-1)
+  int n_in;
+  int* head;        // work-stealing counter
+  int* queue_out;   // cells that did not finish within the budget
+  int* n_out;
+  double* save;     // per-cell saved integrator state (save_stride doubles per cell)
+  int save_stride;
+  int* resume;      // per cell: 1 = integrator state in save
+  int budget;       // internal steps per cell and pass
+  double rtol, atol, dgmax;
+  int max_steps, maxcor, msbp;
+  int* nst;         // per-cell counters (accumulated over passes)
+  int* nni;
+  int* nje;
+  int* status;
+  int smem_warp;    // doubles of shared memory per warp
+  int rs;           // row stride of the matrix
+};
+
+// shared-memory regions of one warp (offsets in doubles)
+struct WarpMem {
+  double* mat;  // NV x rs
+  double* W;    // nslot: rates (RHS) or rate constants (Jacobian)
+  double* C;    // 64 concentrations
+  double* Ms;   // nm third-body sums
+  double* lcm;  // nm log concentration for falloff
+  double* fc;   // nfc x 3 (ln Fc, Troe N, Troe C)
+  double* part; // ncdchunk partial production rates
+  double* G;    // ngpair
+  double* vb;   // 64 vector buffer
+  double* hb;   // 64 enthalpies / heat capacities scratch
+  double* cb;   // 64
+  int* piv;     // 64 pivots
+};
+
+__host__ __device__ inline int warp_mem_doubles(const SvLayout& L, int rs) {
+  const int nv = L.size[SZ_NV];
+  return nv * rs + L.size[SZ_NSLOT] + 64 + 2 * L.size[SZ_NM] + 3 * L.size[SZ_NFC] + L.size[SZ_NCDCHUNK] +
+         L.size[SZ_NGPAIR] + 3 * 64 + 32 /* pivots as ints */ + 8;
+}
+
+__device__ __forceinline__ WarpMem warp_mem(double* base, const SvLayout& L, int rs) {
+  WarpMem w;
+  const int nv = L.size[SZ_NV];
+  double* p = base;
+  w.mat = p; p += nv * rs;
+  w.W = p; p += L.size[SZ_NSLOT];
+  w.C = p; p += 64;
+  w.Ms = p; p += L.size[SZ_NM];
+  w.lcm = p; p += L.size[SZ_NM];
+  w.fc = p; p += 3 * L.size[SZ_NFC];
+  w.part = p; p += L.size[SZ_NCDCHUNK];
+  w.G = p; p += L.size[SZ_NGPAIR];
+  w.vb = p; p += 64;
+  w.hb = p; p += 64;
+  w.cb = p; p += 64;
+  w.piv = reinterpret_cast<int*>(p);
+  return w;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(kFull, v, off);
+  return __shfl_sync(kFull, v, 0);
+}
+
+__device__ __forceinline__ double expo(const double lnA, const double n, const double E, const int fl, const double LT,
+                                       const double invRT) {
+  double e = lnA;
+  if (fl & 4) e = fma(E, invRT, e);
+  if (fl & 2) e = fma(n, LT, e);
+  return e;
+}
+
+// Per-cell thermochemical state shared by the rate and Jacobian evaluations.
+struct CellPrep {
+  double rho, T, LT, invRT, invT, irho;
+};
+
+// Stage the state (two entries per lane) and fill C, third-body sums, falloff [M] logs and the
+// F_cent terms in shared memory.
+__device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+                                           const double p, const int lane) {
+  const int ns = t.L.size[SZ_NS], nv = ns + 1, nm = t.L.size[SZ_NM], nfc = t.L.size[SZ_NFC];
+  const double* sc = t.dp(D_SCAL);
+  const double* invw = t.dp(D_INVW);
+  if (lane < nv) w.vb[lane] = y0;
+  if (lane + 32 < nv) w.vb[lane + 32] = y1;
+  CellPrep c;
+  c.rho = warp_sum((lane < ns ? y0 : 0.0) + (lane + 32 < ns ? y1 : 0.0));
+  __syncwarp();
+  c.irho = 1.0 / c.rho;
+  c.T = w.vb[ns] / c.rho;  // by division, as the reference (the T > 1000 range switch is strict)
+  c.LT = log(c.T);
+  c.invRT = 1.0 / (sc[SC_RGAS] * c.T);
+  c.invT = sc[SC_RGAS] * c.invRT;
+  if (lane < ns) w.C[lane] = y0 * invw[lane];
+  if (lane + 32 < ns) w.C[lane + 32] = y1 * invw[lane + 32];
+  __syncwarp();
+  const double lnprt = log(p * c.invRT);
+  const int* tbp = t.ip(I_TB_PTR);
+  const int* tbs = t.ip(I_TB_SP);
+  const double* tbc = t.dp(D_TB_COEF);
+  for (int m = lane; m < nm; m += 32) {
+    const int b = tbp[m], e = tbp[m + 1];
+    double acc = tbc[b] == 1.0 ? w.C[tbs[b]] : tbc[b] * w.C[tbs[b]];
+    for (int q = b + 1; q < e; ++q) acc = tbc[q] == 1.0 ? acc + w.C[tbs[q]] : fma(tbc[q], w.C[tbs[q]], acc);
+    w.Ms[m] = acc;
+    w.lcm[m] = acc > 0.0 ? log(acc) : lnprt;
+  }
+  const int* fcf = t.ip(I_FC_FORM);
+  const double* fca = t.dp(D_FC_A);
+  const double* fcc = t.dp(D_FC_C);
+  for (int f = lane; f < nfc; f += 32) {
+    double v = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      const int form = fcf[3 * f + q];
+      if (form < 0) break;
+      const double a = fca[3 * f + q], cc = fcc[3 * f + q];
+      const double term = form == 2 ? a : (form == 0 ? a * exp(-c.T * cc) : a * exp(-cc * c.invT));
+      v = q == 0 ? term : v + term;
+    }
+    const double lfc = log(v);
+    const double l10 = lfc * sc[SC_INVLN10];
+    w.fc[3 * f] = lfc;
+    w.fc[3 * f + 1] = sc[SC_TN0] - sc[SC_TN1] * l10;
+    w.fc[3 * f + 2] = -sc[SC_TC0] - sc[SC_TC1] * l10;
+  }
+  __syncwarp();
+  return c;
+}
+
+// Rate constant of slot r (GETLINDRATECOEFF-equivalent for falloff slots); also returns ln Pr.
+__device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, const CellPrep& c, const int r,
+                                            double* lpr_out) {
+  const int fl = t.ip(I_SLOT_FLAGS)[r];
+  if (fl & 1) {
+    const int f = t.ip(I_SLOT_FO)[r];
+    const double* par = t.dp(D_FO_PAR) + 6 * f;
+    const int* ffl = t.ip(I_FO_FLAGS) + 2 * f;
+    const double* sc = t.dp(D_SCAL);
+    const double lk0 = expo(par[0], par[1], par[2], ffl[0], c.LT, c.invRT);
+    const double lki = expo(par[3], par[4], par[5], ffl[1], c.LT, c.invRT);
+    const double lpr = lk0 + w.lcm[t.ip(I_FO_M)[f]] - fmax(lki, sc[SC_LNKMIN]);
+    if (lpr_out) *lpr_out = lpr;
+    const double pr = exp(lpr);
+    const int fid = t.ip(I_FO_FC)[f];
+    if (fid < 0) return exp(lki) * pr / (1.0 + pr);
+    const double lg = lpr * sc[SC_INVLN10] + w.fc[3 * fid + 2];
+    const double ff = lg / (w.fc[3 * fid + 1] - sc[SC_TD] * lg);
+    return exp(lki + w.fc[3 * fid] / (ff * ff + 1.0)) * pr / (1.0 + pr);
+  }
+  if (fl & 8) return t.dp(D_SLOT_A)[r];
+  return exp(expo(t.dp(D_SLOT_LNA)[r], t.dp(D_SLOT_N)[r], t.dp(D_SLOT_E)[r], fl, c.LT, c.invRT));
+}
+
+// finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
+__device__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, const double y1, const double p,
+                         double& f0, double& f1, const int lane) {
+  const int ns = t.L.size[SZ_NS], nslot = t.L.size[SZ_NSLOT];
+  const CellPrep c = prepare(t, w, y0, y1, p, lane);
+  const int* reac = t.ip(I_SLOT_REAC);
+  const int* mw = t.ip(I_SLOT_MW);
+  for (int r = lane; r < nslot; r += 32) {
+    double v = rate_const(t, w, c, r, nullptr);
+    const int* rr = reac + 3 * r;
+    if (rr[0] >= 0) v = v * w.C[rr[0]];
+    if (rr[1] >= 0) v = v * w.C[rr[1]];
+    if (rr[2] >= 0) v = v * w.C[rr[2]];
+    if (mw[r] >= 0) v = v * w.Ms[mw[r]];
+    w.W[r] = v;
+  }
+  __syncwarp();
+  {
+    const int* lp = t.ip(I_CD_LANE_PTR);
+    const int* ll = t.ip(I_CD_LANE_LIST);
+    const int* cb = t.ip(I_CD_CHUNK_BEG);
+    const int* ce = t.ip(I_CD_CHUNK_END);
+    const int* cs = t.ip(I_CD_SLOT);
+    const double* cn = t.dp(D_CD_NU);
+    for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
+      const int ch = ll[i];
+      double acc = 0.0;
+      for (int q = cb[ch]; q < ce[ch]; ++q) {
+        const double nu = cn[q], wv = w.W[cs[q]];
+        acc = nu == 1.0 ? acc + wv : (nu == -1.0 ? acc - wv : fma(nu, wv, acc));
+      }
+      w.part[ch] = acc;
+    }
+  }
+  __syncwarp();
+  const int* spp = t.ip(I_CD_SP_PTR);
+  const double* wm = t.dp(D_WMOL);
+  const double* sc = t.dp(D_SCAL);
+  const double* th = c.T > sc[SC_TMID] ? t.dp(D_TH_HI) : t.dp(D_TH_LO);
+  double cpm = 0.0, tmp = 0.0, r0 = 0.0, r1 = 0.0;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const int k = lane + 32 * half;
+    if (k < ns) {
+      double cd = 0.0;
+      for (int q = spp[k]; q < spp[k + 1]; ++q) cd += w.part[q];
+      const double* a = th + 12 * k;
+      const double T = c.T;
+      const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
+      const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
+      const double rk = cd * wm[k];
+      const double y = w.C[k] * (wm[k] * c.irho);
+      cpm = fma(y, cpk, cpm);
+      tmp = fma(-hk, rk, tmp);
+      if (half == 0) r0 = rk; else r1 = rk;
+    }
+  }
+  cpm = warp_sum(cpm);
+  tmp = warp_sum(tmp);
+  const double rT = tmp / cpm;
+  f0 = lane < ns ? r0 : (lane == ns ? rT : 0.0);
+  f1 = lane + 32 < ns ? r1 : (lane + 32 == ns ? rT : 0.0);
+  __syncwarp();
+}
+
+// Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
+// row stride rs). Uses one extra right-hand side for the temperature column.
+__device__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const double y0, const double y1,
+                         const double f0, const double f1, const double p, const int lane) {
+  const int ns = t.L.size[SZ_NS], nv = ns + 1, nslot = t.L.size[SZ_NSLOT];
+  const CellPrep c = prepare(t, w, y0, y1, p, lane);
+  const int* reac = t.ip(I_SLOT_REAC);
+  const int* mw = t.ip(I_SLOT_MW);
+  for (int r = lane; r < nslot; r += 32) w.W[r] = rate_const(t, w, c, r, nullptr);
+  for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
+  __syncwarp();
+  // direct mass-action part: dW_r/dC_j for every reactant occurrence
+  {
+    const int* lp = t.ip(I_JD_LANE_PTR);
+    const int* ll = t.ip(I_JD_LANE_LIST);
+    const int* tg = t.ip(I_JD_TGT);
+    const int* gb = t.ip(I_JD_BEG);
+    const int* ge = t.ip(I_JD_END);
+    const int* js = t.ip(I_JD_SLOT);
+    const int* jp = t.ip(I_JD_POS);
+    const double* jn = t.dp(D_JD_NU);
+    for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
+      const int g = ll[i];
+      double acc = 0.0;
+      for (int q = gb[g]; q < ge[g]; ++q) {
+        const int r = js[q], pos = jp[q];
+        double d = w.W[r];
+        if (mw[r] >= 0) d *= w.Ms[mw[r]];
+        const int* rr = reac + 3 * r;
+#pragma unroll
+        for (int o = 0; o < 3; ++o)
+          if (o != pos && rr[o] >= 0) d *= w.C[rr[o]];
+        acc = fma(jn[q], d, acc);
+      }
+      const int tgt = tg[g];
+      w.mat[(tgt / nv) * rs + tgt % nv] = acc;
+    }
+  }
+  // third-body and falloff-[M] part: G[i][m] = sum_r nu_ir dW_r/dM_m
+  {
+    const int* lp = t.ip(I_G_LANE_PTR);
+    const int* ll = t.ip(I_G_LANE_LIST);
+    const int* gb = t.ip(I_G_BEG);
+    const int* ge = t.ip(I_G_END);
+    const int* gs = t.ip(I_G_SLOT);
+    const int* gk = t.ip(I_G_KIND);
+    const double* gn = t.dp(D_G_NU);
+    for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
+      const int g = ll[i];
+      double acc = 0.0;
+      for (int q = gb[g]; q < ge[g]; ++q) {
+        const int r = gs[q];
+        const int* rr = reac + 3 * r;
+        double prodC = 1.0;
+#pragma unroll
+        for (int o = 0; o < 3; ++o)
+          if (rr[o] >= 0) prodC *= w.C[rr[o]];
+        double val = 0.0;
+        if (gk[q] == 0) {
+          val = w.W[r] * prodC;
+        } else {
+          const int f = t.ip(I_SLOT_FO)[r];
+          const double Mf = w.Ms[t.ip(I_FO_M)[f]];
+          if (Mf > 0.0) {
+            double lpr;
+            rate_const(t, w, c, r, &lpr);
+            const double pr = exp(lpr);
+            val = w.W[r] / (Mf * (1.0 + pr)) * prodC * (mw[r] >= 0 ? w.Ms[mw[r]] : 1.0);
+          }
+        }
+        acc = fma(gn[q], val, acc);
+      }
+      w.G[g] = acc;
+    }
+  }
+  __syncwarp();
+  {
+    const int ng = t.L.size[SZ_NGPAIR];
+    const int* gi = t.ip(I_G_I);
+    const int* gm = t.ip(I_G_M);
+    const double* eff = t.dp(D_EFF);
+    for (int j = lane; j < ns; j += 32)
+      for (int g = 0; g < ng; ++g) {
+        const double v = w.G[g];
+        if (v != 0.0) w.mat[gi[g] * rs + j] = fma(v, eff[gm[g] * ns + j], w.mat[gi[g] * rs + j]);
+      }
+  }
+  __syncwarp();
+  // temperature column: forward difference (one right-hand side)
+  const double T = c.T, rho = c.rho;
+  const double yN = __shfl_sync(kFull, ns < 32 ? y0 : y1, ns & 31);
+  const double dlt = 1.4901161193847656e-08 * fmax(fabs(yN), 1e-30);
+  const double yNp = yN + dlt;
+  const double idl = 1.0 / (yNp - yN);
+  double g0, g1;
+  rhs_warp(t, w, lane == ns ? yNp : y0, lane + 32 == ns ? yNp : y1, p, g0, g1, lane);
+  if (lane < nv) w.mat[lane * rs + ns] = (g0 - f0) * idl;
+  if (lane + 32 < nv) w.mat[(lane + 32) * rs + ns] = (g1 - f1) * idl;
+  __syncwarp();
+  // species columns
+  const double* wm = t.dp(D_WMOL);
+  for (int e = lane; e < ns * ns; e += 32) {
+    const int i = e / ns, j = e % ns;
+    w.mat[i * rs + j] = wm[i] * w.mat[i * rs + j] / wm[j] - T * w.mat[i * rs + ns];
+  }
+  // temperature row
+  const double* sc = t.dp(D_SCAL);
+  const double* th = T > sc[SC_TMID] ? t.dp(D_TH_HI) : t.dp(D_TH_LO);
+  double cpm = 0.0, ydcp = 0.0, scp = 0.0;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const int k = lane + 32 * half;
+    if (k < ns) {
+      const double* a = th + 12 * k;
+      const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
+      const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
+      const double dcp = a[0] * (a[8] + T * (2.0 * a[9] + T * (3.0 * a[10] + T * (4.0 * a[11]))));
+      const double y = (half == 0 ? y0 : y1) / rho;
+      cpm += y * cpk;
+      ydcp += y * dcp;
+      scp += cpk * (half == 0 ? f0 : f1);
+      w.hb[k] = hk;
+      w.cb[k] = cpk;
+    }
+  }
+  cpm = warp_sum(cpm);
+  ydcp = warp_sum(ydcp);
+  scp = warp_sum(scp);
+  const double fT = __shfl_sync(kFull, ns < 32 ? f0 : f1, ns & 31);
+  __syncwarp();
+  const double dTdu = -T / rho;
+  for (int j = lane; j < ns; j += 32) {
+    double s = 0.0;
+    for (int k = 0; k < ns; ++k) s += w.hb[k] * w.mat[k * rs + j];
+    s += dTdu * scp;
+    const double dcpm = (w.cb[j] - cpm) / rho + dTdu * ydcp;
+    w.mat[ns * rs + j] = -(s + fT * dcpm) / cpm;
+  }
+  __syncwarp();
+}
+
+// In-place LU with partial pivoting (first maximum) of the n x n matrix a (row stride rs).
+// Returns nonzero if a pivot is zero or not finite.
+__device__ int lu_warp(double* a, const int n, const int rs, int* piv, const int lane) {
+  int sing = 0;
+  const int lr = lane >> 3, lc = lane & 7;
+  for (int k = 0; k < n; ++k) {
+    double best = -1.0;
+    int bi = n;
+    for (int i = k + lane; i < n; i += 32) {
+      const double v = fabs(a[i * rs + k]);
+      if (v > best || (v == best && i < bi)) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_down_sync(kFull, best, off);
+      const int oi = __shfl_down_sync(kFull, bi, off);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    bi = __shfl_sync(kFull, bi, 0);
+    if (bi >= n) {  // the column holds only NaNs
+      bi = k;
+      sing = 1;
+    }
+    if (lane == 0) piv[k] = bi;
+    if (bi != k)
+      for (int j = lane; j < n; j += 32) {
+        const double tmp = a[k * rs + j];
+        a[k * rs + j] = a[bi * rs + j];
+        a[bi * rs + j] = tmp;
+      }
+    __syncwarp();
+    const double d = a[k * rs + k];
+    if (d == 0.0 || !isfinite(d)) {
+      sing = 1;
+      continue;
+    }
+    for (int i = k + 1 + lane; i < n; i += 32) a[i * rs + k] = a[i * rs + k] / d;
+    __syncwarp();
+    for (int i = k + 1 + lr; i < n; i += 4) {
+      const double l = a[i * rs + k];
+      for (int j = k + 1 + lc; j < n; j += 8) a[i * rs + j] = fma(-l, a[k * rs + j], a[i * rs + j]);
+    }
+    __syncwarp();
+  }
+  return sing;
+}
+
+// Solve (LU) x = b in place; b in shared memory.
+__device__ void lu_solve_warp(const double* a, const int n, const int rs, const int* piv, double* b, const int lane) {
+  if (lane == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      if (p != k) {
+        const double tmp = b[k];
+        b[k] = b[p];
+        b[p] = tmp;
+      }
+    }
+  __syncwarp();
+  for (int k = 0; k < n; ++k) {
+    const double bk = b[k];
+    for (int i = k + 1 + lane; i < n; i += 32) b[i] = fma(-a[i * rs + k], bk, b[i]);
+    __syncwarp();
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double v = b[k];
+    __syncwarp();
+    const double bk = v / a[k * rs + k];
+    for (int i = lane; i < k; i += 32) b[i] = fma(-a[i * rs + k], bk, b[i]);
+    if (lane == 0) b[k] = bk;
+    __syncwarp();
+  }
+}
+
+}  // namespace tng

@@ -7,6 +7,8 @@
 #include "kernels.cuh"
 #include "tiger_chem.h"
 
+struct tng_chem;
+
 namespace tng {
 
 int set_error(int code, const char* fmt, ...);
@@ -50,6 +52,9 @@ struct DevBuf {
   }
 };
 
+struct SolverState;
+void solver_release(tng_chem* h);
+
 }  // namespace tng
 
 struct tng_chem {
@@ -59,4 +64,5 @@ struct tng_chem {
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream[2] = {nullptr, nullptr};
   tng::DevBuf bufs[8];
+  tng::SolverState* solver = nullptr;
 };

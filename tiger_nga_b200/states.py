@@ -44,6 +44,8 @@ def fourier_field(shape, seed: int, modes: int = 16, kmax: int = 4) -> np.ndarra
             + (2 * np.pi * k[2] * axes[2])[None, None, :]
         f += a * np.cos(arg + ph)
     lo, hi = f.min(), f.max()
+    if not hi > lo:
+        return np.full(shape, 0.5)
     return (f - lo) / (hi - lo)
 
 
