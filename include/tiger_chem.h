@@ -131,6 +131,86 @@ int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, co
 int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,
                        double* jac);
 
+/* ---- Surrogate network (no counterpart in the reference: the learned replacement of the
+ * substep for most cells). A multilayer perceptron x -> [Linear -> GELU] x layers -> Linear,
+ * trained on the device with hand-written FP32 forward/backward/Adam kernels. Inputs and
+ * outputs are row-major (rows x padded width), widths padded to multiples of 16 with zeros.
+ * Parameters are one flat float array [W_0 b_0 W_1 b_1 ...], W_l row-major (out x in). */
+typedef struct tng_mlp tng_mlp;
+int tng_mlp_create(tng_chem* h, int n_in, int n_out, int hidden, int layers, uint64_t seed, tng_mlp** out);
+int tng_mlp_destroy(tng_mlp* m);
+int64_t tng_mlp_param_count(const tng_mlp* m);
+/* which: 0 parameters, 1 last gradients, 2 / 3 Adam first / second moments */
+int tng_mlp_get_params(tng_mlp* m, float* host, int which);
+int tng_mlp_set_params(tng_mlp* m, const float* host);
+/* FP32 forward on the device: X (rows x in_pad) -> Y (rows x out_pad), device pointers */
+int tng_mlp_forward(tng_mlp* m, const float* X, int64_t rows, float* Y);
+/* forward + backward of the weighted mean squared error; gradients stay on the device
+ * (tng_mlp_get_params(which=1)), loss to *loss (host) when non-null */
+int tng_mlp_grad(tng_mlp* m, const float* X, const float* T, const float* w_out, int64_t rows, float* loss);
+int tng_mlp_adam_step(tng_mlp* m, float lr);
+/* minibatch training: epochs over n rows (shuffled per epoch), cosine learning-rate decay from
+ * lr; per-epoch loss (last minibatch) to losses[epochs] when non-null */
+int tng_mlp_train(tng_mlp* m, const float* X, const float* T, const float* w_out, int64_t n, int epochs, int batch,
+                  double lr, uint64_t seed, float* losses);
+
+/* ---- The substep through the surrogate, with fallback (no counterpart in the reference).
+ * The network maps (T, log P, log10 Y_k for every species but the bath gas, log10 dt) to the
+ * substep's (dT, dY_k). Its BF16 weights run on the tensor cores (FP32 accumulation); the
+ * prediction then gets an FP64 element-conservation projection, clipping and renormalisation
+ * of Y, and T from the enthalpy balance h(Y1, T1) = h(Y0, T0) (the low-Mach substep conserves
+ * enthalpy). A cell falls back to the implicit solve (tng_substep_batch's algorithm) when a
+ * feature lies outside the training range, when the network's dT disagrees with the
+ * enthalpy-implied dT, or when clipping removed too much mass. Every call also re-solves
+ * judge_cells sampled cells with the implicit solver and reports the surrogate's error. */
+typedef struct tng_surrogate_cfg {
+  int hidden;             /* width of the hidden layers (default 256) */
+  int layers;             /* hidden layers (default 4) */
+  uint64_t seed;          /* weight initialisation */
+  double ood_margin;      /* allowed excursion beyond the training range, fraction of the range (0.02) */
+  double consist_tol_K;   /* fallback when network and enthalpy temperatures differ by more (K, 5) */
+  double clip_tol;        /* fallback when clipping removed more mass fraction (1e-3) */
+  int judge_cells;        /* cells re-solved every call to measure the error (1024) */
+  int reserved[8];
+} tng_surrogate_cfg;
+
+typedef struct tng_surrogate_stats {
+  int64_t cells, accepted;
+  int64_t fallback_ood, fallback_consistency, fallback_clip;
+  int64_t judged;               /* sampled cells solved twice */
+  double judge_max_rel_dT;      /* max |T_s - T_p| / T_p over the sample (surrogate vs implicit) */
+  double judge_max_dY;          /* max |Y_s,k - Y_p,k| / max_k Y_p,k over the sample */
+  double ms_infer, ms_post, ms_fallback, ms_total;  /* device times */
+  tng_substep_stats fallback;   /* the implicit solve of the fallback cells */
+} tng_surrogate_stats;
+
+typedef struct tng_surrogate tng_surrogate;
+void tng_surrogate_default_cfg(tng_surrogate_cfg* cfg);
+int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogate** out);
+int tng_surrogate_destroy(tng_surrogate* s);
+/* Train on pairs from the implicit solver: state0 before and state1 after a substep of dts[i]
+ * (device pointers, species-major with leading dimension ld). */
+int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                        int64_t ld, double p, int epochs, int batch, double lr, float* losses);
+int tng_surrogate_save(const tng_surrogate* s, const char* path);
+int tng_surrogate_load(tng_surrogate* s, const char* path);
+/* Sizes: raw inputs/outputs, their padded widths, parameter count. */
+int tng_surrogate_dims(const tng_surrogate* s, int* n_in, int* n_out, int* in_pad, int* out_pad, int64_t* nparam);
+/* Parameters (FP32 master copy, layout of tng_mlp_*) to host (set = 0) or from host (set = 1). */
+int tng_surrogate_params(tng_surrogate* s, float* host, int set);
+/* Normalised FP32 features (n x in_pad, device) of a state batch, for checks and tooling. */
+int tng_surrogate_features(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double p,
+                           float* X);
+/* FP32 reference forward of the network on normalised features (device pointers). */
+int tng_surrogate_forward_f32(tng_surrogate* s, const float* X, int64_t n, float* Y);
+/* Tensor-core inference only: normalised predictions (n x out_pad FP32, device) of a state batch. */
+int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double dt,
+                        double p, float* out);
+/* The substep through the surrogate with fallback; same state convention as tng_substep_batch.
+ * flags: TNG_DEVICE_PTRS or TNG_HOST_PTRS. stats may be null. */
+int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t ncells, int64_t ld, const double* dts,
+                          double dt, double p, int flags, tng_surrogate_stats* stats);
+
 /* Measurement helper (no reference counterpart): sustained FP64 FMA throughput of a device in
  * TFLOP/s (FMA = 2 flops), the denominator of the FP64-pipe roofline of the rate kernels. */
 int tng_bench_fp64_peak(int device, double* tflops);

@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -34,7 +35,7 @@ class TngCfg(ctypes.Structure):
                 ("reserved", ctypes.c_int * 4)]
 
 
-class SubstepStats(ctypes.Structure):
+class SubstepStats(ctypes.Structure):  # noqa: E302
     _fields_ = [("cells", ctypes.c_int64), ("cells_failed", ctypes.c_int64), ("steps", ctypes.c_int64),
                 ("newton_iters", ctypes.c_int64), ("jacobians", ctypes.c_int64), ("max_steps_cell", ctypes.c_int),
                 ("max_newton_cell", ctypes.c_int), ("passes", ctypes.c_int), ("newton_hist", ctypes.c_int * 16),
@@ -44,6 +45,25 @@ class SubstepStats(ctypes.Structure):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "newton_hist"}
         d["newton_hist"] = list(self.newton_hist)
         return d
+
+
+class SurrogateStats(ctypes.Structure):
+    _fields_ = [("cells", ctypes.c_int64), ("accepted", ctypes.c_int64), ("fallback_ood", ctypes.c_int64),
+                ("fallback_consistency", ctypes.c_int64), ("fallback_clip", ctypes.c_int64),
+                ("judged", ctypes.c_int64), ("judge_max_rel_dT", ctypes.c_double), ("judge_max_dY", ctypes.c_double),
+                ("ms_infer", ctypes.c_double), ("ms_post", ctypes.c_double), ("ms_fallback", ctypes.c_double),
+                ("ms_total", ctypes.c_double), ("fallback", SubstepStats)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "fallback"}
+        d["fallback"] = self.fallback.as_dict()
+        return d
+
+
+class SurrogateCfg(ctypes.Structure):
+    _fields_ = [("hidden", ctypes.c_int), ("layers", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("ood_margin", ctypes.c_double), ("consist_tol_K", ctypes.c_double), ("clip_tol", ctypes.c_double),
+                ("judge_cells", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
 
 
 class ChemError(RuntimeError):
@@ -78,6 +98,28 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_bench_fp64_peak": (I, [I, ctypes.POINTER(D)]),
         "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
+        "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
+        "tng_mlp_destroy": (I, [V]),
+        "tng_mlp_param_count": (L, [V]),
+        "tng_mlp_get_params": (I, [V, V, I]),
+        "tng_mlp_set_params": (I, [V, V]),
+        "tng_mlp_forward": (I, [V, V, L, V]),
+        "tng_mlp_grad": (I, [V, V, V, V, L, ctypes.POINTER(ctypes.c_float)]),
+        "tng_mlp_adam_step": (I, [V, ctypes.c_float]),
+        "tng_mlp_train": (I, [V, V, V, V, L, I, I, D, ctypes.c_uint64, V]),
+        "tng_surrogate_default_cfg": (None, [ctypes.POINTER(SurrogateCfg)]),
+        "tng_surrogate_create": (I, [V, ctypes.POINTER(SurrogateCfg), ctypes.POINTER(V)]),
+        "tng_surrogate_destroy": (I, [V]),
+        "tng_surrogate_train": (I, [V, V, V, V, L, L, D, I, I, D, V]),
+        "tng_surrogate_save": (I, [V, ctypes.c_char_p]),
+        "tng_surrogate_load": (I, [V, ctypes.c_char_p]),
+        "tng_surrogate_dims": (I, [V, ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I), ctypes.POINTER(I),
+                                   ctypes.POINTER(L)]),
+        "tng_surrogate_params": (I, [V, V, I]),
+        "tng_surrogate_features": (I, [V, V, L, L, V, D, V]),
+        "tng_surrogate_forward_f32": (I, [V, V, L, V]),
+        "tng_surrogate_infer": (I, [V, V, L, L, V, D, D, V]),
+        "tng_substep_surrogate": (I, [V, V, V, L, L, V, D, D, I, ctypes.POINTER(SurrogateStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -135,9 +177,13 @@ class FiniteChem:
         _check(self.lib.tng_chem_sizes(h, ctypes.byref(ns), ctypes.byref(nr), ctypes.byref(nm)), "tng_chem_sizes")
         self.nspecies, self.nreactions, self.nthirdbody = ns.value, nr.value, nm.value
         self._torch_stream = None
+        self._children = weakref.WeakSet()
 
     def close(self) -> None:
+        """Destroy the handle (and first every network/surrogate object created on it)."""
         if getattr(self, "h", None):
+            for c in list(getattr(self, "_children", ())):
+                c.close()
             self.lib.tng_chem_destroy(self.h)
             self.h = None
 
@@ -309,3 +355,231 @@ def _solver_rhs_jac(self, state, p: float, jacobian: bool = True):
 
 FiniteChem.substep = _substep
 FiniteChem.solver_rhs_jac = _solver_rhs_jac
+
+
+class Mlp:
+    """The surrogate network on the device of a FiniteChem handle (tng_mlp_*)."""
+
+    def __init__(self, chem: "FiniteChem", n_in: int, n_out: int, hidden: int = 256, layers: int = 4, seed: int = 0):
+        self.lib = chem.lib
+        self.chem = chem
+        h = ctypes.c_void_p()
+        _check(self.lib.tng_mlp_create(chem.h, n_in, n_out, hidden, layers, seed, ctypes.byref(h)), "tng_mlp_create")
+        self.h = h
+        self.n_in, self.n_out, self.hidden, self.layers = n_in, n_out, hidden, layers
+        self.in_pad, self.out_pad = -(-n_in // 16) * 16, -(-n_out // 16) * 16
+        self.nparam = self.lib.tng_mlp_param_count(h)
+        chem._children.add(self)
+
+    def close(self):
+        if getattr(self, "h", None):
+            if getattr(self.chem, "h", None):
+                self.lib.tng_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def shapes(self):
+        out, fi = [], self.in_pad
+        for l in range(self.layers + 1):
+            fo = self.out_pad if l == self.layers else self.hidden
+            out.append(((fo, fi), (fo,)))
+            fi = fo
+        return out
+
+    def get(self, which: int = 0):
+        buf = np.zeros(self.nparam, dtype=np.float32)
+        _check(self.lib.tng_mlp_get_params(self.h, buf.ctypes.data, which), "tng_mlp_get_params")
+        return self.unflatten(buf)
+
+    def unflatten(self, buf):
+        out, off = [], 0
+        for (ws, bs) in self.shapes():
+            nw = ws[0] * ws[1]
+            W = buf[off:off + nw].reshape(ws)
+            off += nw
+            b = buf[off:off + bs[0]]
+            off += bs[0]
+            out.append((W, b))
+        return out
+
+    def set(self, params):
+        flat = np.concatenate([np.concatenate([W.reshape(-1), b]) for W, b in params]).astype(np.float32)
+        _check(self.lib.tng_mlp_set_params(self.h, flat.ctypes.data), "tng_mlp_set_params")
+
+    def _dev(self, a, width):
+        import torch
+
+        t = torch.as_tensor(a, dtype=torch.float32, device=f"cuda:{self.chem.device}").contiguous()
+        if t.dim() != 2 or t.shape[1] != width:
+            raise ValueError(f"expected (rows, {width})")
+        return t
+
+    def forward(self, X):
+        import torch
+
+        Xd = self._dev(X, self.in_pad)
+        Y = torch.empty((Xd.shape[0], self.out_pad), dtype=torch.float32, device=Xd.device)
+        self._sync_in()
+        _check(self.lib.tng_mlp_forward(self.h, Xd.data_ptr(), Xd.shape[0], Y.data_ptr()), "tng_mlp_forward")
+        self._sync_out()
+        return Y
+
+    def grad(self, X, T, w_out):
+        Xd, Td = self._dev(X, self.in_pad), self._dev(T, self.out_pad)
+        wd = self._dev(np.asarray(w_out, dtype=np.float32)[None, :], self.out_pad)
+        loss = ctypes.c_float()
+        self._sync_in()
+        _check(self.lib.tng_mlp_grad(self.h, Xd.data_ptr(), Td.data_ptr(), wd.data_ptr(), Xd.shape[0],
+                                     ctypes.byref(loss)), "tng_mlp_grad")
+        return loss.value, self.get(1)
+
+    def adam_step(self, lr):
+        _check(self.lib.tng_mlp_adam_step(self.h, float(lr)), "tng_mlp_adam_step")
+
+    def train(self, X, T, w_out, epochs, batch, lr, seed=0):
+        Xd, Td = self._dev(X, self.in_pad), self._dev(T, self.out_pad)
+        wd = self._dev(np.asarray(w_out, dtype=np.float32)[None, :], self.out_pad)
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._sync_in()
+        _check(self.lib.tng_mlp_train(self.h, Xd.data_ptr(), Td.data_ptr(), wd.data_ptr(), Xd.shape[0], epochs, batch,
+                                      float(lr), seed, losses.ctypes.data), "tng_mlp_train")
+        return losses
+
+    def _sync_in(self):
+        import torch
+
+        self.chem.torch_stream().wait_stream(torch.cuda.current_stream(self.chem.device))
+
+    def _sync_out(self):
+        import torch
+
+        torch.cuda.current_stream(self.chem.device).wait_stream(self.chem.torch_stream())
+
+
+class Surrogate:
+    """The learned substep with fallback (tng_surrogate_*), bound to a FiniteChem handle."""
+
+    def __init__(self, chem: "FiniteChem", **cfg_fields):
+        self.lib = chem.lib
+        self.chem = chem
+        cfg = SurrogateCfg()
+        self.lib.tng_surrogate_default_cfg(ctypes.byref(cfg))
+        for k, v in cfg_fields.items():
+            setattr(cfg, k, v)
+        self.cfg = cfg
+        h = ctypes.c_void_p()
+        _check(self.lib.tng_surrogate_create(chem.h, ctypes.byref(cfg), ctypes.byref(h)), "tng_surrogate_create")
+        self.h = h
+        a, b, c, d = (ctypes.c_int() for _ in range(4))
+        n = ctypes.c_int64()
+        _check(self.lib.tng_surrogate_dims(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d),
+                                           ctypes.byref(n)), "tng_surrogate_dims")
+        self.n_in, self.n_out, self.in_pad, self.out_pad, self.nparam = a.value, b.value, c.value, d.value, n.value
+        chem._children.add(self)
+
+    def close(self):
+        if getattr(self, "h", None):
+            if getattr(self.chem, "h", None):
+                self.lib.tng_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _pre(self):
+        import torch
+
+        self.chem.torch_stream().wait_stream(torch.cuda.current_stream(self.chem.device))
+
+    def _post(self):
+        import torch
+
+        torch.cuda.current_stream(self.chem.device).wait_stream(self.chem.torch_stream())
+
+    def train(self, state0, state1, dts, p: float, epochs: int = 10, batch: int = 4096, lr: float = 1e-3):
+        """Fit on implicit-solver pairs (CUDA float64 tensors, species-major)."""
+        n = state0.shape[1]
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._pre()
+        _check(self.lib.tng_surrogate_train(self.h, state0.data_ptr(), state1.data_ptr(), dts.data_ptr(), n,
+                                            state0.stride(0), float(p), epochs, batch, float(lr), losses.ctypes.data),
+               "tng_surrogate_train")
+        self._post()
+        return losses
+
+    def save(self, path: str):
+        _check(self.lib.tng_surrogate_save(self.h, path.encode()), "tng_surrogate_save")
+
+    def load(self, path: str):
+        _check(self.lib.tng_surrogate_load(self.h, path.encode()), "tng_surrogate_load")
+
+    def params(self):
+        buf = np.zeros(self.nparam, dtype=np.float32)
+        _check(self.lib.tng_surrogate_params(self.h, buf.ctypes.data, 0), "tng_surrogate_params")
+        return buf
+
+    def features(self, state, dts, p: float):
+        import torch
+
+        n = state.shape[1]
+        X = torch.empty((n, self.in_pad), dtype=torch.float32, device=state.device)
+        self._pre()
+        _check(self.lib.tng_surrogate_features(self.h, state.data_ptr(), n, state.stride(0), dts.data_ptr(), float(p),
+                                               X.data_ptr()), "tng_surrogate_features")
+        return X
+
+    def forward_f32(self, X):
+        import torch
+
+        Y = torch.empty((X.shape[0], self.out_pad), dtype=torch.float32, device=X.device)
+        self._pre()
+        _check(self.lib.tng_surrogate_forward_f32(self.h, X.data_ptr(), X.shape[0], Y.data_ptr()),
+               "tng_surrogate_forward_f32")
+        return Y
+
+    def infer(self, state, dts, p: float):
+        import torch
+
+        n = state.shape[1]
+        Y = torch.empty((n, self.out_pad), dtype=torch.float32, device=state.device)
+        self._pre()
+        _check(self.lib.tng_surrogate_infer(self.h, state.data_ptr(), n, state.stride(0), dts.data_ptr(), 0.0,
+                                            float(p), Y.data_ptr()), "tng_surrogate_infer")
+        self._post()
+        return Y
+
+    def substep(self, state, dt, p: float):
+        """The substep through the surrogate with fallback; state advanced in place. Returns stats."""
+        st = SurrogateStats()
+        nv = self.chem.nspecies + 1
+        if isinstance(state, np.ndarray):
+            n = state.shape[1]
+            if state.shape[0] != nv or not state.flags.c_contiguous or state.dtype != np.float64:
+                raise ValueError("state must be C-contiguous float64 (N+1, ncells)")
+            dts = np.ascontiguousarray(dt, dtype=np.float64) if np.ndim(dt) else None
+            _check(self.lib.tng_substep_surrogate(self.chem.h, self.h, state.ctypes.data, n, n,
+                                                  dts.ctypes.data if dts is not None else None,
+                                                  0.0 if dts is not None else float(dt), float(p), TNG_HOST_PTRS,
+                                                  ctypes.byref(st)), "tng_substep_surrogate")
+            return st.as_dict()
+        import torch
+
+        n = state.shape[1]
+        dts = None
+        if not isinstance(dt, (float, int)):
+            dts = torch.as_tensor(dt, dtype=torch.float64, device=state.device).contiguous()
+        self._pre()
+        _check(self.lib.tng_substep_surrogate(self.chem.h, self.h, state.data_ptr(), n, max(state.stride(0), n),
+                                              dts.data_ptr() if dts is not None else None,
+                                              0.0 if dts is not None else float(dt), float(p), TNG_DEVICE_PTRS,
+                                              ctypes.byref(st)), "tng_substep_surrogate")
+        self._post()
+        return st.as_dict()

@@ -370,8 +370,14 @@ def write_all(out_dir: str, names=("hydrogen", "grimech30", "dme39")) -> list[st
 # ---------------------------------------------------------------------------------------------
 # Tables of the warp-cooperative implicit solver (csrc/solver.cuh)
 # ---------------------------------------------------------------------------------------------
+#
+# Slots are renumbered into a processing order (falloff, then exponential Arrhenius, then
+# constant rate constants) so that the 32 lanes of a round take the same branch; every table
+# below is indexed by that position p. "Hot" tables (everything the right-hand side touches) are
+# staged into shared memory once per block; "cold" tables (the Jacobian's work lists) are read
+# through L1. Stoichiometric coefficients are small integers and are packed into the index words.
 
-SV_SCALARS = ("rgas", "tmid", "troe_n0", "troe_n1", "troe_c0", "troe_c1", "troe_d", "lnkmin", "inv_ln10")
+NONE7 = 127
 
 
 def _lpt(sizes: list[int], nlanes: int = 32) -> list[list[int]]:
@@ -386,208 +392,198 @@ def _lpt(sizes: list[int], nlanes: int = 32) -> list[list[int]]:
     return [sorted(x) for x in lanes]
 
 
+def _nu8(v: float) -> int:
+    iv = int(round(v))
+    if iv != v or not -127 <= iv <= 127:
+        raise ValueError("stoichiometric coefficient is not a small integer")
+    return iv & 0xFF
+
+
 def solver_tables(name: str) -> dict:
-    """Flat double/int tables for one mechanism: doubles per literal mode, ints shared."""
     g = _Gen(name)
     m32, m64 = g.m32, g.m64
     ns, nslot, nm = g.ns, g.nslot, g.nm
     nv = ns + 1
-    ints: dict[str, list[int]] = {}
-    dbl: dict[str, list[list[float]]] = {}
+    if ns >= NONE7 or nm >= NONE7:
+        raise ValueError("too many species or third-body sets for the packed solver tables")
 
-    def D(key, v32, v64):
-        dbl[key] = [list(map(float, v32)), list(map(float, v64))]
+    def kind(s):
+        if s.kind == "falloff":
+            return 0
+        return 2 if (s.arr.n is None and s.arr.E is None) else 1
 
-    # slots
-    flags, A, lnA, nn, EE, reac, mw, fo = ([], [], [], [], [], [], [], [])
-    A6, lnA6, nn6, EE6 = [], [], [], []
+    order = sorted(range(nslot), key=lambda r: (kind(m32.slots[r]), r))
+    pos = {r: p for p, r in enumerate(order)}
+    hd = {}  # name -> [list32, list64]
+    hi = {}
+    ci = {}
+
+    def HD(key, v32, v64):
+        hd[key] = [list(map(float, v32)), list(map(float, v64))]
+
+    # slots (processing order)
+    sd32, sd64, si = [], [], []
     fos = []
-    for s32, s64 in zip(m32.slots, m64.slots):
-        reac.extend((s32.C + [-1, -1, -1])[:3])
-        mw.append(s32.M)
+    for r in order:
+        s32, s64 = m32.slots[r], m64.slots[r]
+        reac = (s32.C + [NONE7] * 3)[:3]
+        mw = s32.M if s32.M >= 0 else NONE7
         if s32.kind == "falloff":
-            flags.append(1)
-            fo.append(len(fos))
+            flags, fo = 1, len(fos)
             fos.append((s32, s64))
-            A.append(0.0), lnA.append(0.0), nn.append(0.0), EE.append(0.0)
-            A6.append(0.0), lnA6.append(0.0), nn6.append(0.0), EE6.append(0.0)
-            continue
-        a, b = s32.arr, s64.arr
-        f = (2 if a.n is not None else 0) | (4 if a.E is not None else 0)
-        if f == 0:
-            f = 8
-        flags.append(f)
-        fo.append(-1)
-        A.append(a.A), A6.append(b.A)
-        lnA.append(math.log(a.A)), lnA6.append(math.log(b.A))
-        nn.append(a.n or 0.0), nn6.append(b.n or 0.0)
-        EE.append(a.E or 0.0), EE6.append(b.E or 0.0)
-    ints["slot_flags"], ints["slot_reac"], ints["slot_mw"], ints["slot_fo"] = flags, reac, mw, fo
-    D("slot_A", A, A6), D("slot_lnA", lnA, lnA6), D("slot_n", nn, nn6), D("slot_E", EE, EE6)
+            sd32 += [0.0] * 4
+            sd64 += [0.0] * 4
+        else:
+            a, b = s32.arr, s64.arr
+            flags = (2 if a.n is not None else 0) | (4 if a.E is not None else 0)
+            fo = 0
+            if flags == 0:
+                flags = 8
+                sd32 += [a.A, 0.0, 0.0, 0.0]
+                sd64 += [b.A, 0.0, 0.0, 0.0]
+            else:
+                sd32 += [math.log(a.A), a.E or 0.0, a.n or 0.0, 0.0]
+                sd64 += [math.log(b.A), b.E or 0.0, b.n or 0.0, 0.0]
+        si += [flags | (reac[0] << 4) | (reac[1] << 11) | (reac[2] << 18), mw | (fo << 8)]
+    HD("slot", sd32, sd64)
+    hi["slot"] = si
 
-    # falloff and F_cent expressions
     fc_ids: dict[tuple, int] = {}
-    fc_terms32: list[list] = []
-    fc_terms64: list[list] = []
-    fo_flags, fo_fc, fo_m = [], [], []
-    fo_d32, fo_d64 = [], []
+    fcd32, fcd64, fci = [], [], []
+    fod32, fod64, foi = [], [], []
     for s32, s64 in fos:
-        row32, row64, fl = [], [], []
+        fl = []
         for a, b in ((s32.k0, s64.k0), (s32.kinf, s64.kinf)):
             fl.append((2 if a.n is not None else 0) | (4 if a.E is not None else 0))
-            row32 += [math.log(a.A), a.n or 0.0, a.E or 0.0]
-            row64 += [math.log(b.A), b.n or 0.0, b.E or 0.0]
-        fo_flags += fl
-        fo_d32 += row32
-        fo_d64 += row64
-        fo_m.append(s32.M_fall)
+            fod32 += [math.log(a.A), a.E or 0.0, a.n or 0.0]
+            fod64 += [math.log(b.A), b.E or 0.0, b.n or 0.0]
         key = s32.fc_key
         if key == ((1.0, 1, 0.0),):
-            fo_fc.append(-1)
-            continue
-        if key not in fc_ids:
-            fc_ids[key] = len(fc_ids)
-            t32, t64 = [], []
-            for (a, form, x), (a6, _, x6) in zip(s32.fc, s64.fc):
-                if form == 0 and x <= 1e-20:
-                    continue
-                if form == 1 and x >= 1e20:
-                    continue
-                if (form == 0 and x >= 1e20) or (form == 1 and x == 0.0):
-                    t32.append((2, a, 0.0)), t64.append((2, a6, 0.0))
-                elif form == 0:
-                    t32.append((0, a, 1.0 / x)), t64.append((0, a6, 1.0 / x6))
-                else:
-                    t32.append((1, a, x)), t64.append((1, a6, x6))
-            assert 1 <= len(t32) <= 3
-            fc_terms32.append(t32)
-            fc_terms64.append(t64)
-        fo_fc.append(fc_ids[key])
+            fcid = -1
+        else:
+            if key not in fc_ids:
+                fc_ids[key] = len(fc_ids)
+                forms, r32, r64 = [], [], []
+                for (a, form, x), (a6, _, x6) in zip(s32.fc, s64.fc):
+                    if form == 0 and x <= 1e-20:
+                        continue
+                    if form == 1 and x >= 1e20:
+                        continue
+                    if (form == 0 and x >= 1e20) or (form == 1 and x == 0.0):
+                        forms.append(2), r32.append((a, 0.0)), r64.append((a6, 0.0))
+                    elif form == 0:
+                        forms.append(0), r32.append((a, 1.0 / x)), r64.append((a6, 1.0 / x6))
+                    else:
+                        forms.append(1), r32.append((a, x)), r64.append((a6, x6))
+                assert 1 <= len(forms) <= 3
+                while len(forms) < 3:
+                    forms.append(15), r32.append((0.0, 0.0)), r64.append((0.0, 0.0))
+                fci.append(forms[0] | (forms[1] << 4) | (forms[2] << 8))
+                fcd32 += [v for t in r32 for v in t]
+                fcd64 += [v for t in r64 for v in t]
+            fcid = fc_ids[key]
+        foi.append(fl[0] | (fl[1] << 4) | ((fcid + 1) << 8) | (s32.M_fall << 16))
+    HD("fo", fod32, fod64)
+    hi["fo"] = foi
+    HD("fc", fcd32, fcd64)
+    hi["fc"] = fci
     nfo, nfc = len(fos), len(fc_ids)
-    ints["fo_flags"], ints["fo_fc"], ints["fo_m"] = fo_flags, fo_fc, fo_m
-    D("fo_par", fo_d32, fo_d64)
-    fcf, fca32, fcc32, fca64, fcc64 = [], [], [], [], []
-    for t32, t64 in zip(fc_terms32, fc_terms64):
-        for i in range(3):
-            if i < len(t32):
-                fcf.append(t32[i][0]), fca32.append(t32[i][1]), fcc32.append(t32[i][2])
-                fca64.append(t64[i][1]), fcc64.append(t64[i][2])
-            else:
-                fcf.append(-1), fca32.append(0.0), fcc32.append(0.0), fca64.append(0.0), fcc64.append(0.0)
-    ints["fc_form"] = fcf
-    D("fc_a", fca32, fca64), D("fc_c", fcc32, fcc64)
 
-    # third-body sums (table order) and dense efficiencies
-    tb_ptr, tb_sp, tbc32, tbc64 = [0], [], [], []
     eff32 = np.zeros((max(nm, 1), ns))
     eff64 = np.zeros((max(nm, 1), ns))
     for j, (t32, t64) in enumerate(zip(m32.third_body, m64.third_body)):
         for (s_, c), (_, c6) in zip(t32, t64):
-            tb_sp.append(s_), tbc32.append(c), tbc64.append(c6)
             eff32[j, s_] += c
             eff64[j, s_] += c6
-        tb_ptr.append(len(tb_sp))
-    ints["tb_ptr"], ints["tb_sp"] = tb_ptr, tb_sp
-    D("tb_coef", tbc32, tbc64), D("eff", eff32.reshape(-1), eff64.reshape(-1))
-
-    # production rates: species rows split into chunks, chunks balanced over lanes
-    total = int((m32.nu != 0).sum())
-    chunk = max(8, -(-total // 32))
-    cd_chunk_sp, cd_chunk_beg, cd_chunk_end, cd_slot, cdn32, cdn64, cd_sp_ptr = [], [], [], [], [], [], [0]
-    for k in range(ns):
-        rs = [r for r in range(nslot) if m32.nu[k, r] != 0.0 or m64.nu[k, r] != 0.0]
-        for b in range(0, len(rs), chunk):
-            cd_chunk_sp.append(k)
-            cd_chunk_beg.append(len(cd_slot))
-            for r in rs[b:b + chunk]:
-                cd_slot.append(r), cdn32.append(m32.nu[k, r]), cdn64.append(m64.nu[k, r])
-            cd_chunk_end.append(len(cd_slot))
-        cd_sp_ptr.append(len(cd_chunk_sp))
-    lanes = _lpt([e - b for b, e in zip(cd_chunk_beg, cd_chunk_end)])
-    ints["cd_lane_ptr"] = [0]
-    ints["cd_lane_list"] = []
-    for L in lanes:
-        ints["cd_lane_list"] += L
-        ints["cd_lane_ptr"].append(len(ints["cd_lane_list"]))
-    ints["cd_chunk_beg"], ints["cd_chunk_end"], ints["cd_slot"], ints["cd_sp_ptr"] = (
-        cd_chunk_beg, cd_chunk_end, cd_slot, cd_sp_ptr)
-    D("cd_nu", cdn32, cdn64)
-
-    # Jacobian, direct mass-action part: groups per (i, j), balanced over lanes
-    groups: dict[tuple, list] = {}
-    for s in m32.slots:
-        r = s.index
-        for pidx, j in enumerate(s.C):
-            for i in range(ns):
-                if m32.nu[i, r] != 0.0 or m64.nu[i, r] != 0.0:
-                    groups.setdefault((i, j), []).append((r, pidx, m32.nu[i, r], m64.nu[i, r]))
-    keys = sorted(groups)
-    lanes = _lpt([len(groups[k]) for k in keys])
-    jd_tgt, jd_beg, jd_end, jd_slot, jd_pos, jdn32, jdn64 = [], [], [], [], [], [], []
-    for k in keys:
-        jd_tgt.append(k[0] * nv + k[1])
-        jd_beg.append(len(jd_slot))
-        for r, pidx, a, b in groups[k]:
-            jd_slot.append(r), jd_pos.append(pidx), jdn32.append(a), jdn64.append(b)
-        jd_end.append(len(jd_slot))
-    ints["jd_lane_ptr"], ints["jd_lane_list"] = [0], []
-    for L in lanes:
-        ints["jd_lane_list"] += L
-        ints["jd_lane_ptr"].append(len(ints["jd_lane_list"]))
-    ints["jd_tgt"], ints["jd_beg"], ints["jd_end"], ints["jd_slot"], ints["jd_pos"] = jd_tgt, jd_beg, jd_end, jd_slot, jd_pos
-    D("jd_nu", jdn32, jdn64)
-
-    # Jacobian, third-body and falloff-[M] part: G[i][m] pairs
-    pairs: dict[tuple, list] = {}
-    for s in m32.slots:
-        r = s.index
-        src = []
-        if s.M >= 0:
-            src.append((s.M, 0))
-        if s.kind == "falloff":
-            src.append((s.M_fall, 1))
-        for mm, kind in src:
-            for i in range(ns):
-                if m32.nu[i, r] != 0.0 or m64.nu[i, r] != 0.0:
-                    pairs.setdefault((i, mm), []).append((r, kind, m32.nu[i, r], m64.nu[i, r]))
-    pkeys = sorted(pairs)
-    lanes = _lpt([len(pairs[k]) for k in pkeys])
-    g_i, g_m, g_beg, g_end, g_slot, g_kind, gn32, gn64 = [], [], [], [], [], [], [], []
-    for k in pkeys:
-        g_i.append(k[0]), g_m.append(k[1]), g_beg.append(len(g_slot))
-        for r, kind, a, b in pairs[k]:
-            g_slot.append(r), g_kind.append(kind), gn32.append(a), gn64.append(b)
-        g_end.append(len(g_slot))
-    ints["g_lane_ptr"], ints["g_lane_list"] = [0], []
-    for L in lanes:
-        ints["g_lane_list"] += L
-        ints["g_lane_ptr"].append(len(ints["g_lane_list"]))
-    ints["g_i"], ints["g_m"], ints["g_beg"], ints["g_end"], ints["g_slot"], ints["g_kind"] = (
-        g_i, g_m, g_beg, g_end, g_slot, g_kind)
-    D("g_nu", gn32, gn64)
-
-    # thermo and molar masses
-    D("th_hi", m32.th_hi.reshape(-1), m64.th_hi.reshape(-1))
-    D("th_lo", m32.th_lo.reshape(-1), m64.th_lo.reshape(-1))
-    D("wmol", m32.wmol, m64.wmol)
-    D("invw", 1.0 / m32.wmol, 1.0 / m64.wmol)
+    HD("eff", eff32.reshape(-1), eff64.reshape(-1))
+    th32 = np.concatenate([m32.th_hi, m32.th_lo], axis=1).reshape(-1)
+    th64 = np.concatenate([m64.th_hi, m64.th_lo], axis=1).reshape(-1)
+    HD("th", th32, th64)
+    HD("wmol", m32.wmol, m64.wmol)
+    HD("invw", 1.0 / m32.wmol, 1.0 / m64.wmol)
     sc = []
     for mm in (m32, m64):
         t = mm.troe
         sc.append([mm.rgas, mm.tmid, t["c_n0"], t["c_n1"], t["c_c0"], t["c_c1"], t["c_d"], math.log(t["kmin"]),
                    INV_LN10])
-    dbl["scal"] = sc
-    sizes = {"ns": ns, "nv": nv, "nslot": nslot, "nm": nm, "nfo": nfo, "nfc": nfc, "ncdchunk": len(cd_chunk_beg),
-             "njdgrp": len(jd_tgt), "ngpair": len(g_i)}
-    return {"ints": ints, "dbl": dbl, "sizes": sizes}
+    hd["scal"] = sc
+
+    # production rates: species rows split into chunks, chunks balanced over lanes
+    if not np.array_equal(m32.nu, m64.nu):
+        raise ValueError("stoichiometry depends on the literal mode")
+    nu = m32.nu
+    total = int((nu != 0).sum())
+    chunk = max(8, -(-total // 32))
+    cbeg, cend, cterm, spp = [], [], [], [0]
+    for k in range(ns):
+        ps = sorted(pos[r] for r in range(nslot) if nu[k, r] != 0.0)
+        for b in range(0, len(ps), chunk):
+            cbeg.append(len(cterm))
+            for p in ps[b:b + chunk]:
+                cterm.append((p << 8) | _nu8(nu[k, order[p]]))
+            cend.append(len(cterm))
+        spp.append(len(cbeg))
+    lanes = _lpt([e - b for b, e in zip(cbeg, cend)])
+    hi["cd_lane_ptr"], hi["cd_lane_list"] = [0], []
+    for L in lanes:
+        hi["cd_lane_list"] += L
+        hi["cd_lane_ptr"].append(len(hi["cd_lane_list"]))
+    hi["cd_beg"], hi["cd_end"], hi["cd_sp_ptr"], hi["cd_term"] = cbeg, cend, spp, cterm
+
+    # Jacobian, direct mass-action part: groups per (i, j), balanced over lanes
+    groups: dict[tuple, list] = {}
+    for p, r in enumerate(order):
+        s = m32.slots[r]
+        for rp, j in enumerate(s.C):
+            for i in range(ns):
+                if nu[i, r] != 0.0:
+                    groups.setdefault((i, j), []).append((p << 12) | (rp << 8) | _nu8(nu[i, r]))
+    keys = sorted(groups)
+    lanes = _lpt([len(groups[k]) for k in keys])
+    ci["jd_lane_ptr"], ci["jd_lane_list"] = [0], []
+    for L in lanes:
+        ci["jd_lane_list"] += L
+        ci["jd_lane_ptr"].append(len(ci["jd_lane_list"]))
+    ci["jd_tgt"], ci["jd_beg"], ci["jd_end"], ci["jd_term"] = [], [], [], []
+    for k in keys:
+        ci["jd_tgt"].append(k[0] * nv + k[1])
+        ci["jd_beg"].append(len(ci["jd_term"]))
+        ci["jd_term"] += groups[k]
+        ci["jd_end"].append(len(ci["jd_term"]))
+
+    # Jacobian, third-body and falloff-[M] part: G[i][m] pairs
+    pairs: dict[tuple, list] = {}
+    for p, r in enumerate(order):
+        s = m32.slots[r]
+        src = []
+        if s.M >= 0:
+            src.append((s.M, 0))
+        if s.kind == "falloff":
+            src.append((s.M_fall, 1))
+        for mm, kd in src:
+            for i in range(ns):
+                if nu[i, r] != 0.0:
+                    pairs.setdefault((i, mm), []).append((p << 12) | (kd << 8) | _nu8(nu[i, r]))
+    pkeys = sorted(pairs)
+    lanes = _lpt([len(pairs[k]) for k in pkeys])
+    ci["g_lane_ptr"], ci["g_lane_list"] = [0], []
+    for L in lanes:
+        ci["g_lane_list"] += L
+        ci["g_lane_ptr"].append(len(ci["g_lane_list"]))
+    ci["g_i"], ci["g_m"], ci["g_beg"], ci["g_end"], ci["g_term"] = [], [], [], [], []
+    for k in pkeys:
+        ci["g_i"].append(k[0]), ci["g_m"].append(k[1]), ci["g_beg"].append(len(ci["g_term"]))
+        ci["g_term"] += pairs[k]
+        ci["g_end"].append(len(ci["g_term"]))
+    sizes = {"ns": ns, "nv": nv, "nslot": nslot, "nm": nm, "nfo": nfo, "nfc": nfc, "ncdchunk": len(cbeg),
+             "njdgrp": len(keys), "ngpair": len(pkeys)}
+    return {"hd": hd, "hi": hi, "ci": ci, "sizes": sizes, "order": order}
 
 
-SV_INT_KEYS = ("slot_flags", "slot_reac", "slot_mw", "slot_fo", "fo_flags", "fo_fc", "fo_m", "fc_form", "tb_ptr",
-               "tb_sp", "cd_lane_ptr", "cd_lane_list", "cd_chunk_beg", "cd_chunk_end", "cd_slot", "cd_sp_ptr",
-               "jd_lane_ptr", "jd_lane_list", "jd_tgt", "jd_beg", "jd_end", "jd_slot", "jd_pos",
-               "g_lane_ptr", "g_lane_list", "g_i", "g_m", "g_beg", "g_end", "g_slot", "g_kind")
-SV_DBL_KEYS = ("slot_A", "slot_lnA", "slot_n", "slot_E", "fo_par", "fc_a", "fc_c", "tb_coef", "eff", "cd_nu", "jd_nu",
-               "g_nu", "th_hi", "th_lo", "wmol", "invw", "scal")
+SV_HD_KEYS = ("slot", "fo", "fc", "eff", "th", "wmol", "invw", "scal")
+SV_HI_KEYS = ("slot", "fo", "fc", "cd_lane_ptr", "cd_lane_list", "cd_beg", "cd_end", "cd_sp_ptr", "cd_term")
+SV_CI_KEYS = ("jd_lane_ptr", "jd_lane_list", "jd_tgt", "jd_beg", "jd_end", "jd_term",
+              "g_lane_ptr", "g_lane_list", "g_i", "g_m", "g_beg", "g_end", "g_term")
 SV_SIZE_KEYS = ("ns", "nv", "nslot", "nm", "nfo", "nfc", "ncdchunk", "njdgrp", "ngpair")
 
 
@@ -595,25 +591,36 @@ def solver_header(name: str) -> str:
     t = solver_tables(name)
     out = [f"// Generated by tiger_nga_b200/codegen.py: solver tables of mechanism {name}.",
            "#pragma once", '#include "solver_layout.h"', "namespace tng {"]
-    ioff, iflat = [], []
-    for k in SV_INT_KEYS:
-        ioff.append(len(iflat))
-        iflat += [int(x) for x in t["ints"][k]]
-    doff, dflat = [], [[], []]
-    for k in SV_DBL_KEYS:
-        doff.append(len(dflat[0]))
+
+    def flat_int(src, keys):
+        off, flat = [], []
+        for k in keys:
+            off.append(len(flat))
+            flat += [int(x) for x in src[k]]
+        return off, (flat or [0])
+
+    hio, hif = flat_int(t["hi"], SV_HI_KEYS)
+    cio, cif = flat_int(t["ci"], SV_CI_KEYS)
+    hdo, hdf = [], [[], []]
+    for k in SV_HD_KEYS:
+        hdo.append(len(hdf[0]))
         for lm in (0, 1):
-            dflat[lm] += t["dbl"][k][lm]
-    iflat = iflat or [0]
-    out.append(f"static const int {name}_sv_int[{len(iflat)}] = {{" + ", ".join(map(str, iflat)) + "};")
-    out.append(f"static const double {name}_sv_dbl[2][{len(dflat[0])}] = {{"
-               + ", ".join("{" + ", ".join(_d(x) for x in dflat[lm]) + "}" for lm in (0, 1)) + "};")
+            hdf[lm] += t["hd"][k][lm]
+    # keep the double block a multiple of 2 (16-byte staging granule)
+    if len(hdf[0]) % 2:
+        hdf[0].append(0.0), hdf[1].append(0.0)
+    while len(hif) % 4:
+        hif.append(0)
+    out.append(f"static const double {name}_sv_hd[2][{len(hdf[0])}] = {{"
+               + ", ".join("{" + ", ".join(_d(x) for x in hdf[lm]) + "}" for lm in (0, 1)) + "};")
+    out.append(f"static const int {name}_sv_hi[{len(hif)}] = {{" + ", ".join(map(str, hif)) + "};")
+    out.append(f"static const int {name}_sv_ci[{len(cif)}] = {{" + ", ".join(map(str, cif)) + "};")
     sz = ", ".join(str(t["sizes"][k]) for k in SV_SIZE_KEYS)
-    out.append(f"static const SvLayout {name}_sv_layout = {{{{{sz}}}, {{{', '.join(map(str, ioff))}}}, "
-               f"{{{', '.join(map(str, doff))}}}, {len(iflat)}, {len(dflat[0])}}};")
+    out.append(f"static const SvLayout {name}_sv_layout = {{{{{sz}}}, {{{', '.join(map(str, hdo))}}}, "
+               f"{{{', '.join(map(str, hio))}}}, {{{', '.join(map(str, cio))}}}, {len(hdf[0])}, {len(hif)}, "
+               f"{len(cif)}}};")
     out.append("}  // namespace tng")
     return "\n".join(out) + "\n"
-
 
 if __name__ == "__main__":
     for p in write_all(sys.argv[1] if len(sys.argv) > 1 else "tiger_nga_b200/_build/gen"):

@@ -10,9 +10,11 @@ struct BdfCoef {
   double errc[kQmax + 2], dnc[kQmax + 2], upc[kQmax + 2];
 };
 
+// BDF coefficients in constant memory (indexed by the run-time order q).
+__constant__ BdfCoef c_bdf;
+
 struct BdfLaunch {
   BdfArgs a;
-  BdfCoef c;
   const int* n_in_dev;  // when non-null, the number of queued cells is read from device memory
 };
 
@@ -87,10 +89,10 @@ __device__ __forceinline__ void zset(double (&z)[kQmax + 2][2], const int j, con
 
 // Integrate one cell (warp-cooperative). Returns true when the cell is finished (any status),
 // false when it used up the pass budget and was saved for the next pass.
-__device__ bool bdf_cell(const BdfLaunch& P, const WarpMem& w, const int cell, const int lane) {
+__device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, const WarpMem& w, const int cell,
+                                         const int lane) {
   const BdfArgs& a = P.a;
-  const BdfCoef& C = P.c;
-  const SvDev& t = a.tab;
+  const BdfCoef& C = c_bdf;
   const int ns = t.L.size[SZ_NS], nv = ns + 1, rs = a.rs;
   const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
   const double p = a.p, rtol = a.rtol, atol = a.atol;
@@ -408,11 +410,16 @@ finish:
   return true;
 }
 
+// Shared memory of one block: the staged hot tables, then one workspace per warp.
+__host__ __device__ inline int hot_smem_doubles(const SvLayout& L) { return (hot_smem_bytes(L) + 15) / 16 * 2; }
+
+// One block per SM of WARPS warps (the staged tables are shared by the block's warps).
 template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_bdf(const BdfLaunch P) {
-  extern __shared__ double smem[];
+__global__ void __launch_bounds__(WARPS * 32, 1) k_bdf(const BdfLaunch P) {
+  extern __shared__ __align__(16) double smem[];
+  const SvDev t = stage_tables(P.a.tab, smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpMem w = warp_mem(smem + (size_t)warp * P.a.smem_warp, P.a.tab.L, P.a.rs);
+  const WarpMem w = warp_mem(smem + hot_smem_doubles(t.L) + (size_t)warp * P.a.smem_warp, t.L, P.a.rs);
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.a.n_in;
   for (;;) {
     int idx = 0;
@@ -420,18 +427,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_bdf(const BdfLaunch P) {
     idx = __shfl_sync(kFull, idx, 0);
     if (idx >= n_in) break;
     const int cell = P.a.queue_in ? P.a.queue_in[idx] : idx;
-    bdf_cell(P, w, cell, lane);
+    bdf_cell(P, t, w, cell, lane);
   }
 }
 
 // Standalone right-hand side / Jacobian of the table-driven warp path (parity checks).
 template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
-    k_warp_rhs_jac(SvDev t, const double* __restrict__ state, long long ld, int n, double p, double* __restrict__ rhs,
+    k_warp_rhs_jac(SvDev g, const double* __restrict__ state, long long ld, int n, double p, double* __restrict__ rhs,
                    double* __restrict__ jac, int rs, int smem_warp) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
+  const SvDev t = stage_tables(g, smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpMem w = warp_mem(smem + (size_t)warp * smem_warp, t.L, rs);
+  const WarpMem w = warp_mem(smem + hot_smem_doubles(t.L) + (size_t)warp * smem_warp, t.L, rs);
   const int nv = t.L.size[SZ_NV];
   for (int cell = blockIdx.x * WARPS + warp; cell < n; cell += gridDim.x * WARPS) {
     const double y0 = lane < nv ? state[(long long)lane * ld + cell] : 0.0;

@@ -118,6 +118,9 @@ int tng_chem_create(const char* mechanism, const tng_cfg* cfg, tng_chem** out) {
 
 int tng_chem_destroy(tng_chem* h) {
   if (!h) return TNG_OK;
+  if (h->dependents > 0)
+    return set_error(TNG_ERR_STATE, "tng_chem_destroy: %d network/surrogate objects still use this handle",
+                     h->dependents);
   {
     DeviceGuard g(h->cfg.device);
     if (h->stream) cudaStreamSynchronize(h->stream);

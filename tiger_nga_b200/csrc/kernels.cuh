@@ -62,8 +62,9 @@ struct MechOps {
                      long long ld, double p, int block, cudaStream_t st);
   // tables of the implicit solver
   const SvLayout* sv_layout;
-  const int* sv_int;
-  const double* sv_dbl[2];
+  const double* sv_hd[2];  // hot doubles per literal mode
+  const int* sv_hi;        // hot ints
+  const int* sv_ci;        // cold ints
 };
 
 // Kernel variants of the rate evaluation (the autotuner's choices): 0 = plain, 1 = block

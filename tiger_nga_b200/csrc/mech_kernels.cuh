@@ -6,7 +6,8 @@ namespace tng {
 
 template <class Mech>
 MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int nelem, const char* const* elements,
-                 const double* elem, const SvLayout* svl, const int* svi, const double* svd0, const double* svd1) {
+                 const double* elem, const SvLayout* svl, const double* hd0, const double* hd1, const int* hi,
+                 const int* ci) {
   MechOps o{};
   o.name = Mech::NAME;
   o.ns = Mech::NS;
@@ -20,9 +21,10 @@ MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int
   o.elem = elem;
   o.rhs = &launch_rhs<Mech>;
   o.sv_layout = svl;
-  o.sv_int = svi;
-  o.sv_dbl[0] = svd0;
-  o.sv_dbl[1] = svd1;
+  o.sv_hd[0] = hd0;
+  o.sv_hd[1] = hd1;
+  o.sv_hi = hi;
+  o.sv_ci = ci;
   return o;
 }
 

@@ -1,0 +1,304 @@
+// K4: surrogate inference on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// One persistent CTA per SM walks tiles of 128 cells. For each tile:
+//   1. the 128 threads compute the cell features from the FP64 state (one cell per thread,
+//      species-major loads) and store them as BF16 into shared memory in the UMMA canonical
+//      K-major layout (8-row x 16-byte core matrices);
+//   2. every layer is D[128 x N] = H[128 x K] * W^T on tcgen05.mma (kind::f16, BF16 operands,
+//      FP32 accumulator in tensor memory); one elected thread issues the MMAs, weights stream
+//      from global memory (L2-resident, shared by all CTAs) into a two-stage shared-memory ring
+//      with cp.async.bulk + mbarrier transaction counts; tcgen05.commit releases ring stages;
+//   3. the epilogue (all 128 threads, each owning one accumulator row = one TMEM lane) reads D
+//      with tcgen05.ld, adds the bias, applies GELU and writes the next layer's BF16 operand back
+//      into shared memory; the last layer's FP32 outputs go to global memory.
+// Every wait is bounded: on expiry the CTA records an error code and stops issuing work.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tng {
+
+constexpr int kInferRows = 128;
+constexpr int kInferThreads = 128;
+constexpr int kWChunkK = 64;  // K width of one streamed weight chunk
+constexpr int kMaxLayers = 9;
+
+struct InferArgs {
+  const double* state;  // species-major [v*ld + cell]
+  long long ld;
+  int ncells;
+  const double* dts;  // per-cell dt or null
+  double dt_scalar;
+  double logp;        // log(pressure)
+  int ns;             // species count
+  int bath;           // species index left out of the inputs (the bath gas)
+  int n_in, in_pad, hidden, out_pad, nlin;
+  const float* fmean;  // feature normalisation, n_in entries
+  const float* fistd;  // 1/std
+  const __nv_bfloat16* wpack;  // all layers, chunked canonical layout
+  long long w_off[kMaxLayers];  // element offset of layer l in wpack
+  const float* bias;            // all layers, fan_out entries each
+  int b_off[kMaxLayers];
+  float* out;  // [ncells x out_pad] FP32 (normalised predictions)
+  int* error;  // non-zero after a timed-out wait
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// canonical K-major, no swizzle: byte offset of element (r, k) in a [R x K] bf16 operand
+__device__ __forceinline__ uint32_t canon_off(int r, int k, int K) {
+  return (uint32_t)((r >> 3) * (K * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+  return d;              // base offset 0, layout SWIZZLE_NONE
+}
+
+// kind::f16 instruction descriptor: BF16 x BF16 -> F32, both operands K-major
+__device__ __forceinline__ uint32_t umma_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// bounded parity wait; returns false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const uint32_t a = smem_u32(bar);
+  for (int it = 0; it < (1 << 24); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,"
+      "%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu_fast(float x) {
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return 0.5f * x * (1.0f + t);
+}
+
+// shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), two weight stages of
+// 256 x 64 bf16 (32 KB each), barriers and the TMEM address.
+constexpr int kSmemA = kInferRows * 256 * 2;
+constexpr int kSmemStage = 256 * kWChunkK * 2;
+constexpr int kInferSmem = kSmemA + 2 * kSmemStage + 128;
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs a) {
+  extern __shared__ __align__(1024) uint8_t sm[];
+  uint8_t* sA = sm;
+  uint8_t* sW = sm + kSmemA;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kSmemA + 2 * kSmemStage);
+  // bars[0..1]: stage full, bars[2..3]: stage free, bars[4]: layer done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 6);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  if (tid == 0) {
+    for (int i = 0; i < 5; ++i) mbar_init(&bars[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tmem_slot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  uint32_t ph_full[2] = {0, 0}, ph_free[2] = {0, 0}, ph_done = 0;
+  int stage_busy[2] = {0, 0};  // thread 0 only: a commit to stage_free is pending
+  int err = 0;
+  const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
+  for (int tile = blockIdx.x; tile < ntiles && !err; tile += gridDim.x) {
+    // ---- 1. features of the tile's cells into A (K = in_pad)
+    {
+      const int cell = tile * kInferRows + tid;
+      const bool live = cell < a.ncells;
+      float f[64];
+#pragma unroll
+      for (int i = 0; i < 64; ++i) f[i] = 0.f;
+      if (live) {
+        double rho = 0.0;
+        for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
+        const double T = a.state[(long long)a.ns * a.ld + cell] / rho;
+        const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
+        f[0] = (float)T;
+        f[1] = (float)a.logp;
+        int j = 2;
+        for (int k = 0; k < a.ns; ++k) {
+          if (k == a.bath) continue;
+          const double y = a.state[(long long)k * a.ld + cell] / rho;
+          f[j++] = (float)log10(fmax(y, 1e-30));
+        }
+        f[j] = (float)log10(fmax(dt, 1e-30));
+        for (int i = 0; i < a.n_in; ++i) f[i] = (f[i] - a.fmean[i]) * a.fistd[i];
+      }
+      for (int k8 = 0; k8 < a.in_pad; k8 += 8) {
+        __nv_bfloat162 p0 = __floats2bfloat162_rn(f[k8 + 0], f[k8 + 1]);
+        __nv_bfloat162 p1 = __floats2bfloat162_rn(f[k8 + 2], f[k8 + 3]);
+        __nv_bfloat162 p2 = __floats2bfloat162_rn(f[k8 + 4], f[k8 + 5]);
+        __nv_bfloat162 p3 = __floats2bfloat162_rn(f[k8 + 6], f[k8 + 7]);
+        uint4 v;
+        v.x = *reinterpret_cast<uint32_t*>(&p0);
+        v.y = *reinterpret_cast<uint32_t*>(&p1);
+        v.z = *reinterpret_cast<uint32_t*>(&p2);
+        v.w = *reinterpret_cast<uint32_t*>(&p3);
+        *reinterpret_cast<uint4*>(sA + canon_off(tid, k8, a.in_pad)) = v;
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // ---- 2./3. layers
+    for (int l = 0; l < a.nlin && !err; ++l) {
+      const int K = l == 0 ? a.in_pad : a.hidden;
+      const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
+      const int nchunk = (K + kWChunkK - 1) / kWChunkK;
+      if (tid == 0) {
+        const __nv_bfloat16* wl = a.wpack + a.w_off[l];
+        const uint32_t idesc = umma_idesc(kInferRows, N);
+        const uint32_t a_sbo = (uint32_t)K * 16;
+        for (int c = 0; c < nchunk && !err; ++c) {
+          const int s = c & 1;
+          const int kc = min(kWChunkK, K - c * kWChunkK);
+          const uint32_t bytes = (uint32_t)N * kc * 2;
+          if (stage_busy[s]) {  // wait for the MMAs that read this stage
+            if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
+            ph_free[s] ^= 1;
+            stage_busy[s] = 0;
+          }
+          mbar_expect_tx(&bars[s], bytes);
+          bulk_g2s(sW + s * kSmemStage, wl + (long long)c * N * kWChunkK, bytes, &bars[s]);
+          if (!mbar_wait(&bars[s], ph_full[s])) err = 1;
+          ph_full[s] ^= 1;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t wbase = smem_u32(sW + s * kSmemStage);
+          const uint32_t abase = smem_u32(sA);
+          for (int kk = 0; kk < kc; kk += 16) {
+            const int kg = c * kWChunkK + kk;
+            const uint64_t ad = umma_desc(abase + (uint32_t)(kg >> 3) * 128, 128, a_sbo);
+            const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
+            umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+          }
+          umma_commit(&bars[2 + s]);
+          stage_busy[s] = 1;
+        }
+        umma_commit(&bars[4]);
+      }
+      // epilogue
+      const bool ok = mbar_wait(&bars[4], ph_done);
+      ph_done ^= 1;
+      if (!ok) err = 1;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const float* bl = a.bias + a.b_off[l];
+      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+      const bool last = l == a.nlin - 1;
+      const int cell = tile * kInferRows + tid;
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        float v[32];
+        tmem_ld32(trow + (uint32_t)c0, v);
+        if (last) {
+          if (cell < a.ncells) {
+            float* o = a.out + (long long)cell * a.out_pad + c0;
+            const int nc = min(32, N - c0);
+            for (int i = 0; i < nc; ++i) o[i] = v[i] + __ldg(bl + c0 + i);
+          }
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            float x[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) x[i] = gelu_fast(v[q * 8 + i] + __ldg(bl + c0 + q * 8 + i));
+            __nv_bfloat162 p0 = __floats2bfloat162_rn(x[0], x[1]);
+            __nv_bfloat162 p1 = __floats2bfloat162_rn(x[2], x[3]);
+            __nv_bfloat162 p2 = __floats2bfloat162_rn(x[4], x[5]);
+            __nv_bfloat162 p3 = __floats2bfloat162_rn(x[6], x[7]);
+            uint4 u;
+            u.x = *reinterpret_cast<uint32_t*>(&p0);
+            u.y = *reinterpret_cast<uint32_t*>(&p1);
+            u.z = *reinterpret_cast<uint32_t*>(&p2);
+            u.w = *reinterpret_cast<uint32_t*>(&p3);
+            *reinterpret_cast<uint4*>(sA + canon_off(tid, c0 + q * 8, a.hidden)) = u;
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      err = __syncthreads_or(err);
+    }
+  }
+  // drain: the last commits on the stage barriers must complete before the CTA exits
+  if (tid == 0 && !err) {
+    for (int s = 0; s < 2; ++s)
+      if (stage_busy[s]) {
+        if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
+        ph_free[s] ^= 1;
+      }
+  }
+  if (err && tid == 0 && a.error) atomicExch(a.error, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+}
+
+}  // namespace tng

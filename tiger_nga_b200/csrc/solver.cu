@@ -36,6 +36,8 @@ static BdfCoef make_coef() {
 struct SubstepKey {
   const double* state;
   int64_t ncells, ld;
+  const int* list;
+  const int* nlist;
   const double* dts;
   double dt, p;
   int warps, budget, passes;
@@ -48,13 +50,15 @@ struct SubstepKey {
 struct SolverState {
   bool tables_ready = false;
   SvDev dev{};
-  int* d_int = nullptr;
+  int* d_int = nullptr;  // hot ints then cold ints
   double* d_dbl = nullptr;
   int rs = 0, smem_warp = 0;
   DevBuf queue[2], counters, save, resume, nst, nni, nje, status, stats;
   size_t cap = 0;
-  cudaGraphExec_t graph = nullptr;
-  SubstepKey key{};
+  static constexpr int kGraphs = 4;  // a few argument sets alternate (e.g. fallback list and judge sample)
+  cudaGraphExec_t graph[kGraphs] = {};
+  SubstepKey key[kGraphs] = {};
+  int next_slot = 0;
   int warps = 0, blocks = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -62,7 +66,8 @@ struct SolverState {
 void solver_release(tng_chem* h) {
   SolverState* s = h->solver;
   if (!s) return;
-  if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (auto& g : s->graph)
+    if (g) cudaGraphExecDestroy(g);
   if (s->d_int) cudaFree(s->d_int);
   if (s->d_dbl) cudaFree(s->d_dbl);
   for (DevBuf* b : {&s->queue[0], &s->queue[1], &s->counters, &s->save, &s->resume, &s->nst, &s->nni, &s->nje,
@@ -78,15 +83,22 @@ static int ensure_tables(tng_chem* h) {
   if (!h->solver) h->solver = new SolverState();
   SolverState* s = h->solver;
   if (s->tables_ready) return TNG_OK;
+  {
+    const BdfCoef coef = make_coef();
+    cudaError_t ce = cudaMemcpyToSymbol(c_bdf, &coef, sizeof(coef));
+    if (ce != cudaSuccess) return cuda_error(ce, "BDF coefficients");
+  }
   const MechOps* o = h->ops;
   const SvLayout& L = *o->sv_layout;
   cudaError_t e;
-  if ((e = cudaMalloc(&s->d_int, sizeof(int) * L.nint)) != cudaSuccess) return cuda_error(e, "solver tables");
-  if ((e = cudaMalloc(&s->d_dbl, sizeof(double) * L.ndbl)) != cudaSuccess) return cuda_error(e, "solver tables");
-  cudaMemcpy(s->d_int, o->sv_int, sizeof(int) * L.nint, cudaMemcpyHostToDevice);
-  cudaMemcpy(s->d_dbl, o->sv_dbl[h->cfg.literal_mode], sizeof(double) * L.ndbl, cudaMemcpyHostToDevice);
-  s->dev.I = s->d_int;
-  s->dev.D = s->d_dbl;
+  if ((e = cudaMalloc(&s->d_int, sizeof(int) * (L.nhi + L.nci))) != cudaSuccess) return cuda_error(e, "solver tables");
+  if ((e = cudaMalloc(&s->d_dbl, sizeof(double) * L.nhd)) != cudaSuccess) return cuda_error(e, "solver tables");
+  cudaMemcpy(s->d_int, o->sv_hi, sizeof(int) * L.nhi, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->d_int + L.nhi, o->sv_ci, sizeof(int) * L.nci, cudaMemcpyHostToDevice);
+  cudaMemcpy(s->d_dbl, o->sv_hd[h->cfg.literal_mode], sizeof(double) * L.nhd, cudaMemcpyHostToDevice);
+  s->dev.hd = s->d_dbl;
+  s->dev.hi = s->d_int;
+  s->dev.ci = s->d_int + L.nhi;
   s->dev.L = L;
   const int nv = L.size[SZ_NV];
   s->rs = (nv % 2 == 0) ? nv + 1 : nv;
@@ -111,9 +123,13 @@ static BdfKernel bdf_kernel(int warps) {
   }
 }
 
+static size_t block_smem(const SolverState* s, int warps) {
+  return ((size_t)hot_smem_doubles(s->dev.L) + (size_t)warps * s->smem_warp) * sizeof(double);
+}
+
 static int configure_kernel(tng_chem* h, int warps, int* blocks_out) {
   SolverState* s = h->solver;
-  const size_t smem = (size_t)warps * s->smem_warp * sizeof(double);
+  const size_t smem = block_smem(s, warps);
   BdfKernel k = bdf_kernel(warps);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
@@ -141,6 +157,24 @@ static __global__ void k_stats(const int* nst, const int* nni, const int* nje, c
   }
 }
 
+int solver_prepare(tng_chem* h) {
+  DeviceGuard g(h->cfg.device);
+  return ensure_tables(h);
+}
+
+void solver_thermo(tng_chem* h, const double** th, double* tmid) {
+  const SolverState* s = h->solver;
+  *th = s->dev.hd + s->dev.L.hd[HD_TH];
+  const int lm = h->cfg.literal_mode;
+  *tmid = h->ops->sv_hd[lm][h->ops->sv_layout->hd[HD_SCAL] + SC_TMID];
+}
+
+// The implicit substep over ncells cells of a device state, or over the cells listed in
+// list[0 .. *nlist) (device pointers; *nlist read on the device) when list is non-null.
+int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
+                int flags, const int* list, const int* nlist, int* cell_nst, int* cell_nni, int* cell_status,
+                tng_substep_stats* stats);
+
 }  // namespace tng
 
 using namespace tng;
@@ -148,6 +182,15 @@ using namespace tng;
 extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt,
                                  double p, int flags, int* cell_nst, int* cell_nni, int* cell_status,
                                  tng_substep_stats* stats) {
+  return tng::substep_run(h, state, ncells, ld, dts, dt, p, flags, nullptr, nullptr, cell_nst, cell_nni, cell_status,
+                          stats);
+}
+
+namespace tng {
+
+int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
+                int flags, const int* list, const int* nlist, int* cell_nst, int* cell_nni, int* cell_status,
+                tng_substep_stats* stats) {
   if (!h) return set_error(TNG_ERR_ARG, "tng_substep_batch: null handle");
   if (ncells < 0 || ld < ncells) return set_error(TNG_ERR_ARG, "tng_substep_batch: need 0 <= ncells <= ld");
   if (ncells > (int64_t)0x7fffffff) return set_error(TNG_ERR_ARG, "tng_substep_batch: at most 2^31-1 cells");
@@ -185,7 +228,7 @@ extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int
   // scratch
   const int budget = h->cfg.pass_budget > 0 ? h->cfg.pass_budget : 0x7fffffff;
   const int passes = budget == 0x7fffffff ? 1 : std::max(2, h->cfg.max_passes > 0 ? h->cfg.max_passes : 8);
-  const int warps = (h->cfg.solver_warps == 2 || h->cfg.solver_warps == 8) ? h->cfg.solver_warps : 4;
+  const int warps = (h->cfg.solver_warps == 2 || h->cfg.solver_warps == 4) ? h->cfg.solver_warps : 8;
   const int save_stride = ((kQmax + 2) * nv + 16 + 3) & ~3;
   bool ok = s->counters.reserve(64 * sizeof(int)) && s->queue[0].reserve(ncells * sizeof(int)) &&
             s->queue[1].reserve(ncells * sizeof(int)) && s->resume.reserve(ncells * sizeof(int)) &&
@@ -201,15 +244,20 @@ extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int
   int* nst = cell_nst ? cell_nst : (int*)s->nst.ptr;
   int* nni = cell_nni ? cell_nni : (int*)s->nni.ptr;
   int* sts = cell_status ? cell_status : (int*)s->status.ptr;
-  SubstepKey key{dstate, ncells, dld, ddts, dt, p, warps, budget, passes, nst, nni, sts};
-  if (!s->graph || !(s->key == key)) {
-    if (s->graph) {
-      cudaGraphExecDestroy(s->graph);
-      s->graph = nullptr;
+  if (list && flags != TNG_DEVICE_PTRS) return set_error(TNG_ERR_ARG, "substep: cell lists need device pointers");
+  SubstepKey key{dstate, ncells, dld, list, nlist, ddts, dt, p, warps, budget, passes, nst, nni, sts};
+  int slot = -1;
+  for (int i = 0; i < SolverState::kGraphs; ++i)
+    if (s->graph[i] && s->key[i] == key) slot = i;
+  if (slot < 0) {
+    slot = s->next_slot;
+    s->next_slot = (s->next_slot + 1) % SolverState::kGraphs;
+    if (s->graph[slot]) {
+      cudaGraphExecDestroy(s->graph[slot]);
+      s->graph[slot] = nullptr;
     }
     BdfLaunch L;
     std::memset(&L, 0, sizeof(L));
-    L.c = make_coef();
     BdfArgs& a = L.a;
     a.tab = s->dev;
     a.state = dstate;
@@ -233,7 +281,7 @@ extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int
     a.smem_warp = s->smem_warp;
     a.rs = s->rs;
     int* cnt = (int*)s->counters.ptr;  // [0..1] heads, [2..3] out counts
-    const size_t smem = (size_t)warps * s->smem_warp * sizeof(double);
+    const size_t smem = block_smem(s, warps);
     cudaStream_t st = h->stream;
     cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     cudaMemsetAsync(s->resume.ptr, 0, ncells * sizeof(int), st);
@@ -242,30 +290,36 @@ extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int
       a.head = cnt + cur;
       a.n_out = cnt + 2 + cur;
       k_reset_counters<<<1, 32, 0, st>>>(a.head, a.n_out);
-      a.queue_in = pass == 0 ? nullptr : (const int*)s->queue[cur ^ 1].ptr;
+      a.queue_in = pass == 0 ? list : (const int*)s->queue[cur ^ 1].ptr;
       a.queue_out = (int*)s->queue[cur].ptr;
       a.n_in = (int)ncells;
-      L.n_in_dev = pass == 0 ? nullptr : cnt + 2 + (cur ^ 1);
+      L.n_in_dev = pass == 0 ? nlist : cnt + 2 + (cur ^ 1);
       a.budget = pass == passes - 1 ? 0x7fffffff : budget;
       bdf_kernel(warps)<<<s->blocks, warps * 32, smem, st>>>(L);
     }
     cudaGraph_t graph;
     e = cudaStreamEndCapture(st, &graph);
     if (e != cudaSuccess) return cuda_error(e, "solver graph capture");
-    e = cudaGraphInstantiate(&s->graph, graph, 0);
+    e = cudaGraphInstantiate(&s->graph[slot], graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return cuda_error(e, "solver graph instantiate");
-    s->key = key;
+    s->key[slot] = key;
   }
   cudaEventRecord(s->ev0, h->stream);
-  if ((e = cudaGraphLaunch(s->graph, h->stream)) != cudaSuccess) return cuda_error(e, "solver graph launch");
+  if ((e = cudaGraphLaunch(s->graph[slot], h->stream)) != cudaSuccess) return cuda_error(e, "solver graph launch");
   cudaEventRecord(s->ev1, h->stream);
   if (flags == TNG_HOST_PTRS) {
     e = cudaMemcpy2DAsync(state, ld * sizeof(double), dstate, ncells * sizeof(double), ncells * sizeof(double), nv,
                           cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_error(e, "state device->host");
   }
-  if (stats) {
+  if (stats && list) {
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_error(e, "implicit substep");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    stats->passes = passes;
+    stats->ms = ms;
+  } else if (stats) {
     unsigned long long* acc = (unsigned long long*)s->stats.ptr;
     cudaMemsetAsync(acc, 0, 32 * sizeof(unsigned long long), h->stream);
     k_stats<<<std::min<int64_t>(1184, (ncells + 255) / 256), 256, 0, h->stream>>>(nst, nni, (int*)s->nje.ptr, sts,
@@ -294,6 +348,8 @@ extern "C" int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int
   return TNG_OK;
 }
 
+}  // namespace tng
+
 extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,
                                   double* jac) {
   if (!h || !state || !rhs) return set_error(TNG_ERR_ARG, "tng_solver_rhs_jac: null argument");
@@ -302,7 +358,7 @@ extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncel
   int rc = ensure_tables(h);
   if (rc) return rc;
   SolverState* s = h->solver;
-  const size_t smem = (size_t)4 * s->smem_warp * sizeof(double);
+  const size_t smem = block_smem(s, 4);
   cudaError_t e = cudaFuncSetAttribute(k_warp_rhs_jac<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   const int blocks = (int)std::min<int64_t>((ncells + 3) / 4, 148 * 8);

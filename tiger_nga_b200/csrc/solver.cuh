@@ -32,13 +32,36 @@ namespace tng {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kQmax = 5;
 
+// Table view inside a kernel: hot tables in shared memory (staged per block), cold tables and
+// the layout in global/parameter space.
 struct SvDev {
-  const int* __restrict__ I;
-  const double* __restrict__ D;
+  const double* __restrict__ hd;  // hot doubles (shared memory once staged)
+  const int* __restrict__ hi;     // hot ints (shared memory once staged)
+  const int* __restrict__ ci;     // cold ints (global, read through L1)
   SvLayout L;
-  __device__ __forceinline__ const int* ip(int k) const { return I + L.ioff[k]; }
-  __device__ __forceinline__ const double* dp(int k) const { return D + L.doff[k]; }
+  __device__ __forceinline__ const double* d(int k) const { return hd + L.hd[k]; }
+  __device__ __forceinline__ const int* i(int k) const { return hi + L.hi[k]; }
+  __device__ __forceinline__ const int* c(int k) const { return ci + L.ci[k]; }
 };
+
+// Copy the hot tables from global memory into the block's shared memory (all threads).
+__device__ __forceinline__ SvDev stage_tables(const SvDev& g, void* smem) {
+  double* d = reinterpret_cast<double*>(smem);
+  int* i = reinterpret_cast<int*>(d + g.L.nhd);
+  const double2* gs = reinterpret_cast<const double2*>(g.hd);
+  double2* ds = reinterpret_cast<double2*>(d);
+  for (int e = threadIdx.x; e < g.L.nhd / 2; e += blockDim.x) ds[e] = gs[e];
+  const int4* gi = reinterpret_cast<const int4*>(g.hi);
+  int4* di = reinterpret_cast<int4*>(i);
+  for (int e = threadIdx.x; e < g.L.nhi / 4; e += blockDim.x) di[e] = gi[e];
+  __syncthreads();
+  SvDev t = g;
+  t.hd = d;
+  t.hi = i;
+  return t;
+}
+
+__host__ __device__ inline int hot_smem_bytes(const SvLayout& L) { return L.nhd * 8 + L.nhi * 4; }
 
 // status codes per cell
 enum { ST_OK = 0, ST_MAXSTEPS = 1, ST_CONVFAIL = 2, ST_ERRFAIL = 3, ST_NONFINITE = 4, ST_HMIN = 5, ST_PENDING = 9 };
@@ -72,7 +95,7 @@ struct BdfArgs {
 // shared-memory regions of one warp (offsets in doubles)
 struct WarpMem {
   double* mat;  // NV x rs
-  double* W;    // nslot: rates (RHS) or rate constants (Jacobian)
+  double* W;    // nslot: rates (RHS) or rate constants (Jacobian), by processing position
   double* C;    // 64 concentrations
   double* Ms;   // nm third-body sums
   double* lcm;  // nm log concentration for falloff
@@ -80,8 +103,8 @@ struct WarpMem {
   double* part; // ncdchunk partial production rates
   double* G;    // ngpair
   double* vb;   // 64 vector buffer
-  double* hb;   // 64 enthalpies / heat capacities scratch
-  double* cb;   // 64
+  double* hb;   // 64 enthalpies
+  double* cb;   // 64 heat capacities
   int* piv;     // 64 pivots
 };
 
@@ -116,13 +139,15 @@ __device__ __forceinline__ double warp_sum(double v) {
   return __shfl_sync(kFull, v, 0);
 }
 
-__device__ __forceinline__ double expo(const double lnA, const double n, const double E, const int fl, const double LT,
+__device__ __forceinline__ double expo(const double lnA, const double E, const double n, const int fl, const double LT,
                                        const double invRT) {
   double e = lnA;
   if (fl & 4) e = fma(E, invRT, e);
   if (fl & 2) e = fma(n, LT, e);
   return e;
 }
+
+__device__ __forceinline__ int nu_of(const int term) { return (int)(int8_t)(term & 0xFF); }
 
 // Per-cell thermochemical state shared by the rate and Jacobian evaluations.
 struct CellPrep {
@@ -134,8 +159,8 @@ struct CellPrep {
 __device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, const double y0, const double y1,
                                            const double p, const int lane) {
   const int ns = t.L.size[SZ_NS], nv = ns + 1, nm = t.L.size[SZ_NM], nfc = t.L.size[SZ_NFC];
-  const double* sc = t.dp(D_SCAL);
-  const double* invw = t.dp(D_INVW);
+  const double* sc = t.d(HD_SCAL);
+  const double* invw = t.d(HD_INVW);
   if (lane < nv) w.vb[lane] = y0;
   if (lane + 32 < nv) w.vb[lane + 32] = y1;
   CellPrep c;
@@ -150,25 +175,24 @@ __device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, co
   if (lane + 32 < ns) w.C[lane + 32] = y1 * invw[lane + 32];
   __syncwarp();
   const double lnprt = log(p * c.invRT);
-  const int* tbp = t.ip(I_TB_PTR);
-  const int* tbs = t.ip(I_TB_SP);
-  const double* tbc = t.dp(D_TB_COEF);
+  const double* eff = t.d(HD_EFF);
   for (int m = lane; m < nm; m += 32) {
-    const int b = tbp[m], e = tbp[m + 1];
-    double acc = tbc[b] == 1.0 ? w.C[tbs[b]] : tbc[b] * w.C[tbs[b]];
-    for (int q = b + 1; q < e; ++q) acc = tbc[q] == 1.0 ? acc + w.C[tbs[q]] : fma(tbc[q], w.C[tbs[q]], acc);
+    const double* e = eff + m * ns;
+    double acc = 0.0;
+    for (int j = 0; j < ns; ++j) acc = fma(e[j], w.C[j], acc);
     w.Ms[m] = acc;
     w.lcm[m] = acc > 0.0 ? log(acc) : lnprt;
   }
-  const int* fcf = t.ip(I_FC_FORM);
-  const double* fca = t.dp(D_FC_A);
-  const double* fcc = t.dp(D_FC_C);
+  const int* fcf = t.i(HI_FC);
+  const double* fcd = t.d(HD_FC);
   for (int f = lane; f < nfc; f += 32) {
+    const int forms = fcf[f];
     double v = 0.0;
+#pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const int form = fcf[3 * f + q];
-      if (form < 0) break;
-      const double a = fca[3 * f + q], cc = fcc[3 * f + q];
+      const int form = (forms >> (4 * q)) & 15;
+      if (form == 15) break;
+      const double a = fcd[6 * f + 2 * q], cc = fcd[6 * f + 2 * q + 1];
       const double term = form == 2 ? a : (form == 0 ? a * exp(-c.T * cc) : a * exp(-cc * c.invT));
       v = q == 0 ? term : v + term;
     }
@@ -182,69 +206,73 @@ __device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, co
   return c;
 }
 
-// Rate constant of slot r (GETLINDRATECOEFF-equivalent for falloff slots); also returns ln Pr.
-__device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, const CellPrep& c, const int r,
-                                            double* lpr_out) {
-  const int fl = t.ip(I_SLOT_FLAGS)[r];
+// Rate constant of the slot at position p (GETLINDRATECOEFF-equivalent for falloff slots);
+// also returns ln Pr for falloff slots.
+__device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, const CellPrep& c, const int p,
+                                            const int w0, const int w1, double* lpr_out) {
+  const int fl = w0 & 15;
   if (fl & 1) {
-    const int f = t.ip(I_SLOT_FO)[r];
-    const double* par = t.dp(D_FO_PAR) + 6 * f;
-    const int* ffl = t.ip(I_FO_FLAGS) + 2 * f;
-    const double* sc = t.dp(D_SCAL);
-    const double lk0 = expo(par[0], par[1], par[2], ffl[0], c.LT, c.invRT);
-    const double lki = expo(par[3], par[4], par[5], ffl[1], c.LT, c.invRT);
-    const double lpr = lk0 + w.lcm[t.ip(I_FO_M)[f]] - fmax(lki, sc[SC_LNKMIN]);
+    const int f = w1 >> 8;
+    const double* par = t.d(HD_FO) + 6 * f;
+    const int fw = t.i(HI_FO)[f];
+    const double* sc = t.d(HD_SCAL);
+    const double lk0 = expo(par[0], par[1], par[2], fw & 15, c.LT, c.invRT);
+    const double lki = expo(par[3], par[4], par[5], (fw >> 4) & 15, c.LT, c.invRT);
+    const double lpr = lk0 + w.lcm[fw >> 16] - fmax(lki, sc[SC_LNKMIN]);
     if (lpr_out) *lpr_out = lpr;
     const double pr = exp(lpr);
-    const int fid = t.ip(I_FO_FC)[f];
+    const int fid = ((fw >> 8) & 255) - 1;
     if (fid < 0) return exp(lki) * pr / (1.0 + pr);
     const double lg = lpr * sc[SC_INVLN10] + w.fc[3 * fid + 2];
     const double ff = lg / (w.fc[3 * fid + 1] - sc[SC_TD] * lg);
     return exp(lki + w.fc[3 * fid] / (ff * ff + 1.0)) * pr / (1.0 + pr);
   }
-  if (fl & 8) return t.dp(D_SLOT_A)[r];
-  return exp(expo(t.dp(D_SLOT_LNA)[r], t.dp(D_SLOT_N)[r], t.dp(D_SLOT_E)[r], fl, c.LT, c.invRT));
+  const double* sd = t.d(HD_SLOT) + 4 * p;
+  if (fl & 8) return sd[0];
+  return exp(expo(sd[0], sd[1], sd[2], fl, c.LT, c.invRT));
 }
 
 // finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
-__device__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, const double y1, const double p,
-                         double& f0, double& f1, const int lane) {
+__device__ __forceinline__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+                                         const double p, double& f0, double& f1, const int lane) {
   const int ns = t.L.size[SZ_NS], nslot = t.L.size[SZ_NSLOT];
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
-  const int* reac = t.ip(I_SLOT_REAC);
-  const int* mw = t.ip(I_SLOT_MW);
-  for (int r = lane; r < nslot; r += 32) {
-    double v = rate_const(t, w, c, r, nullptr);
-    const int* rr = reac + 3 * r;
-    if (rr[0] >= 0) v = v * w.C[rr[0]];
-    if (rr[1] >= 0) v = v * w.C[rr[1]];
-    if (rr[2] >= 0) v = v * w.C[rr[2]];
-    if (mw[r] >= 0) v = v * w.Ms[mw[r]];
-    w.W[r] = v;
+  const int* sw = t.i(HI_SLOT);
+  for (int q = lane; q < nslot; q += 32) {
+    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
+    double v = rate_const(t, w, c, q, w0, w1, nullptr);
+    const int r0 = (w0 >> 4) & 127, r1 = (w0 >> 11) & 127, r2 = (w0 >> 18) & 127, mw = w1 & 127;
+    if (r0 != kNone7) v = v * w.C[r0];
+    if (r1 != kNone7) v = v * w.C[r1];
+    if (r2 != kNone7) v = v * w.C[r2];
+    if (mw != kNone7) v = v * w.Ms[mw];
+    w.W[q] = v;
   }
   __syncwarp();
   {
-    const int* lp = t.ip(I_CD_LANE_PTR);
-    const int* ll = t.ip(I_CD_LANE_LIST);
-    const int* cb = t.ip(I_CD_CHUNK_BEG);
-    const int* ce = t.ip(I_CD_CHUNK_END);
-    const int* cs = t.ip(I_CD_SLOT);
-    const double* cn = t.dp(D_CD_NU);
+    const int* lp = t.i(HI_CD_LANE_PTR);
+    const int* ll = t.i(HI_CD_LANE_LIST);
+    const int* cb = t.i(HI_CD_BEG);
+    const int* ce = t.i(HI_CD_END);
+    const int* ct = t.i(HI_CD_TERM);
     for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
       const int ch = ll[i];
       double acc = 0.0;
       for (int q = cb[ch]; q < ce[ch]; ++q) {
-        const double nu = cn[q], wv = w.W[cs[q]];
-        acc = nu == 1.0 ? acc + wv : (nu == -1.0 ? acc - wv : fma(nu, wv, acc));
+        const int term = ct[q];
+        const int nu = nu_of(term);
+        const double wv = w.W[term >> 8];
+        acc = nu == 1 ? acc + wv : (nu == -1 ? acc - wv : fma((double)nu, wv, acc));
       }
       w.part[ch] = acc;
     }
   }
   __syncwarp();
-  const int* spp = t.ip(I_CD_SP_PTR);
-  const double* wm = t.dp(D_WMOL);
-  const double* sc = t.dp(D_SCAL);
-  const double* th = c.T > sc[SC_TMID] ? t.dp(D_TH_HI) : t.dp(D_TH_LO);
+  const int* spp = t.i(HI_CD_SP_PTR);
+  const double* wm = t.d(HD_WMOL);
+  const double* sc = t.d(HD_SCAL);
+  const int toff = c.T > sc[SC_TMID] ? 0 : 12;
+  const double* th = t.d(HD_TH);
   double cpm = 0.0, tmp = 0.0, r0 = 0.0, r1 = 0.0;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
@@ -252,7 +280,7 @@ __device__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, cons
     if (k < ns) {
       double cd = 0.0;
       for (int q = spp[k]; q < spp[k + 1]; ++q) cd += w.part[q];
-      const double* a = th + 12 * k;
+      const double* a = th + 24 * k + toff;
       const double T = c.T;
       const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
       const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
@@ -273,75 +301,79 @@ __device__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, cons
 
 // Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
 // row stride rs). Uses one extra right-hand side for the temperature column.
-__device__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const double y0, const double y1,
-                         const double f0, const double f1, const double p, const int lane) {
+__device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const double y0,
+                                         const double y1, const double f0, const double f1, const double p,
+                                         const int lane) {
   const int ns = t.L.size[SZ_NS], nv = ns + 1, nslot = t.L.size[SZ_NSLOT];
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
-  const int* reac = t.ip(I_SLOT_REAC);
-  const int* mw = t.ip(I_SLOT_MW);
-  for (int r = lane; r < nslot; r += 32) w.W[r] = rate_const(t, w, c, r, nullptr);
+  const int* sw = t.i(HI_SLOT);
+  for (int q = lane; q < nslot; q += 32) w.W[q] = rate_const(t, w, c, q, sw[2 * q], sw[2 * q + 1], nullptr);
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
-  // direct mass-action part: dW_r/dC_j for every reactant occurrence
+  // direct mass-action part: dW_p/dC_j for every reactant occurrence
   {
-    const int* lp = t.ip(I_JD_LANE_PTR);
-    const int* ll = t.ip(I_JD_LANE_LIST);
-    const int* tg = t.ip(I_JD_TGT);
-    const int* gb = t.ip(I_JD_BEG);
-    const int* ge = t.ip(I_JD_END);
-    const int* js = t.ip(I_JD_SLOT);
-    const int* jp = t.ip(I_JD_POS);
-    const double* jn = t.dp(D_JD_NU);
+    const int* lp = t.c(CI_JD_LANE_PTR);
+    const int* ll = t.c(CI_JD_LANE_LIST);
+    const int* tg = t.c(CI_JD_TGT);
+    const int* gb = t.c(CI_JD_BEG);
+    const int* ge = t.c(CI_JD_END);
+    const int* jt = t.c(CI_JD_TERM);
     for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
       const int g = ll[i];
       double acc = 0.0;
       for (int q = gb[g]; q < ge[g]; ++q) {
-        const int r = js[q], pos = jp[q];
-        double d = w.W[r];
-        if (mw[r] >= 0) d *= w.Ms[mw[r]];
-        const int* rr = reac + 3 * r;
+        const int term = jt[q];
+        const int pp = term >> 12, rp = (term >> 8) & 15;
+        const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
+        double d = w.W[pp];
+        const int mw = w1 & 127;
+        if (mw != kNone7) d *= w.Ms[mw];
 #pragma unroll
-        for (int o = 0; o < 3; ++o)
-          if (o != pos && rr[o] >= 0) d *= w.C[rr[o]];
-        acc = fma(jn[q], d, acc);
+        for (int o = 0; o < 3; ++o) {
+          const int r = (w0 >> (4 + 7 * o)) & 127;
+          if (o != rp && r != kNone7) d *= w.C[r];
+        }
+        acc = fma((double)nu_of(term), d, acc);
       }
       const int tgt = tg[g];
       w.mat[(tgt / nv) * rs + tgt % nv] = acc;
     }
   }
-  // third-body and falloff-[M] part: G[i][m] = sum_r nu_ir dW_r/dM_m
+  // third-body and falloff-[M] part: G[i][m] = sum_p nu_ip dW_p/dM_m
   {
-    const int* lp = t.ip(I_G_LANE_PTR);
-    const int* ll = t.ip(I_G_LANE_LIST);
-    const int* gb = t.ip(I_G_BEG);
-    const int* ge = t.ip(I_G_END);
-    const int* gs = t.ip(I_G_SLOT);
-    const int* gk = t.ip(I_G_KIND);
-    const double* gn = t.dp(D_G_NU);
+    const int* lp = t.c(CI_G_LANE_PTR);
+    const int* ll = t.c(CI_G_LANE_LIST);
+    const int* gb = t.c(CI_G_BEG);
+    const int* ge = t.c(CI_G_END);
+    const int* gt = t.c(CI_G_TERM);
     for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
       const int g = ll[i];
       double acc = 0.0;
       for (int q = gb[g]; q < ge[g]; ++q) {
-        const int r = gs[q];
-        const int* rr = reac + 3 * r;
+        const int term = gt[q];
+        const int pp = term >> 12, kind = (term >> 8) & 15;
+        const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
         double prodC = 1.0;
 #pragma unroll
-        for (int o = 0; o < 3; ++o)
-          if (rr[o] >= 0) prodC *= w.C[rr[o]];
+        for (int o = 0; o < 3; ++o) {
+          const int r = (w0 >> (4 + 7 * o)) & 127;
+          if (r != kNone7) prodC *= w.C[r];
+        }
         double val = 0.0;
-        if (gk[q] == 0) {
-          val = w.W[r] * prodC;
+        if (kind == 0) {
+          val = w.W[pp] * prodC;
         } else {
-          const int f = t.ip(I_SLOT_FO)[r];
-          const double Mf = w.Ms[t.ip(I_FO_M)[f]];
+          const int fw = t.i(HI_FO)[w1 >> 8];
+          const double Mf = w.Ms[fw >> 16];
           if (Mf > 0.0) {
             double lpr;
-            rate_const(t, w, c, r, &lpr);
+            rate_const(t, w, c, pp, w0, w1, &lpr);
             const double pr = exp(lpr);
-            val = w.W[r] / (Mf * (1.0 + pr)) * prodC * (mw[r] >= 0 ? w.Ms[mw[r]] : 1.0);
+            const int mw = w1 & 127;
+            val = w.W[pp] / (Mf * (1.0 + pr)) * prodC * (mw != kNone7 ? w.Ms[mw] : 1.0);
           }
         }
-        acc = fma(gn[q], val, acc);
+        acc = fma((double)nu_of(term), val, acc);
       }
       w.G[g] = acc;
     }
@@ -349,9 +381,9 @@ __device__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const d
   __syncwarp();
   {
     const int ng = t.L.size[SZ_NGPAIR];
-    const int* gi = t.ip(I_G_I);
-    const int* gm = t.ip(I_G_M);
-    const double* eff = t.dp(D_EFF);
+    const int* gi = t.c(CI_G_I);
+    const int* gm = t.c(CI_G_M);
+    const double* eff = t.d(HD_EFF);
     for (int j = lane; j < ns; j += 32)
       for (int g = 0; g < ng; ++g) {
         const double v = w.G[g];
@@ -371,20 +403,21 @@ __device__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const d
   if (lane + 32 < nv) w.mat[(lane + 32) * rs + ns] = (g1 - f1) * idl;
   __syncwarp();
   // species columns
-  const double* wm = t.dp(D_WMOL);
+  const double* wm = t.d(HD_WMOL);
   for (int e = lane; e < ns * ns; e += 32) {
     const int i = e / ns, j = e % ns;
     w.mat[i * rs + j] = wm[i] * w.mat[i * rs + j] / wm[j] - T * w.mat[i * rs + ns];
   }
   // temperature row
-  const double* sc = t.dp(D_SCAL);
-  const double* th = T > sc[SC_TMID] ? t.dp(D_TH_HI) : t.dp(D_TH_LO);
+  const double* sc = t.d(HD_SCAL);
+  const int toff = T > sc[SC_TMID] ? 0 : 12;
+  const double* th = t.d(HD_TH);
   double cpm = 0.0, ydcp = 0.0, scp = 0.0;
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     const int k = lane + 32 * half;
     if (k < ns) {
-      const double* a = th + 12 * k;
+      const double* a = th + 24 * k + toff;
       const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
       const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
       const double dcp = a[0] * (a[8] + T * (2.0 * a[9] + T * (3.0 * a[10] + T * (4.0 * a[11]))));
@@ -414,7 +447,7 @@ __device__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const d
 
 // In-place LU with partial pivoting (first maximum) of the n x n matrix a (row stride rs).
 // Returns nonzero if a pivot is zero or not finite.
-__device__ int lu_warp(double* a, const int n, const int rs, int* piv, const int lane) {
+__device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int* piv, const int lane) {
   int sing = 0;
   const int lr = lane >> 3, lc = lane & 7;
   for (int k = 0; k < n; ++k) {
@@ -466,7 +499,7 @@ __device__ int lu_warp(double* a, const int n, const int rs, int* piv, const int
 }
 
 // Solve (LU) x = b in place; b in shared memory.
-__device__ void lu_solve_warp(const double* a, const int n, const int rs, const int* piv, double* b, const int lane) {
+__device__ __forceinline__ void lu_solve_warp(const double* a, const int n, const int rs, const int* piv, double* b, const int lane) {
   if (lane == 0)
     for (int k = 0; k < n; ++k) {
       const int p = piv[k];

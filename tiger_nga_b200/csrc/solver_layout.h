@@ -1,26 +1,34 @@
-// Layout of the generated solver tables (see tiger_nga_b200/codegen.py: solver_tables).
+// Layout of the generated solver tables (tiger_nga_b200/codegen.py: solver_tables).
+// Hot tables (everything the right-hand side reads) are staged into shared memory per block;
+// cold tables (the Jacobian's work lists) are read from global memory through L1. All tables
+// are indexed by the slot's processing position p (falloff, exponential, constant).
 #pragma once
 
 namespace tng {
 
 enum SvSize { SZ_NS, SZ_NV, SZ_NSLOT, SZ_NM, SZ_NFO, SZ_NFC, SZ_NCDCHUNK, SZ_NJDGRP, SZ_NGPAIR, SZ_COUNT };
-enum SvInt {
-  I_SLOT_FLAGS, I_SLOT_REAC, I_SLOT_MW, I_SLOT_FO, I_FO_FLAGS, I_FO_FC, I_FO_M, I_FC_FORM, I_TB_PTR, I_TB_SP,
-  I_CD_LANE_PTR, I_CD_LANE_LIST, I_CD_CHUNK_BEG, I_CD_CHUNK_END, I_CD_SLOT, I_CD_SP_PTR,
-  I_JD_LANE_PTR, I_JD_LANE_LIST, I_JD_TGT, I_JD_BEG, I_JD_END, I_JD_SLOT, I_JD_POS,
-  I_G_LANE_PTR, I_G_LANE_LIST, I_G_I, I_G_M, I_G_BEG, I_G_END, I_G_SLOT, I_G_KIND, I_COUNT
-};
-enum SvDbl {
-  D_SLOT_A, D_SLOT_LNA, D_SLOT_N, D_SLOT_E, D_FO_PAR, D_FC_A, D_FC_C, D_TB_COEF, D_EFF, D_CD_NU, D_JD_NU, D_G_NU,
-  D_TH_HI, D_TH_LO, D_WMOL, D_INVW, D_SCAL, D_COUNT
+// hot doubles: slot records (4 per slot: lnA|A, E, n, -), falloff (6: lnA0 E0 n0 lnAi Ei ni),
+// F_cent (6: a0 c0 a1 c1 a2 c2), dense efficiencies (nm x ns), thermo (ns x 24: hi 12, lo 12),
+// molar masses, their inverses, scalars
+enum SvHd { HD_SLOT, HD_FO, HD_FC, HD_EFF, HD_TH, HD_WMOL, HD_INVW, HD_SCAL, HD_COUNT };
+// hot ints: slot words (2 per slot: flags|r0<<4|r1<<11|r2<<18, mw|fo<<8), falloff word
+// (f0|f1<<4|(fc+1)<<8|m<<16), F_cent forms, production-rate chunk lists (terms p<<8|nu)
+enum SvHi { HI_SLOT, HI_FO, HI_FC, HI_CD_LANE_PTR, HI_CD_LANE_LIST, HI_CD_BEG, HI_CD_END, HI_CD_SP_PTR, HI_CD_TERM, HI_COUNT };
+// cold ints: Jacobian direct groups (terms p<<12|reactant position<<8|nu) and third-body pairs
+// (terms p<<12|kind<<8|nu)
+enum SvCi {
+  CI_JD_LANE_PTR, CI_JD_LANE_LIST, CI_JD_TGT, CI_JD_BEG, CI_JD_END, CI_JD_TERM,
+  CI_G_LANE_PTR, CI_G_LANE_LIST, CI_G_I, CI_G_M, CI_G_BEG, CI_G_END, CI_G_TERM, CI_COUNT
 };
 enum SvScal { SC_RGAS, SC_TMID, SC_TN0, SC_TN1, SC_TC0, SC_TC1, SC_TD, SC_LNKMIN, SC_INVLN10 };
+constexpr int kNone7 = 127;
 
 struct SvLayout {
   int size[SZ_COUNT];
-  int ioff[I_COUNT];
-  int doff[D_COUNT];
-  int nint, ndbl;
+  int hd[HD_COUNT];
+  int hi[HI_COUNT];
+  int ci[CI_COUNT];
+  int nhd, nhi, nci;
 };
 
 }  // namespace tng

@@ -1,0 +1,791 @@
+// The surrogate substep: features and targets from implicit-solver pairs, normalisation,
+// training (mlp.cu), BF16 weight packing, tensor-core inference (mlp_infer.cuh), the FP64
+// conservation/renormalisation post-processing with fallback flags, the implicit fallback solve
+// and the held-out judge. C-ABI tng_surrogate_* and tng_substep_surrogate.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "mlp.h"
+#include "mlp_infer.cuh"
+#include "solver.cuh"
+#include "tiger_chem.h"
+#include "tng_runtime.h"
+
+namespace tng {
+
+constexpr int kMaxNs = 64;
+constexpr int kMaxEl = 8;
+
+struct SurPost {
+  double* state;
+  long long ld;
+  int ncells;
+  const double* dts;
+  double dt_scalar;
+  double logp;
+  int ns, bath, n_in, n_out, out_pad, nel;
+  const float* out;      // network outputs, normalised
+  const double* tmean;   // target mean/std, n_out
+  const double* tstd;
+  const float* fmin;     // raw-feature training range, n_in
+  const float* fmax;
+  double margin, consist_tol, clip_tol;
+  const double* E;   // nel x ns: element atoms per kg of species (a_ek / W_k)
+  const double* th;  // ns x 24 NASA (hi 12, lo 12)
+  double tmid;
+  int* fb_list;      // fallback cells
+  int* fb_count;
+  unsigned long long* cnt;  // [accepted, ood, consistency, clip]
+};
+
+__device__ __forceinline__ void nasa(const double* th, double tmid, int k, double T, double* h, double* cp) {
+  const double* a = th + 24 * k + (T > tmid ? 0 : 12);
+  *cp = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
+  *h = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
+}
+
+// raw features of one cell (same formulas as the inference kernel's featurisation)
+__device__ __forceinline__ int raw_features(const double* state, long long ld, int cell, int ns, int bath, double logp,
+                                            double dt, float* f, double* rho_out, double* T_out) {
+  double rho = 0.0;
+  for (int k = 0; k < ns; ++k) rho += state[(long long)k * ld + cell];
+  const double T = state[(long long)ns * ld + cell] / rho;
+  f[0] = (float)T;
+  f[1] = (float)logp;
+  int j = 2;
+  for (int k = 0; k < ns; ++k) {
+    if (k == bath) continue;
+    f[j++] = (float)log10(fmax(state[(long long)k * ld + cell] / rho, 1e-30));
+  }
+  f[j++] = (float)log10(fmax(dt, 1e-30));
+  *rho_out = rho;
+  *T_out = T;
+  return j;
+}
+
+__global__ void k_sur_features(const double* __restrict__ state, long long ld, int n, const double* __restrict__ dts,
+                               double logp, int ns, int bath, int in_pad, float* __restrict__ X) {
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n; cell += gridDim.x * blockDim.x) {
+    float f[kMaxNs + 4];
+    double rho, T;
+    const int nf = raw_features(state, ld, cell, ns, bath, logp, dts[cell], f, &rho, &T);
+    for (int i = 0; i < in_pad; ++i) X[(size_t)cell * in_pad + i] = i < nf ? f[i] : 0.f;
+  }
+}
+
+// targets (dT, dY_k) of a pair, FP64 then stored as float
+__global__ void k_sur_targets(const double* __restrict__ s0, const double* __restrict__ s1, long long ld, int n,
+                              int ns, int out_pad, float* __restrict__ Tt) {
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n; cell += gridDim.x * blockDim.x) {
+    double r0 = 0.0, r1 = 0.0;
+    for (int k = 0; k < ns; ++k) {
+      r0 += s0[(long long)k * ld + cell];
+      r1 += s1[(long long)k * ld + cell];
+    }
+    float* t = Tt + (size_t)cell * out_pad;
+    t[0] = (float)(s1[(long long)ns * ld + cell] / r1 - s0[(long long)ns * ld + cell] / r0);
+    for (int k = 0; k < ns; ++k)
+      t[1 + k] = (float)(s1[(long long)k * ld + cell] / r1 - s0[(long long)k * ld + cell] / r0);
+    for (int i = ns + 1; i < out_pad; ++i) t[i] = 0.f;
+  }
+}
+
+// per-column FP64 sum, sum of squares, min, max over rows (one block per column, fixed order)
+__global__ void k_colstats(const float* __restrict__ A, int rows, int ld, double* __restrict__ out) {
+  __shared__ double s1[256], s2[256], mn[256], mx[256];
+  const int c = blockIdx.x;
+  double a = 0.0, b = 0.0, lo = 1e300, hi = -1e300;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const double v = A[(size_t)r * ld + c];
+    a += v;
+    b += v * v;
+    lo = fmin(lo, v);
+    hi = fmax(hi, v);
+  }
+  s1[threadIdx.x] = a, s2[threadIdx.x] = b, mn[threadIdx.x] = lo, mx[threadIdx.x] = hi;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if (threadIdx.x < off) {
+      s1[threadIdx.x] += s1[threadIdx.x + off];
+      s2[threadIdx.x] += s2[threadIdx.x + off];
+      mn[threadIdx.x] = fmin(mn[threadIdx.x], mn[threadIdx.x + off]);
+      mx[threadIdx.x] = fmax(mx[threadIdx.x], mx[threadIdx.x + off]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[4 * c] = s1[0], out[4 * c + 1] = s2[0], out[4 * c + 2] = mn[0], out[4 * c + 3] = mx[0];
+  }
+}
+
+// A[r][c] = (A[r][c] - mean[c]) * scale[c] for c < ncol, 0 beyond
+__global__ void k_normalise(float* __restrict__ A, int rows, int ld, int ncol, const float* __restrict__ mean,
+                            const float* __restrict__ scale) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < (int64_t)rows * ld;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(e % ld);
+    A[e] = c < ncol ? (A[e] - mean[c]) * scale[c] : 0.f;
+  }
+}
+
+// FP32 parameters -> BF16 chunked canonical K-major layout of the inference kernel
+__global__ void k_pack_weights(const float* __restrict__ W, int fo, int fi, __nv_bfloat16* __restrict__ dst) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < fo * fi; e += gridDim.x * blockDim.x) {
+    const int n = e / fi, k = e % fi;
+    const int c = k / kWChunkK, kk = k % kWChunkK;
+    const int kc = min(kWChunkK, fi - c * kWChunkK);
+    const int off = c * fo * kWChunkK + (int)(((n >> 3) * (kc * 16) + (kk >> 3) * 128 + (n & 7) * 16 + (kk & 7) * 2) / 2);
+    dst[off] = __float2bfloat16_rn(W[e]);
+  }
+}
+
+__device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// prediction -> state with conservation; fallback cells keep their state and are listed
+__global__ void k_sur_post(const SurPost a) {
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells; cell += gridDim.x * blockDim.x) {
+    const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
+    float f[kMaxNs + 4];
+    double rho, T0;
+    raw_features(a.state, a.ld, cell, a.ns, a.bath, a.logp, dt, f, &rho, &T0);
+    int reason = 0;
+    for (int i = 0; i < a.n_in && !reason; ++i) {
+      const float span = a.fmax[i] - a.fmin[i];
+      if (f[i] < a.fmin[i] - a.margin * span || f[i] > a.fmax[i] + a.margin * span) reason = 1;
+    }
+    double Y0[kMaxNs], dY[kMaxNs], D[kMaxNs];
+    const float* o = a.out + (size_t)cell * a.out_pad;
+    const double dT = (double)o[0] * a.tstd[0] + a.tmean[0];
+    for (int k = 0; k < a.ns; ++k) {
+      Y0[k] = a.state[(long long)k * a.ld + cell] / rho;
+      dY[k] = (double)o[1 + k] * a.tstd[1 + k] + a.tmean[1 + k];
+      D[k] = fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12;
+    }
+    // element conservation: minimise sum dY'^2/D subject to E dY' = 0 (normal equations, nel <= 8)
+    double G[kMaxEl][kMaxEl], r[kMaxEl];
+    for (int e = 0; e < a.nel; ++e) {
+      r[e] = 0.0;
+      for (int k = 0; k < a.ns; ++k) r[e] += a.E[e * a.ns + k] * dY[k];
+      for (int g = 0; g <= e; ++g) {
+        double s = 0.0;
+        for (int k = 0; k < a.ns; ++k) s += a.E[e * a.ns + k] * D[k] * a.E[g * a.ns + k];
+        G[e][g] = G[g][e] = s;
+      }
+    }
+    // Cholesky solve G lam = r
+    double Lc[kMaxEl][kMaxEl];
+    bool spd = true;
+    for (int i = 0; i < a.nel; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double s = G[i][j];
+        for (int q = 0; q < j; ++q) s -= Lc[i][q] * Lc[j][q];
+        if (i == j) {
+          if (!(s > 0.0)) spd = false;
+          Lc[i][i] = sqrt(fmax(s, 1e-300));
+        } else {
+          Lc[i][j] = s / Lc[j][j];
+        }
+      }
+    double lam[kMaxEl];
+    for (int i = 0; i < a.nel; ++i) {
+      double s = r[i];
+      for (int q = 0; q < i; ++q) s -= Lc[i][q] * lam[q];
+      lam[i] = s / Lc[i][i];
+    }
+    for (int i = a.nel - 1; i >= 0; --i) {
+      double s = lam[i];
+      for (int q = i + 1; q < a.nel; ++q) s -= Lc[q][i] * lam[q];
+      lam[i] = s / Lc[i][i];
+    }
+    double Y1[kMaxNs], neg = 0.0, sum = 0.0;
+    for (int k = 0; k < a.ns; ++k) {
+      double corr = 0.0;
+      if (spd)
+        for (int e = 0; e < a.nel; ++e) corr += a.E[e * a.ns + k] * lam[e];
+      double y = Y0[k] + dY[k] - D[k] * corr;
+      if (y < 0.0) {
+        neg -= y;
+        y = 0.0;
+      }
+      Y1[k] = y;
+      sum += y;
+    }
+    for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
+    // temperature from the enthalpy balance
+    double h0 = 0.0;
+    for (int k = 0; k < a.ns; ++k) {
+      double hk, cpk;
+      nasa(a.th, a.tmid, k, T0, &hk, &cpk);
+      h0 += Y0[k] * hk;
+    }
+    double T1 = fmin(fmax(T0 + dT, 200.0), 6000.0);
+    for (int it = 0; it < 12; ++it) {
+      double hh = 0.0, cp = 0.0;
+      for (int k = 0; k < a.ns; ++k) {
+        double hk, cpk;
+        nasa(a.th, a.tmid, k, T1, &hk, &cpk);
+        hh += Y1[k] * hk;
+        cp += Y1[k] * cpk;
+      }
+      const double step = (hh - h0) / cp;
+      T1 -= step;
+      if (fabs(step) < 1e-9 * T1) break;
+    }
+    if (!reason && !(fabs(T1 - (T0 + dT)) <= a.consist_tol)) reason = 2;
+    if (!reason && !(neg <= a.clip_tol)) reason = 3;
+    if (!reason && !(isfinite(T1) && spd)) reason = 2;
+    if (reason) {
+      const int slot = atomicAdd(a.fb_count, 1);
+      a.fb_list[slot] = cell;
+      atomicAdd(&a.cnt[reason], 1ULL);
+    } else {
+      for (int k = 0; k < a.ns; ++k) a.state[(long long)k * a.ld + cell] = rho * Y1[k];
+      a.state[(long long)a.ns * a.ld + cell] = rho * T1;
+      atomicAdd(&a.cnt[0], 1ULL);
+    }
+  }
+}
+
+__global__ void k_gather_cells(const double* __restrict__ src, long long ld, int nv, const int* __restrict__ idx, int m,
+                               double* __restrict__ dst, const double* __restrict__ dts, double dt,
+                               double* __restrict__ dts_out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    for (int v = 0; v < nv; ++v) dst[(long long)v * m + j] = src[(long long)v * ld + idx[j]];
+    dts_out[j] = dts ? dts[idx[j]] : dt;
+  }
+}
+
+// surrogate(+fallback) result vs implicit result on the judged cells
+__global__ void k_judge(const double* __restrict__ state, long long ld, int ns, const int* __restrict__ idx, int m,
+                        const double* __restrict__ ref, double* __restrict__ out) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int c = idx[j];
+    double rs = 0.0, rr = 0.0, ymax = 0.0;
+    for (int k = 0; k < ns; ++k) {
+      rs += state[(long long)k * ld + c];
+      rr += ref[(long long)k * m + j];
+    }
+    for (int k = 0; k < ns; ++k) ymax = fmax(ymax, ref[(long long)k * m + j] / rr);
+    const double Ts = state[(long long)ns * ld + c] / rs, Tp = ref[(long long)ns * m + j] / rr;
+    double dy = 0.0;
+    for (int k = 0; k < ns; ++k)
+      dy = fmax(dy, fabs(state[(long long)k * ld + c] / rs - ref[(long long)k * m + j] / rr));
+    atomic_max_pos(&out[0], fabs(Ts - Tp) / Tp);
+    atomic_max_pos(&out[1], dy / ymax);
+  }
+}
+
+}  // namespace tng
+
+using namespace tng;
+
+struct tng_surrogate {
+  tng_chem* h = nullptr;
+  tng_surrogate_cfg cfg{};
+  Mlp m;
+  int ns = 0, bath = 0, n_in = 0, n_out = 0, nel = 0;
+  std::vector<double> fmean, fstd, fmin, fmax, tmean, tstd;  // host copies
+  bool trained = false;
+  // device
+  float* d_fnorm = nullptr;  // fmean (in_pad), fistd (in_pad), fmin (in_pad), fmax (in_pad)
+  double* d_tnorm = nullptr;  // tmean (out_pad), tstd (out_pad)
+  double* d_E = nullptr;
+  __nv_bfloat16* d_wpack = nullptr;
+  long long w_off[kMaxLayers] = {};
+  DevBuf out, fb, cnt, judge_state, judge_dts, judge_idx, work;
+  cudaEvent_t ev[5] = {};
+  int calls = 0;
+};
+
+static int sur_upload_norm(tng_surrogate* s) {
+  const int ip = s->m.in_pad, op = s->m.out_pad;
+  std::vector<float> f(4 * ip, 0.f);
+  for (int i = 0; i < s->n_in; ++i) {
+    f[i] = (float)s->fmean[i];
+    f[ip + i] = (float)(1.0 / s->fstd[i]);
+    f[2 * ip + i] = (float)s->fmin[i];
+    f[3 * ip + i] = (float)s->fmax[i];
+  }
+  std::vector<double> t(2 * op, 0.0);
+  for (int i = 0; i < s->n_out; ++i) {
+    t[i] = s->tmean[i];
+    t[op + i] = s->tstd[i];
+  }
+  cudaMemcpy(s->d_fnorm, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpy(s->d_tnorm, t.data(), sizeof(double) * t.size(), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate normalisation");
+}
+
+static int sur_pack(tng_surrogate* s) {
+  long long off = 0;
+  for (int l = 0; l < s->m.nlin; ++l) {
+    s->w_off[l] = off;
+    const int fo = s->m.fan_out[l], fi = s->m.fan_in[l];
+    k_pack_weights<<<256, 256, 0, s->m.stream>>>(s->m.params + s->m.w_off[l], fo, fi, s->d_wpack + off);
+    off += (long long)fo * fi;
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate weight packing");
+}
+
+static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
+                        const double* ddts, double dt, double p, float* out, int* err) {
+  InferArgs ia{};
+  ia.state = dstate;
+  ia.ld = dld;
+  ia.ncells = (int)ncells;
+  ia.dts = ddts;
+  ia.dt_scalar = dt;
+  ia.logp = std::log(p);
+  ia.ns = s->ns;
+  ia.bath = s->bath;
+  ia.n_in = s->n_in;
+  ia.in_pad = s->m.in_pad;
+  ia.hidden = s->m.hidden;
+  ia.out_pad = s->m.out_pad;
+  ia.nlin = s->m.nlin;
+  ia.fmean = s->d_fnorm;
+  ia.fistd = s->d_fnorm + s->m.in_pad;
+  ia.wpack = s->d_wpack;
+  for (int l = 0; l < s->m.nlin; ++l) {
+    ia.w_off[l] = s->w_off[l];
+    ia.b_off[l] = (int)s->m.b_off[l];
+  }
+  ia.bias = s->m.params;
+  ia.out = out;
+  ia.error = err;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
+  if (e != cudaSuccess) return cuda_error(e, "inference shared memory");
+  const int grid = (int)std::min<int64_t>(h->sm_count, (ncells + kInferRows - 1) / kInferRows);
+  k_mlp_infer<<<grid, kInferThreads, kInferSmem, h->stream>>>(ia);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "tensor-core inference");
+}
+
+extern "C" {
+
+void tng_surrogate_default_cfg(tng_surrogate_cfg* c) {
+  if (!c) return;
+  std::memset(c, 0, sizeof(*c));
+  c->hidden = 256;
+  c->layers = 4;
+  c->seed = 20261203;
+  c->ood_margin = 0.02;
+  c->consist_tol_K = 5.0;
+  c->clip_tol = 1e-3;
+  c->judge_cells = 1024;
+}
+
+int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogate** out) {
+  if (!h || !out) return set_error(TNG_ERR_ARG, "tng_surrogate_create: null argument");
+  *out = nullptr;
+  tng_surrogate_cfg c;
+  if (cfg)
+    c = *cfg;
+  else
+    tng_surrogate_default_cfg(&c);
+  if (c.hidden != 256 || c.layers < 1 || c.layers > kMaxLayers - 1)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_create: hidden width must be 256 (the tensor-core tile), 1..%d layers",
+                     kMaxLayers - 1);
+  const MechOps* o = h->ops;
+  if (o->ns + 3 > kMaxNs || o->nelem > kMaxEl) return set_error(TNG_ERR_ARG, "tng_surrogate_create: mechanism too large");
+  DeviceGuard g(h->cfg.device);
+  tng_surrogate* s = new tng_surrogate();
+  s->h = h;
+  s->cfg = c;
+  s->ns = o->ns;
+  s->bath = 0;
+  for (int k = 0; k < o->ns; ++k)
+    if (std::strcmp(o->species[k], "N2") == 0) s->bath = k;
+  s->n_in = o->ns + 2;  // T, log P, ns-1 species, log dt
+  s->n_out = o->ns + 1;
+  s->nel = o->nelem;
+  int rc = mlp_init(&s->m, h->cfg.device, h->stream, s->n_in, s->n_out, c.hidden, c.layers, c.seed);
+  if (rc) {
+    delete s;
+    return rc;
+  }
+  if (s->m.in_pad > 256 || s->m.out_pad > 256 || s->m.in_pad % 16 || s->m.out_pad % 16) {
+    mlp_free(&s->m);
+    delete s;
+    return set_error(TNG_ERR_ARG, "tng_surrogate_create: unsupported layer widths");
+  }
+  cudaMalloc(&s->d_fnorm, sizeof(float) * 4 * s->m.in_pad);
+  cudaMalloc(&s->d_tnorm, sizeof(double) * 2 * s->m.out_pad);
+  cudaMalloc(&s->d_wpack, sizeof(__nv_bfloat16) * s->m.nparam);
+  // element matrix per kg: a_ek / W_k (reference literal kinds of W_k)
+  std::vector<double> E(s->nel * s->ns);
+  const double* wm = o->wmol[h->cfg.literal_mode];
+  for (int e = 0; e < s->nel; ++e)
+    for (int k = 0; k < s->ns; ++k) E[e * s->ns + k] = o->elem[e * s->ns + k] / wm[k];
+  cudaMalloc(&s->d_E, sizeof(double) * E.size());
+  cudaMemcpy(s->d_E, E.data(), sizeof(double) * E.size(), cudaMemcpyHostToDevice);
+  for (auto& ev : s->ev) cudaEventCreate(&ev);
+  h->dependents++;
+  s->fmean.assign(s->n_in, 0.0), s->fstd.assign(s->n_in, 1.0), s->fmin.assign(s->n_in, 0.0),
+      s->fmax.assign(s->n_in, 0.0);
+  s->tmean.assign(s->n_out, 0.0), s->tstd.assign(s->n_out, 1.0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    tng_surrogate_destroy(s);
+    return cuda_error(e, "tng_surrogate_create");
+  }
+  *out = s;
+  return TNG_OK;
+}
+
+int tng_surrogate_destroy(tng_surrogate* s) {
+  if (!s) return TNG_OK;
+  DeviceGuard g(s->m.device);
+  cudaStreamSynchronize(s->m.stream);
+  mlp_free(&s->m);
+  if (s->d_fnorm) cudaFree(s->d_fnorm);
+  if (s->d_tnorm) cudaFree(s->d_tnorm);
+  if (s->d_E) cudaFree(s->d_E);
+  if (s->d_wpack) cudaFree(s->d_wpack);
+  for (DevBuf* b : {&s->out, &s->fb, &s->cnt, &s->judge_state, &s->judge_dts, &s->judge_idx, &s->work}) b->release();
+  for (auto& ev : s->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (s->h) s->h->dependents--;
+  delete s;
+  return TNG_OK;
+}
+
+int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                        int64_t ld, double p, int epochs, int batch, double lr, float* losses) {
+  if (!s || !state0 || !state1 || !dts || n < 16 || ld < n || !(p > 0.0) || n > (1LL << 31) - 1)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_train: bad argument");
+  DeviceGuard g(s->m.device);
+  const int ip = s->m.in_pad, op = s->m.out_pad;
+  cudaStream_t st = s->m.stream;
+  if (!s->work.reserve((size_t)n * (ip + op) * sizeof(float) + sizeof(double) * 4 * (ip + op) + 256 * sizeof(float)))
+    return set_error(TNG_ERR_CUDA, "tng_surrogate_train: %lld pairs do not fit", (long long)n);
+  float* X = (float*)s->work.ptr;
+  float* T = X + (size_t)n * ip;
+  double* stats = (double*)(T + (size_t)n * op);
+  float* nrm = (float*)(stats + 4 * (ip + op));
+  k_sur_features<<<1184, 128, 0, st>>>(state0, ld, (int)n, dts, std::log(p), s->ns, s->bath, ip, X);
+  k_sur_targets<<<1184, 128, 0, st>>>(state0, state1, ld, (int)n, s->ns, op, T);
+  k_colstats<<<ip, 256, 0, st>>>(X, (int)n, ip, stats);
+  k_colstats<<<op, 256, 0, st>>>(T, (int)n, op, stats + 4 * ip);
+  std::vector<double> hs(4 * (ip + op));
+  cudaMemcpyAsync(hs.data(), stats, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_error(e, "surrogate statistics");
+  for (int i = 0; i < s->n_in; ++i) {
+    const double mu = hs[4 * i] / n, var = std::max(hs[4 * i + 1] / n - mu * mu, 0.0);
+    s->fmean[i] = mu;
+    s->fstd[i] = std::max(std::sqrt(var), 1e-3 * std::max(1.0, std::fabs(mu)));
+    s->fmin[i] = hs[4 * i + 2];
+    s->fmax[i] = hs[4 * i + 3];
+  }
+  for (int i = 0; i < s->n_out; ++i) {
+    const double* q = &hs[4 * (ip + i)];
+    const double mu = q[0] / n, var = std::max(q[1] / n - mu * mu, 0.0);
+    s->tmean[i] = mu;
+    s->tstd[i] = std::max(std::sqrt(var), 1e-14);
+  }
+  int rc = sur_upload_norm(s);
+  if (rc) return rc;
+  std::vector<float> hn(2 * (ip + op), 0.f);
+  for (int i = 0; i < s->n_in; ++i) hn[i] = (float)s->fmean[i], hn[ip + i] = (float)(1.0 / s->fstd[i]);
+  for (int i = 0; i < s->n_out; ++i)
+    hn[2 * ip + i] = (float)s->tmean[i], hn[2 * ip + op + i] = (float)(1.0 / s->tstd[i]);
+  cudaMemcpyAsync(nrm, hn.data(), sizeof(float) * hn.size(), cudaMemcpyHostToDevice, st);
+  k_normalise<<<2048, 256, 0, st>>>(X, (int)n, ip, s->n_in, nrm, nrm + ip);
+  k_normalise<<<2048, 256, 0, st>>>(T, (int)n, op, s->n_out, nrm + 2 * ip, nrm + 2 * ip + op);
+  // loss weights: every output equally (outputs are normalised), temperature doubled
+  std::vector<float> w(op, 0.f);
+  for (int i = 0; i < s->n_out; ++i) w[i] = i == 0 ? 2.f : 1.f;
+  float* dw;
+  if ((e = cudaMalloc(&dw, sizeof(float) * op)) != cudaSuccess) return cuda_error(e, "loss weights");
+  cudaMemcpyAsync(dw, w.data(), sizeof(float) * op, cudaMemcpyHostToDevice, st);
+  rc = mlp_train(&s->m, X, T, dw, n, epochs, batch, (float)lr, s->cfg.seed + 1, losses);
+  cudaStreamSynchronize(st);
+  cudaFree(dw);
+  if (rc) return rc;
+  if ((rc = sur_pack(s))) return rc;
+  s->trained = true;
+  return TNG_OK;
+}
+
+int tng_surrogate_save(const tng_surrogate* s, const char* path) {
+  if (!s || !path) return set_error(TNG_ERR_ARG, "tng_surrogate_save: null argument");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_save: surrogate not trained");
+  std::vector<float> params(s->m.nparam);
+  DeviceGuard g(s->m.device);
+  cudaStreamSynchronize(s->m.stream);
+  cudaMemcpy(params.data(), s->m.params, sizeof(float) * s->m.nparam, cudaMemcpyDeviceToHost);
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_error(TNG_ERR_ARG, "tng_surrogate_save: cannot open %s", path);
+  char magic[8] = {'T', 'N', 'G', 'S', 'U', 'R', '1', 0};
+  char mech[32] = {};
+  std::snprintf(mech, sizeof(mech), "%s", s->h->ops->name);
+  int hdr[8] = {s->ns, s->n_in, s->n_out, s->cfg.hidden, s->cfg.layers, s->bath, s->h->cfg.literal_mode, 0};
+  int64_t np = s->m.nparam;
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(mech, 1, 32, f) == 32 && std::fwrite(hdr, 4, 8, f) == 8 &&
+            std::fwrite(&np, 8, 1, f) == 1;
+  for (const std::vector<double>* v : {&s->fmean, &s->fstd, &s->fmin, &s->fmax, &s->tmean, &s->tstd})
+    ok = ok && std::fwrite(v->data(), 8, v->size(), f) == v->size();
+  ok = ok && std::fwrite(params.data(), 4, params.size(), f) == params.size();
+  std::fclose(f);
+  return ok ? TNG_OK : set_error(TNG_ERR_ARG, "tng_surrogate_save: write failed");
+}
+
+int tng_surrogate_load(tng_surrogate* s, const char* path) {
+  if (!s || !path) return set_error(TNG_ERR_ARG, "tng_surrogate_load: null argument");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_error(TNG_ERR_ARG, "tng_surrogate_load: cannot open %s", path);
+  char magic[8], mech[32];
+  int hdr[8];
+  int64_t np = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::fread(mech, 1, 32, f) == 32 && std::fread(hdr, 4, 8, f) == 8 &&
+            std::fread(&np, 8, 1, f) == 1;
+  if (!ok || std::memcmp(magic, "TNGSUR1", 8) != 0) {
+    std::fclose(f);
+    return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is not a surrogate file", path);
+  }
+  mech[31] = 0;
+  if (std::strcmp(mech, s->h->ops->name) != 0 || hdr[0] != s->ns || hdr[1] != s->n_in || hdr[2] != s->n_out ||
+      hdr[3] != s->cfg.hidden || hdr[4] != s->cfg.layers || np != s->m.nparam) {
+    std::fclose(f);
+    return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s was trained for %s with other sizes", path, mech);
+  }
+  for (std::vector<double>* v : {&s->fmean, &s->fstd, &s->fmin, &s->fmax, &s->tmean, &s->tstd})
+    ok = ok && std::fread(v->data(), 8, v->size(), f) == v->size();
+  std::vector<float> params(np);
+  ok = ok && std::fread(params.data(), 4, np, f) == (size_t)np;
+  std::fclose(f);
+  if (!ok) return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is truncated", path);
+  DeviceGuard g(s->m.device);
+  cudaMemcpy(s->m.params, params.data(), sizeof(float) * np, cudaMemcpyHostToDevice);
+  int rc = sur_upload_norm(s);
+  if (rc) return rc;
+  if ((rc = sur_pack(s))) return rc;
+  cudaError_t e = cudaStreamSynchronize(s->m.stream);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_load");
+  s->trained = true;
+  return TNG_OK;
+}
+
+int tng_surrogate_dims(const tng_surrogate* s, int* n_in, int* n_out, int* in_pad, int* out_pad, int64_t* nparam) {
+  if (!s) return set_error(TNG_ERR_ARG, "tng_surrogate_dims: null handle");
+  if (n_in) *n_in = s->n_in;
+  if (n_out) *n_out = s->n_out;
+  if (in_pad) *in_pad = s->m.in_pad;
+  if (out_pad) *out_pad = s->m.out_pad;
+  if (nparam) *nparam = s->m.nparam;
+  return TNG_OK;
+}
+
+int tng_surrogate_params(tng_surrogate* s, float* host, int set) {
+  if (!s || !host) return set_error(TNG_ERR_ARG, "tng_surrogate_params: null argument");
+  DeviceGuard g(s->m.device);
+  cudaStreamSynchronize(s->m.stream);
+  cudaError_t e;
+  if (set) {
+    e = cudaMemcpy(s->m.params, host, sizeof(float) * s->m.nparam, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && s->trained) {
+      int rc = sur_pack(s);
+      if (rc) return rc;
+      e = cudaStreamSynchronize(s->m.stream);
+    }
+  } else {
+    e = cudaMemcpy(host, s->m.params, sizeof(float) * s->m.nparam, cudaMemcpyDeviceToHost);
+  }
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "tng_surrogate_params");
+}
+
+int tng_surrogate_features(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double p,
+                           float* X) {
+  if (!s || !state || !dts || !X || n <= 0 || ld < n) return set_error(TNG_ERR_ARG, "tng_surrogate_features: bad argument");
+  DeviceGuard g(s->m.device);
+  const int ip = s->m.in_pad;
+  k_sur_features<<<1184, 128, 0, s->m.stream>>>(state, ld, (int)n, dts, std::log(p), s->ns, s->bath, ip, X);
+  std::vector<float> hn(2 * ip, 0.f);
+  for (int i = 0; i < s->n_in; ++i) hn[i] = (float)s->fmean[i], hn[ip + i] = (float)(1.0 / s->fstd[i]);
+  float* dn;
+  cudaError_t e = cudaMalloc(&dn, sizeof(float) * 2 * ip);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_features");
+  cudaMemcpyAsync(dn, hn.data(), sizeof(float) * 2 * ip, cudaMemcpyHostToDevice, s->m.stream);
+  k_normalise<<<1024, 256, 0, s->m.stream>>>(X, (int)n, ip, s->n_in, dn, dn + ip);
+  e = cudaStreamSynchronize(s->m.stream);
+  cudaFree(dn);
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "tng_surrogate_features");
+}
+
+int tng_surrogate_forward_f32(tng_surrogate* s, const float* X, int64_t n, float* Y) {
+  if (!s || !X || !Y || n <= 0 || n > (1 << 24)) return set_error(TNG_ERR_ARG, "tng_surrogate_forward_f32: bad argument");
+  DeviceGuard g(s->m.device);
+  float* out;
+  int rc = mlp_forward_f32(&s->m, X, (int)n, &out);
+  if (rc) return rc;
+  cudaMemcpyAsync(Y, out, sizeof(float) * n * s->m.out_pad, cudaMemcpyDeviceToDevice, s->m.stream);
+  cudaError_t e = cudaStreamSynchronize(s->m.stream);
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "tng_surrogate_forward_f32");
+}
+
+int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double dt,
+                        double p, float* out) {
+  if (!s || !state || !out || n <= 0 || ld < n) return set_error(TNG_ERR_ARG, "tng_surrogate_infer: bad argument");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_infer: surrogate not trained or loaded");
+  DeviceGuard g(s->m.device);
+  if (!s->cnt.reserve(16 * sizeof(unsigned long long))) return set_error(TNG_ERR_CUDA, "scratch");
+  int* err = (int*)((unsigned long long*)s->cnt.ptr + 8);
+  cudaMemsetAsync(err, 0, sizeof(int), s->m.stream);
+  int rc = launch_infer(s->h, s, state, n, ld, dts, dt, p, out, err);
+  if (rc) return rc;
+  int herr = 0;
+  cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s->m.stream);
+  cudaError_t e = cudaStreamSynchronize(s->m.stream);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_infer");
+  if (herr) return set_error(TNG_ERR_CUDA, "tng_surrogate_infer: tensor-core inference timed out");
+  return TNG_OK;
+}
+
+int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t ncells, int64_t ld, const double* dts,
+                          double dt, double p, int flags, tng_surrogate_stats* stats) {
+  if (!h || !s || s->h != h) return set_error(TNG_ERR_ARG, "tng_substep_surrogate: handle/surrogate mismatch");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_substep_surrogate: surrogate not trained or loaded");
+  if (ncells < 0 || ld < ncells || ncells > (1LL << 31) - 1)
+    return set_error(TNG_ERR_ARG, "tng_substep_surrogate: need 0 <= ncells <= ld < 2^31");
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (ncells == 0) return TNG_OK;
+  if (!state || !(p > 0.0) || (!dts && !(dt >= 0.0))) return set_error(TNG_ERR_ARG, "tng_substep_surrogate: bad argument");
+  if (flags != TNG_DEVICE_PTRS && flags != TNG_HOST_PTRS) return set_error(TNG_ERR_ARG, "tng_substep_surrogate: bad flags");
+  DeviceGuard g(h->cfg.device);
+  cudaStream_t st = h->stream;
+  const int nv = s->ns + 1;
+  cudaError_t e;
+  double* dstate = state;
+  const double* ddts = dts;
+  int64_t dld = ld;
+  if (flags == TNG_HOST_PTRS) {
+    if (!h->bufs[6].reserve((size_t)nv * ncells * sizeof(double)) ||
+        (dts && !h->bufs[7].reserve(ncells * sizeof(double))))
+      return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: device state allocation failed");
+    dstate = (double*)h->bufs[6].ptr;
+    dld = ncells;
+    cudaMemcpy2DAsync(dstate, ncells * sizeof(double), state, ld * sizeof(double), ncells * sizeof(double), nv,
+                      cudaMemcpyHostToDevice, st);
+    if (dts) {
+      cudaMemcpyAsync(h->bufs[7].ptr, dts, ncells * sizeof(double), cudaMemcpyHostToDevice, st);
+      ddts = (const double*)h->bufs[7].ptr;
+    }
+  }
+  const int J = (int)std::min<int64_t>(ncells, std::max(0, s->cfg.judge_cells));
+  bool ok = s->out.reserve((size_t)ncells * s->m.out_pad * sizeof(float)) && s->fb.reserve((ncells + 1) * sizeof(int)) &&
+            s->cnt.reserve(16 * sizeof(unsigned long long)) &&
+            (J == 0 || (s->judge_state.reserve((size_t)J * nv * sizeof(double)) &&
+                        s->judge_dts.reserve((size_t)J * sizeof(double)) && s->judge_idx.reserve(J * sizeof(int))));
+  if (!ok) return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: scratch allocation failed");
+  int rc = solver_prepare(h);  // the solver tables (thermo for the enthalpy balance) on the device
+  if (rc) return rc;
+  int* fb_count = (int*)s->fb.ptr;
+  int* fb_list = fb_count + 1;
+  unsigned long long* cnt = (unsigned long long*)s->cnt.ptr;
+  cudaMemsetAsync(fb_count, 0, sizeof(int), st);
+  cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), st);
+  // held-out sample: a strided set of cells that rotates from call to call
+  if (J > 0) {
+    std::vector<int> idx(J);
+    const int64_t stride = std::max<int64_t>(1, ncells / J);
+    const int64_t off = (int64_t)(s->calls * 7919) % stride;
+    for (int j = 0; j < J; ++j) idx[j] = (int)((off + (int64_t)j * stride) % ncells);
+    cudaMemcpyAsync(s->judge_idx.ptr, idx.data(), sizeof(int) * J, cudaMemcpyHostToDevice, st);
+    k_gather_cells<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, nv, (const int*)s->judge_idx.ptr, J,
+                                                    (double*)s->judge_state.ptr, ddts, dt,
+                                                    (double*)s->judge_dts.ptr);
+  }
+  s->calls++;
+  // inference on the tensor cores
+  cudaEventRecord(s->ev[0], st);
+  rc = launch_infer(h, s, dstate, ncells, dld, ddts, dt, p, (float*)s->out.ptr, (int*)(cnt + 8));
+  if (rc) return rc;
+  cudaEventRecord(s->ev[1], st);
+  // post-processing and fallback list
+  SurPost pa{};
+  pa.state = dstate;
+  pa.ld = dld;
+  pa.ncells = (int)ncells;
+  pa.dts = ddts;
+  pa.dt_scalar = dt;
+  pa.logp = std::log(p);
+  pa.ns = s->ns;
+  pa.bath = s->bath;
+  pa.n_in = s->n_in;
+  pa.n_out = s->n_out;
+  pa.out_pad = s->m.out_pad;
+  pa.nel = s->nel;
+  pa.out = (const float*)s->out.ptr;
+  pa.tmean = s->d_tnorm;
+  pa.tstd = s->d_tnorm + s->m.out_pad;
+  pa.fmin = s->d_fnorm + 2 * s->m.in_pad;
+  pa.fmax = s->d_fnorm + 3 * s->m.in_pad;
+  pa.margin = s->cfg.ood_margin;
+  pa.consist_tol = s->cfg.consist_tol_K;
+  pa.clip_tol = s->cfg.clip_tol;
+  pa.E = s->d_E;
+  solver_thermo(h, &pa.th, &pa.tmid);
+  pa.fb_list = fb_list;
+  pa.fb_count = fb_count;
+  pa.cnt = cnt;
+  k_sur_post<<<(int)std::min<int64_t>(4096, (ncells + 127) / 128), 128, 0, st>>>(pa);
+  cudaEventRecord(s->ev[2], st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "surrogate kernels");
+  // implicit fallback on the listed cells, in place
+  tng_substep_stats fst;
+  rc = substep_run(h, dstate, ncells, dld, ddts, dt, p, TNG_DEVICE_PTRS, fb_list, fb_count, nullptr, nullptr, nullptr,
+                   stats ? &fst : nullptr);
+  if (rc) return rc;
+  cudaEventRecord(s->ev[3], st);
+  // judge: the implicit solve of the sample, compared with the surrogate(+fallback) result
+  if (J > 0 && stats) {
+    rc = substep_run(h, (double*)s->judge_state.ptr, J, J, (const double*)s->judge_dts.ptr, 0.0, p, TNG_DEVICE_PTRS,
+                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    k_judge<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, s->ns, (const int*)s->judge_idx.ptr, J,
+                                             (const double*)s->judge_state.ptr, (double*)(cnt + 10));
+  }
+  cudaEventRecord(s->ev[4], st);
+  if (flags == TNG_HOST_PTRS)
+    cudaMemcpy2DAsync(state, ld * sizeof(double), dstate, ncells * sizeof(double), ncells * sizeof(double), nv,
+                      cudaMemcpyDeviceToHost, st);
+  if (stats || flags == TNG_HOST_PTRS) {
+    unsigned long long hc[16];
+    cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "surrogate substep");
+    if (hc[8]) return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: tensor-core inference timed out");
+    if (stats) {
+      stats->cells = ncells;
+      stats->accepted = (int64_t)hc[0];
+      stats->fallback_ood = (int64_t)hc[1];
+      stats->fallback_consistency = (int64_t)hc[2];
+      stats->fallback_clip = (int64_t)hc[3];
+      stats->judged = J;
+      double jd[2];
+      std::memcpy(jd, &hc[10], sizeof(jd));
+      stats->judge_max_rel_dT = jd[0];
+      stats->judge_max_dY = jd[1];
+      float a = 0, b = 0, c = 0, d = 0;
+      cudaEventElapsedTime(&a, s->ev[0], s->ev[1]);
+      cudaEventElapsedTime(&b, s->ev[1], s->ev[2]);
+      cudaEventElapsedTime(&c, s->ev[2], s->ev[3]);
+      cudaEventElapsedTime(&d, s->ev[0], s->ev[3]);
+      stats->ms_infer = a, stats->ms_post = b, stats->ms_fallback = c, stats->ms_total = d;
+      stats->fallback = fst;
+      stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3]);
+    }
+  }
+  return TNG_OK;
+}
+
+}  // extern "C"

@@ -54,6 +54,12 @@ struct DevBuf {
 
 struct SolverState;
 void solver_release(tng_chem* h);
+int solver_prepare(tng_chem* h);
+// NASA tables on the device (ns x 24: high range 12, low range 12) and the switch temperature
+void solver_thermo(tng_chem* h, const double** th, double* tmid);
+int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
+                int flags, const int* list, const int* nlist, int* cell_nst, int* cell_nni, int* cell_status,
+                tng_substep_stats* stats);
 
 }  // namespace tng
 
@@ -65,4 +71,5 @@ struct tng_chem {
   cudaStream_t copy_stream[2] = {nullptr, nullptr};
   tng::DevBuf bufs[8];
   tng::SolverState* solver = nullptr;
+  int dependents = 0;  // live tng_mlp / tng_surrogate objects using this handle's stream
 };
