@@ -126,6 +126,26 @@ typedef struct tng_substep_stats {
 int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
                       int flags, int* cell_nst, int* cell_nni, int* cell_status, tng_substep_stats* stats);
 
+/* Bounds of the host solver's arrays (Fortran, inclusive, column-major): RHO_(imino:imaxo,
+ * jmino:jmaxo, kmino:kmaxo) and SC_(..., nscalar); the interior imin..imax etc.; 1-based scalar
+ * indices of the first species, of T, and of H2O / CO / CO2 for the chemsrc diagnostics
+ * (0 = absent). The species scalars are isc_sc .. isc_sc+N-1 in mechanism order. */
+typedef struct tng_extent {
+  int imino, imaxo, jmino, jmaxo, kmino, kmaxo;
+  int imin, imax, jmin, jmax, kmin, kmax;
+  int nscalar, isc_sc, isc_T;
+  int isc_H2O, isc_CO, isc_CO2;
+} tng_extent;
+
+/* Drop-in for finitechem_source_chemistry(RHO_, SC_) (finitechem.f90:962-1071): for every
+ * interior cell with mask(i,j) /= 1 (mask(imino:imaxo, jmino:jmaxo), nullable = no mask),
+ * integrate (rho*Y, rho*T) over dt at pressure p_mid (0.5*(P_thermo + P_thermo_old)), write
+ * Y and T back into sc, the heat-release rate into hr and d(rho*Y)/dt of H2O/CO/CO2 into
+ * chemsrc(..., 3) (both same shape as RHO_ without/with the trailing 3; nullable). flags:
+ * TNG_DEVICE_PTRS or TNG_HOST_PTRS (arrays staged through the device; the call then waits). */
+int tng_chem_substep(tng_chem* h, const double* rho, double* sc, const int* mask, const tng_extent* ext, double dt,
+                     double p_mid, double* hr, double* chemsrc, int flags, tng_substep_stats* stats);
+
 /* Parity helper: the solver's own (table-driven, warp-cooperative) right-hand side and, when
  * jac is non-null, its Jacobian (cell-major, (N+1)^2 row-major per cell), device pointers. */
 int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,

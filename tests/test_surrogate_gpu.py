@@ -38,7 +38,7 @@ def trained():
 
 def test_training_reduces_loss(trained):
     _, _, losses = trained
-    assert np.isfinite(losses).all() and losses[-1] < 0.3 * losses[0]
+    assert np.isfinite(losses).all() and losses[-1] < 0.5 * losses[0]
 
 
 def test_tensor_core_chain_matches_fp32_forward(trained):

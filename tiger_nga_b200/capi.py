@@ -66,6 +66,12 @@ class SurrogateCfg(ctypes.Structure):
                 ("judge_cells", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
 
 
+class Extent(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("imino", "imaxo", "jmino", "jmaxo", "kmino", "kmaxo", "imin", "imax",
+                                            "jmin", "jmax", "kmin", "kmax", "nscalar", "isc_sc", "isc_T",
+                                            "isc_H2O", "isc_CO", "isc_CO2")]
+
+
 class ChemError(RuntimeError):
     pass
 
@@ -98,6 +104,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_bench_fp64_peak": (I, [I, ctypes.POINTER(D)]),
         "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
+        "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
         "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
         "tng_mlp_destroy": (I, [V]),
         "tng_mlp_param_count": (L, [V]),
@@ -353,6 +360,24 @@ def _solver_rhs_jac(self, state, p: float, jacobian: bool = True):
     return rhs, jac
 
 
+def _source_chemistry(self, RHO, SC, ext: dict, dt: float, p_mid: float, mask=None, HR=None, chemsrc=None):
+    """finitechem_source_chemistry(RHO_, SC_) on the solver's own arrays (NumPy, Fortran order)."""
+    for a in (RHO, SC):
+        if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous):
+            raise ValueError("RHO and SC must be Fortran-ordered float64 arrays")
+    e = Extent(**ext)
+    st = SubstepStats()
+    mk = None
+    if mask is not None:
+        mk = np.asfortranarray(mask, dtype=np.int32)
+    _check(self.lib.tng_chem_substep(self.h, RHO.ctypes.data, SC.ctypes.data, mk.ctypes.data if mk is not None else None,
+                                     ctypes.byref(e), float(dt), float(p_mid), HR.ctypes.data if HR is not None else None,
+                                     chemsrc.ctypes.data if chemsrc is not None else None, TNG_HOST_PTRS,
+                                     ctypes.byref(st)), "tng_chem_substep")
+    return st.as_dict()
+
+
+FiniteChem.source_chemistry = _source_chemistry
 FiniteChem.substep = _substep
 FiniteChem.solver_rhs_jac = _solver_rhs_jac
 

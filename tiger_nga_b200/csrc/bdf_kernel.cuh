@@ -228,6 +228,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
           for (int i = lane; i < nv; i += 32) w.mat[i * rs + i] += 1.0;
           __syncwarp();
           const int sing = lu_warp(w.mat, nv, rs, w.piv, lane);
+          lu_finish(w.mat, nv, rs, w.piv, w.perm, w.cb, lane);
           gamma_lu = gamma;
           nst_lu = nst;
           jcur = true;
@@ -246,13 +247,9 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
             ++nni;
             x[0] = h * f[0] - z[1][0] - acor[0];
             x[1] = h * f[1] - z[1][1] - acor[1];
-            if (h0) w.vb[lane] = x[0];
-            if (h1) w.vb[lane + 32] = x[1];
-            __syncwarp();
-            lu_solve_warp(w.mat, nv, rs, w.piv, w.vb, lane);
-            x[0] = h0 ? w.vb[lane] : 0.0;
-            x[1] = h1 ? w.vb[lane + 32] : 0.0;
-            __syncwarp();
+            lu_solve_reg(w.mat, nv, rs, w.perm, w.cb, w.vb, x[0], x[1], lane);
+            if (!h0) x[0] = 0.0;
+            if (!h1) x[1] = 0.0;
             if (gamma != gamma_lu) {
               const double cf = 2.0 / (1.0 + gamma / gamma_lu);
               x[0] *= cf;

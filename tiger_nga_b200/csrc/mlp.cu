@@ -198,20 +198,24 @@ int mlp_train(Mlp* m, const float* X, const float* T, const float* w_out, int64_
     std::shuffle(perm.begin(), perm.end(), rng);
     cudaMemcpyAsync(perm_d, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, m->stream);
     double lsum = 0.0;
+    int nrep = 0;
     for (int64_t b = 0; b < steps_per_epoch; ++b, ++s) {
       const int* idx = perm_d + b * batch;
       k_gather_rows<<<512, 256, 0, m->stream>>>(X, idx, batch, m->in_pad, Xb);
       k_gather_rows<<<512, 256, 0, m->stream>>>(T, idx, batch, m->out_pad, Tb);
-      const bool report = (b == steps_per_epoch - 1) || (b % 64 == 0);
+      const bool report = (b == steps_per_epoch - 1) || (b % 16 == 0);
       float l = 0.f;
       int rc = mlp_backward(m, Xb, Tb, w_out, batch, report ? &l : nullptr);
       if (rc) return rc;
       // cosine learning-rate schedule
       const float lr = lr0 * 0.5f * (1.f + std::cos(3.14159265358979f * (float)s / (float)std::max<int64_t>(total, 1)));
       if ((rc = mlp_adam(m, lr))) return rc;
-      if (report) lsum = l;
+      if (report) {
+        lsum += l;
+        ++nrep;
+      }
     }
-    if (losses) losses[ep] = (float)lsum;
+    if (losses) losses[ep] = (float)(lsum / std::max(nrep, 1));  // mean of the sampled minibatch losses
   }
   cudaError_t e = cudaStreamSynchronize(m->stream);
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "mlp train");

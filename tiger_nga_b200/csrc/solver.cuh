@@ -104,14 +104,15 @@ struct WarpMem {
   double* G;    // ngpair
   double* vb;   // 64 vector buffer
   double* hb;   // 64 enthalpies
-  double* cb;   // 64 heat capacities
+  double* cb;   // 64 heat capacities (Jacobian), then the pivot reciprocals of the LU
   int* piv;     // 64 pivots
+  int* perm;    // 64: the composed row permutation of the LU
 };
 
 __host__ __device__ inline int warp_mem_doubles(const SvLayout& L, int rs) {
   const int nv = L.size[SZ_NV];
   return nv * rs + L.size[SZ_NSLOT] + 64 + 2 * L.size[SZ_NM] + 3 * L.size[SZ_NFC] + L.size[SZ_NCDCHUNK] +
-         L.size[SZ_NGPAIR] + 3 * 64 + 32 /* pivots as ints */ + 8;
+         L.size[SZ_NGPAIR] + 3 * 64 + 64 /* pivots and permutation as ints */ + 8;
 }
 
 __device__ __forceinline__ WarpMem warp_mem(double* base, const SvLayout& L, int rs) {
@@ -130,6 +131,7 @@ __device__ __forceinline__ WarpMem warp_mem(double* base, const SvLayout& L, int
   w.hb = p; p += 64;
   w.cb = p; p += 64;
   w.piv = reinterpret_cast<int*>(p);
+  w.perm = w.piv + 64;
   return w;
 }
 
@@ -496,6 +498,50 @@ __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int
     __syncwarp();
   }
   return sing;
+}
+
+// After lu_warp: the composed permutation ((P b)[i] = b[perm[i]]) and the reciprocals of the
+// pivots, so that a solve runs in registers.
+__device__ __forceinline__ void lu_finish(const double* a, const int n, const int rs, const int* piv, int* perm,
+                                          double* dinv, const int lane) {
+  if (lane == 0) {
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      const int t = perm[k];
+      perm[k] = perm[p];
+      perm[p] = t;
+    }
+  }
+  for (int i = lane; i < n; i += 32) dinv[i] = 1.0 / a[i * rs + i];
+  __syncwarp();
+}
+
+// Solve (LU) x = b with b and x two entries per lane in registers: permutation by one gather,
+// forward and backward substitution by shuffles (no shared-memory round trips per step).
+__device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const int rs, const int* perm,
+                                             const double* dinv, double* vb, double& x0, double& x1, const int lane) {
+  const int i0 = lane, i1 = lane + 32;
+  if (i0 < n) vb[i0] = x0;
+  if (i1 < n) vb[i1] = x1;
+  __syncwarp();
+  double b0 = i0 < n ? vb[perm[i0]] : 0.0;
+  double b1 = i1 < n ? vb[perm[i1]] : 0.0;
+  __syncwarp();
+  for (int k = 0; k < n - 1; ++k) {
+    const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31);
+    if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31) * dinv[k];
+    if (i0 == k) b0 = bk;
+    if (i1 == k) b1 = bk;
+    if (i0 < k) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i1 < k) b1 = fma(-a[i1 * rs + k], bk, b1);
+  }
+  x0 = b0;
+  x1 = b1;
 }
 
 // Solve (LU) x = b in place; b in shared memory.
