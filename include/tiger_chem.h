@@ -126,6 +126,16 @@ typedef struct tng_substep_stats {
 int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt, double p,
                       int flags, int* cell_nst, int* cell_nni, int* cell_status, tng_substep_stats* stats);
 
+/* The same implicit substep (device pointers, one pass, no step budget) for callers that must
+ * not allocate device memory during the call; no counterpart in the reference, which lets
+ * CVODE allocate per cell. All scratch (tables, per-cell counters) lives in one static device
+ * array: at most 262144 cells per call (TNG_ERR_ARG beyond). The first call on a device does
+ * a synchronous set-up and should precede any stream capture. Calls that overlap in time on
+ * one device race on the shared scratch: order them (e.g. one stream). n_failed (host,
+ * nullable) receives the number of cells with a nonzero status; when given the call waits. */
+int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt,
+                             double p, int* n_failed);
+
 /* Bounds of the host solver's arrays (Fortran, inclusive, column-major): RHO_(imino:imaxo,
  * jmino:jmaxo, kmino:kmaxo) and SC_(..., nscalar); the interior imin..imax etc.; 1-based scalar
  * indices of the first species, of T, and of H2O / CO / CO2 for the chemsrc diagnostics

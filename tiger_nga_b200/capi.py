@@ -104,6 +104,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_bench_fp64_peak": (I, [I, ctypes.POINTER(D)]),
         "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
+        "tng_substep_batch_static": (I, [V, V, L, L, V, D, D, ctypes.POINTER(I)]),
         "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
         "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
         "tng_mlp_destroy": (I, [V]),
@@ -377,7 +378,35 @@ def _source_chemistry(self, RHO, SC, ext: dict, dt: float, p_mid: float, mask=No
     return st.as_dict()
 
 
+def _substep_static(self, state, dt, p: float) -> int:
+    """tng_substep_batch_static on a CUDA tensor (allocates nothing on the device during the
+    call; at most 262144 cells; calls must not overlap). Returns the number of failed cells."""
+    import torch
+
+    nv = self.nspecies + 1
+    if not (state.is_cuda and state.dtype == torch.float64 and state.dim() == 2 and state.shape[0] == nv):
+        raise ValueError(f"state must be a CUDA float64 tensor of shape ({nv}, ncells)")
+    n = state.shape[1]
+    if n > 1 and state.stride(1) != 1:
+        raise ValueError("state must be species-major with unit stride along cells")
+    dts = None
+    if not isinstance(dt, (float, int)):
+        dts = torch.as_tensor(dt, dtype=torch.float64, device=state.device).contiguous()
+        if dts.shape != (n,):
+            raise ValueError("per-cell dt must have shape (ncells,)")
+    failed = ctypes.c_int(0)
+    sst = self.torch_stream()
+    sst.wait_stream(torch.cuda.current_stream(state.device))
+    _check(self.lib.tng_substep_batch_static(self.h, state.data_ptr(), n, max(state.stride(0), n),
+                                             dts.data_ptr() if dts is not None else None,
+                                             0.0 if dts is not None else float(dt), float(p), ctypes.byref(failed)),
+           "tng_substep_batch_static")
+    torch.cuda.current_stream(state.device).wait_stream(sst)
+    return failed.value
+
+
 FiniteChem.source_chemistry = _source_chemistry
+FiniteChem.substep_static = _substep_static
 FiniteChem.substep = _substep
 FiniteChem.solver_rhs_jac = _solver_rhs_jac
 

@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(WARPS * 32)
   }
 }
 
-__global__ void k_reset_counters(int* a, int* b) {
+static __global__ void k_reset_counters(int* a, int* b) {
   if (threadIdx.x == 0) {
     *a = 0;
     if (b) *b = 0;

@@ -14,7 +14,7 @@ namespace tng {
 
 // The BDF coefficients: l(x) = prod_{i=1..q} (1 + x/i) normalised to l_1 = 1, and the error
 // constants of orders q, q-1 and q+1 (same arithmetic as oracle/solver_oracle.c).
-static BdfCoef make_coef() {
+BdfCoef make_coef() {
   BdfCoef c;
   std::memset(&c, 0, sizeof(c));
   for (int q = 1; q <= kQmax + 1; ++q) {
