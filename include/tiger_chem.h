@@ -201,7 +201,12 @@ typedef struct tng_surrogate_cfg {
   double consist_tol_K;   /* fallback when network and enthalpy temperatures differ by more (K, 5) */
   double clip_tol;        /* fallback when clipping removed more mass fraction (1e-3) */
   int judge_cells;        /* cells re-solved every call to measure the error (1024) */
-  int reserved[8];
+  int post_mode;          /* 0: T from the enthalpy balance of the conserved Y; 1: T from the network,
+                             enthalpy held by the projection of Y (default 0) */
+  int target_mode;        /* training targets: 0 each output scaled by its own spread; 1 dY_k share
+                             one scale (errors weighted as the dY <= tol*max(Y) criterion) (0) */
+  float loss_T_weight;    /* loss weight of dT relative to one species output (0 = default 2) */
+  int reserved[5];
 } tng_surrogate_cfg;
 
 typedef struct tng_surrogate_stats {
@@ -231,6 +236,13 @@ int tng_surrogate_params(tng_surrogate* s, float* host, int set);
 /* Normalised FP32 features (n x in_pad, device) of a state batch, for checks and tooling. */
 int tng_surrogate_features(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double p,
                            float* X);
+/* The surrogate's prediction without fallback (device pointers): out (species-major, ld_out)
+ * receives the conserved post-processed state of every cell; reason (nullable, int per cell)
+ * 0 accepted / 1 out of range / 2 inconsistent / 3 clipped; indicator (nullable, double per
+ * cell) the network-vs-enthalpy temperature mismatch in K. dts per cell or the scalar dt. */
+int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, int64_t ncells, int64_t ld,
+                          const double* dts, double dt, double p, double* out, int64_t ld_out, int* reason,
+                          double* indicator);
 /* FP32 reference forward of the network on normalised features (device pointers). */
 int tng_surrogate_forward_f32(tng_surrogate* s, const float* X, int64_t n, float* Y);
 /* Tensor-core inference only: normalised predictions (n x out_pad FP32, device) of a state batch. */

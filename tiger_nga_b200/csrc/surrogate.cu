@@ -39,9 +39,14 @@ struct SurPost {
   const double* E;   // nel x ns: element atoms per kg of species (a_ek / W_k)
   const double* th;  // ns x 24 NASA (hi 12, lo 12)
   double tmid;
+  int post_mode;     // 0: T from the enthalpy balance; 1: T from the network, enthalpy in the projection
   int* fb_list;      // fallback cells
   int* fb_count;
   unsigned long long* cnt;  // [accepted, ood, consistency, clip]
+  double* out_state;  // predict mode: every cell's post-processed state here (state untouched, no list)
+  long long ld_out;
+  int* reason_out;    // per cell, nullable
+  double* ind_out;    // per cell, nullable
 };
 
 __device__ __forceinline__ void nasa(const double* th, double tmid, int k, double T, double* h, double* cp) {
@@ -150,6 +155,82 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 }
 
 // prediction -> state with conservation; fallback cells keep their state and are listed
+// Smallest change of dY in the metric sum dY'^2/D_k that satisfies the linear constraints
+// A dY = b (rows: the nel element rows of E, then optionally one enthalpy row), by the normal
+// equations (Cholesky). Species driven below zero are pinned at zero (dY = -Y0, weight 0) and
+// the projection repeated over the rest (an active set), so clipping keeps the constraints.
+// Returns false when the constraints cannot be met (no free carrier of some constraint).
+__device__ bool project(const SurPost& a, const double* Y0, double* dY, double* D, const double* hrow, double hrhs) {
+  const int nc = a.nel + (hrow ? 1 : 0);
+  auto A = [&](int e, int k) { return e < a.nel ? a.E[e * a.ns + k] : hrow[k]; };
+  for (int pass = 0; pass < 4; ++pass) {
+    double G[kMaxEl + 1][kMaxEl + 1], r[kMaxEl + 1];
+    for (int e = 0; e < nc; ++e) {
+      r[e] = e < a.nel ? 0.0 : -hrhs;
+      for (int k = 0; k < a.ns; ++k) r[e] += A(e, k) * dY[k];
+      for (int g = 0; g <= e; ++g) {
+        double sg = 0.0;
+        for (int k = 0; k < a.ns; ++k) sg += A(e, k) * D[k] * A(g, k);
+        G[e][g] = G[g][e] = sg;
+      }
+    }
+    double Lc[kMaxEl + 1][kMaxEl + 1];
+    for (int i = 0; i < nc; ++i)
+      for (int j = 0; j <= i; ++j) {
+        double sg = G[i][j];
+        for (int q = 0; q < j; ++q) sg -= Lc[i][q] * Lc[j][q];
+        if (i == j) {
+          if (!(sg > 0.0)) return false;
+          Lc[i][i] = sqrt(sg);
+        } else {
+          Lc[i][j] = sg / Lc[j][j];
+        }
+      }
+    double lam[kMaxEl + 1];
+    for (int i = 0; i < nc; ++i) {
+      double sg = r[i];
+      for (int q = 0; q < i; ++q) sg -= Lc[i][q] * lam[q];
+      lam[i] = sg / Lc[i][i];
+    }
+    for (int i = nc - 1; i >= 0; --i) {
+      double sg = lam[i];
+      for (int q = i + 1; q < nc; ++q) sg -= Lc[q][i] * lam[q];
+      lam[i] = sg / Lc[i][i];
+    }
+    bool pinned = false;
+    for (int k = 0; k < a.ns; ++k) {
+      if (D[k] == 0.0) continue;
+      double corr = 0.0;
+      for (int e = 0; e < nc; ++e) corr += A(e, k) * lam[e];
+      dY[k] -= D[k] * corr;
+      if (Y0[k] + dY[k] < 0.0) {
+        dY[k] = -Y0[k];
+        D[k] = 0.0;
+        pinned = true;
+      }
+    }
+    if (!pinned) return true;
+  }
+  return false;  // still pinning species after four passes: leave the cell to the implicit solve
+}
+
+// temperature with sum Y_k h_k(T) = h0 (Newton from T)
+__device__ double enthalpy_T(const SurPost& a, const double* Y, double h0, double T) {
+  for (int it = 0; it < 12; ++it) {
+    double hh = 0.0, cp = 0.0;
+    for (int k = 0; k < a.ns; ++k) {
+      double hk, cpk;
+      nasa(a.th, a.tmid, k, T, &hk, &cpk);
+      hh += Y[k] * hk;
+      cp += Y[k] * cpk;
+    }
+    const double step = (hh - h0) / cp;
+    T -= step;
+    if (fabs(step) < 1e-9 * T) break;
+  }
+  return T;
+}
+
 __global__ void k_sur_post(const SurPost a) {
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells; cell += gridDim.x * blockDim.x) {
     const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
@@ -163,86 +244,62 @@ __global__ void k_sur_post(const SurPost a) {
     }
     double Y0[kMaxNs], dY[kMaxNs], D[kMaxNs];
     const float* o = a.out + (size_t)cell * a.out_pad;
-    const double dT = (double)o[0] * a.tstd[0] + a.tmean[0];
+    const double Tnet = fmin(fmax(T0 + ((double)o[0] * a.tstd[0] + a.tmean[0]), 200.0), 6000.0);
+    double neg = 0.0;  // negative mass fraction the network predicted (clip test)
     for (int k = 0; k < a.ns; ++k) {
       Y0[k] = a.state[(long long)k * a.ld + cell] / rho;
       dY[k] = (double)o[1 + k] * a.tstd[1 + k] + a.tmean[1 + k];
       D[k] = fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12;
+      if (Y0[k] + dY[k] < 0.0) neg -= Y0[k] + dY[k];
     }
-    // element conservation: minimise sum dY'^2/D subject to E dY' = 0 (normal equations, nel <= 8)
-    double G[kMaxEl][kMaxEl], r[kMaxEl];
-    for (int e = 0; e < a.nel; ++e) {
-      r[e] = 0.0;
-      for (int k = 0; k < a.ns; ++k) r[e] += a.E[e * a.ns + k] * dY[k];
-      for (int g = 0; g <= e; ++g) {
-        double s = 0.0;
-        for (int k = 0; k < a.ns; ++k) s += a.E[e * a.ns + k] * D[k] * a.E[g * a.ns + k];
-        G[e][g] = G[g][e] = s;
-      }
-    }
-    // Cholesky solve G lam = r
-    double Lc[kMaxEl][kMaxEl];
-    bool spd = true;
-    for (int i = 0; i < a.nel; ++i)
-      for (int j = 0; j <= i; ++j) {
-        double s = G[i][j];
-        for (int q = 0; q < j; ++q) s -= Lc[i][q] * Lc[j][q];
-        if (i == j) {
-          if (!(s > 0.0)) spd = false;
-          Lc[i][i] = sqrt(fmax(s, 1e-300));
-        } else {
-          Lc[i][j] = s / Lc[j][j];
-        }
-      }
-    double lam[kMaxEl];
-    for (int i = 0; i < a.nel; ++i) {
-      double s = r[i];
-      for (int q = 0; q < i; ++q) s -= Lc[i][q] * lam[q];
-      lam[i] = s / Lc[i][i];
-    }
-    for (int i = a.nel - 1; i >= 0; --i) {
-      double s = lam[i];
-      for (int q = i + 1; q < a.nel; ++q) s -= Lc[q][i] * lam[q];
-      lam[i] = s / Lc[i][i];
-    }
-    double Y1[kMaxNs], neg = 0.0, sum = 0.0;
-    for (int k = 0; k < a.ns; ++k) {
-      double corr = 0.0;
-      if (spd)
-        for (int e = 0; e < a.nel; ++e) corr += a.E[e * a.ns + k] * lam[e];
-      double y = Y0[k] + dY[k] - D[k] * corr;
-      if (y < 0.0) {
-        neg -= y;
-        y = 0.0;
-      }
-      Y1[k] = y;
-      sum += y;
-    }
-    for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
-    // temperature from the enthalpy balance
     double h0 = 0.0;
     for (int k = 0; k < a.ns; ++k) {
       double hk, cpk;
       nasa(a.th, a.tmid, k, T0, &hk, &cpk);
       h0 += Y0[k] * hk;
     }
-    double T1 = fmin(fmax(T0 + dT, 200.0), 6000.0);
-    for (int it = 0; it < 12; ++it) {
-      double hh = 0.0, cp = 0.0;
+    // element conservation, then the temperature the conserved Y implies
+    bool ok = project(a, Y0, dY, D, nullptr, 0.0);
+    double Y1[kMaxNs], sum = 0.0;
+    for (int k = 0; k < a.ns; ++k) {
+      Y1[k] = fmax(Y0[k] + dY[k], 0.0);
+      sum += Y1[k];
+    }
+    for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
+    double T1 = enthalpy_T(a, Y1, h0, Tnet);
+    const double ind = fabs(T1 - Tnet);
+    if (ok && a.post_mode == 1) {
+      // keep the network's temperature: move Y (elements held) until h(Y, Tnet) = h0
+      double hrow[kMaxNs], cpm = 0.0, hy = 0.0;
       for (int k = 0; k < a.ns; ++k) {
         double hk, cpk;
-        nasa(a.th, a.tmid, k, T1, &hk, &cpk);
-        hh += Y1[k] * hk;
-        cp += Y1[k] * cpk;
+        nasa(a.th, a.tmid, k, Tnet, &hk, &cpk);
+        hrow[k] = hk;
+        cpm += Y1[k] * cpk;
       }
-      const double step = (hh - h0) / cp;
-      T1 -= step;
-      if (fabs(step) < 1e-9 * T1) break;
+      const double sc = 1.0 / (cpm * Tnet);  // enthalpy row in units of cp*T
+      for (int k = 0; k < a.ns; ++k) {
+        hrow[k] *= sc;
+        hy += hrow[k] * Y0[k];
+      }
+      ok = project(a, Y0, dY, D, hrow, h0 * sc - hy);
+      sum = 0.0;
+      for (int k = 0; k < a.ns; ++k) {
+        Y1[k] = fmax(Y0[k] + dY[k], 0.0);
+        sum += Y1[k];
+      }
+      for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
+      T1 = enthalpy_T(a, Y1, h0, Tnet);  // one correction for the renormalisation
     }
-    if (!reason && !(fabs(T1 - (T0 + dT)) <= a.consist_tol)) reason = 2;
+    if (!reason && !(ind <= a.consist_tol)) reason = 2;
     if (!reason && !(neg <= a.clip_tol)) reason = 3;
-    if (!reason && !(isfinite(T1) && spd)) reason = 2;
-    if (reason) {
+    if (!reason && !(isfinite(T1) && ok)) reason = 2;
+    if (a.reason_out) a.reason_out[cell] = reason;
+    if (a.ind_out) a.ind_out[cell] = ok ? ind : INFINITY;
+    if (a.out_state) {
+      for (int k = 0; k < a.ns; ++k) a.out_state[(long long)k * a.ld_out + cell] = rho * Y1[k];
+      a.out_state[(long long)a.ns * a.ld_out + cell] = rho * T1;
+    } else if (reason) {
       const int slot = atomicAdd(a.fb_count, 1);
       a.fb_list[slot] = cell;
       atomicAdd(&a.cnt[reason], 1ULL);
@@ -370,6 +427,38 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "tensor-core inference");
 }
 
+namespace tng {
+// arguments of the post-processing kernel common to the substep and the plain prediction
+static SurPost post_args(tng_chem* h, tng_surrogate* s, double* state, int64_t ld, int64_t ncells, const double* dts,
+                         double dt, double p) {
+  SurPost pa{};
+  pa.state = state;
+  pa.ld = ld;
+  pa.ncells = (int)ncells;
+  pa.dts = dts;
+  pa.dt_scalar = dt;
+  pa.logp = std::log(p);
+  pa.ns = s->ns;
+  pa.bath = s->bath;
+  pa.n_in = s->n_in;
+  pa.n_out = s->n_out;
+  pa.out_pad = s->m.out_pad;
+  pa.nel = s->nel;
+  pa.out = (const float*)s->out.ptr;
+  pa.tmean = s->d_tnorm;
+  pa.tstd = s->d_tnorm + s->m.out_pad;
+  pa.fmin = s->d_fnorm + 2 * s->m.in_pad;
+  pa.fmax = s->d_fnorm + 3 * s->m.in_pad;
+  pa.margin = s->cfg.ood_margin;
+  pa.consist_tol = s->cfg.consist_tol_K;
+  pa.clip_tol = s->cfg.clip_tol;
+  pa.post_mode = s->cfg.post_mode;
+  pa.E = s->d_E;
+  solver_thermo(h, &pa.th, &pa.tmid);
+  return pa;
+}
+}  // namespace tng
+
 extern "C" {
 
 void tng_surrogate_default_cfg(tng_surrogate_cfg* c) {
@@ -487,11 +576,17 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
     s->fmin[i] = hs[4 * i + 2];
     s->fmax[i] = hs[4 * i + 3];
   }
+  double shared = 0.0;  // target_mode 1: the RMS spread over the species outputs, one scale for all
   for (int i = 0; i < s->n_out; ++i) {
     const double* q = &hs[4 * (ip + i)];
     const double mu = q[0] / n, var = std::max(q[1] / n - mu * mu, 0.0);
     s->tmean[i] = mu;
     s->tstd[i] = std::max(std::sqrt(var), 1e-14);
+    if (i > 0) shared += var;
+  }
+  if (s->cfg.target_mode == 1) {
+    shared = std::max(std::sqrt(shared / std::max(1, s->n_out - 1)), 1e-14);
+    for (int i = 1; i < s->n_out; ++i) s->tstd[i] = shared;
   }
   int rc = sur_upload_norm(s);
   if (rc) return rc;
@@ -502,9 +597,10 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
   cudaMemcpyAsync(nrm, hn.data(), sizeof(float) * hn.size(), cudaMemcpyHostToDevice, st);
   k_normalise<<<2048, 256, 0, st>>>(X, (int)n, ip, s->n_in, nrm, nrm + ip);
   k_normalise<<<2048, 256, 0, st>>>(T, (int)n, op, s->n_out, nrm + 2 * ip, nrm + 2 * ip + op);
-  // loss weights: every output equally (outputs are normalised), temperature doubled
+  // loss weights: every species output equally (outputs are normalised), temperature wT
   std::vector<float> w(op, 0.f);
-  for (int i = 0; i < s->n_out; ++i) w[i] = i == 0 ? 2.f : 1.f;
+  const float wT = s->cfg.loss_T_weight > 0.f ? s->cfg.loss_T_weight : 2.f;
+  for (int i = 0; i < s->n_out; ++i) w[i] = i == 0 ? wT : 1.f;
   float* dw;
   if ((e = cudaMalloc(&dw, sizeof(float) * op)) != cudaSuccess) return cuda_error(e, "loss weights");
   cudaMemcpyAsync(dw, w.data(), sizeof(float) * op, cudaMemcpyHostToDevice, st);
@@ -712,29 +808,7 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   if (rc) return rc;
   cudaEventRecord(s->ev[1], st);
   // post-processing and fallback list
-  SurPost pa{};
-  pa.state = dstate;
-  pa.ld = dld;
-  pa.ncells = (int)ncells;
-  pa.dts = ddts;
-  pa.dt_scalar = dt;
-  pa.logp = std::log(p);
-  pa.ns = s->ns;
-  pa.bath = s->bath;
-  pa.n_in = s->n_in;
-  pa.n_out = s->n_out;
-  pa.out_pad = s->m.out_pad;
-  pa.nel = s->nel;
-  pa.out = (const float*)s->out.ptr;
-  pa.tmean = s->d_tnorm;
-  pa.tstd = s->d_tnorm + s->m.out_pad;
-  pa.fmin = s->d_fnorm + 2 * s->m.in_pad;
-  pa.fmax = s->d_fnorm + 3 * s->m.in_pad;
-  pa.margin = s->cfg.ood_margin;
-  pa.consist_tol = s->cfg.consist_tol_K;
-  pa.clip_tol = s->cfg.clip_tol;
-  pa.E = s->d_E;
-  solver_thermo(h, &pa.th, &pa.tmid);
+  SurPost pa = post_args(h, s, dstate, dld, ncells, ddts, dt, p);
   pa.fb_list = fb_list;
   pa.fb_count = fb_count;
   pa.cnt = cnt;
@@ -785,6 +859,40 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
       stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3]);
     }
   }
+  return TNG_OK;
+}
+
+int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, int64_t ncells, int64_t ld,
+                          const double* dts, double dt, double p, double* out, int64_t ld_out, int* reason,
+                          double* indicator) {
+  if (!h || !s || s->h != h) return set_error(TNG_ERR_ARG, "tng_surrogate_predict: handle/surrogate mismatch");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_predict: surrogate not trained or loaded");
+  if (ncells < 0 || ld < ncells || ld_out < ncells || ncells > (1LL << 31) - 1)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_predict: need 0 <= ncells <= ld, ld_out < 2^31");
+  if (ncells == 0) return TNG_OK;
+  if (!state || !out || !(p > 0.0) || (!dts && !(dt >= 0.0)))
+    return set_error(TNG_ERR_ARG, "tng_surrogate_predict: bad argument");
+  DeviceGuard g(h->cfg.device);
+  cudaStream_t st = h->stream;
+  if (!s->out.reserve((size_t)ncells * s->m.out_pad * sizeof(float)) || !s->cnt.reserve(16 * sizeof(unsigned long long)))
+    return set_error(TNG_ERR_CUDA, "tng_surrogate_predict: scratch allocation failed");
+  int rc = solver_prepare(h);
+  if (rc) return rc;
+  unsigned long long* cnt = (unsigned long long*)s->cnt.ptr;
+  cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), st);
+  rc = launch_infer(h, s, state, ncells, ld, dts, dt, p, (float*)s->out.ptr, (int*)(cnt + 8));
+  if (rc) return rc;
+  SurPost pa = post_args(h, s, const_cast<double*>(state), ld, ncells, dts, dt, p);
+  pa.out_state = out;
+  pa.ld_out = ld_out;
+  pa.reason_out = reason;
+  pa.ind_out = indicator;
+  k_sur_post<<<(int)std::min<int64_t>(4096, (ncells + 127) / 128), 128, 0, st>>>(pa);
+  unsigned long long flag = 0;
+  cudaMemcpyAsync(&flag, cnt + 8, sizeof(flag), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_predict");
+  if (flag) return set_error(TNG_ERR_CUDA, "tng_surrogate_predict: tensor-core inference timed out");
   return TNG_OK;
 }
 

@@ -1,0 +1,168 @@
+"""Train the learned substep of a mechanism on pairs from the plain implicit GPU solver.
+
+    python -m tiger_nga_b200.train_surrogate --mech grimech30 --pairs 8388608 \\
+        --out tiger_nga_b200/models/grimech30.tngs
+
+Pairs: seeded states of the uneven-stiffness batch -- 128^3 grids of a smooth Fourier-mode
+mixture-fraction field (CH4 fuel / air at 300 K for GRI-Mech, DME at 400 K for DME39),
+progress c ~ Beta(2,2) mapped to T in [300, 2400] K, minor species log-uniform in
+[1e-10, 1e-3], dt log-uniform in [1e-7, 1e-5] s per cell, P = 1 atm -- each advanced by
+tng_substep_batch. The network is trained by the library's own CUDA kernels
+(tng_surrogate_train: FP32 forward/backward, Adam, cosine learning rate), then evaluated
+on fresh cells against the plain solve (accepted fraction, max relative error of T, max
+species error over max Y). Writes the weights file and a JSON log beside it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import capi, states
+from .mechanism import load
+
+FUEL = {"grimech30": ("CH4", 300.0), "dme39": ("CH3OCH3", 400.0), "hydrogen": ("H2", 300.0)}
+P_ATM = 101325.0
+
+
+def state_batch(mech_name: str, n: int, seed: int, side: int = 128):
+    """Seeded (state (N+1, n), dt (n,)) of the uneven-stiffness distribution, on the host."""
+    m = load(mech_name)
+    fuel, t_fuel = FUEL[mech_name]
+    grid = (side, side, side) if side ** 3 == n else (n, 1, 1)
+    sol, _ = states.chem_state(m, n, seed, fuel, T_fuel=t_fuel, progress="beta22", T_range=(300.0, 2400.0), grid=grid)
+    rng = np.random.default_rng(seed + 104729)
+    dts = 10.0 ** rng.uniform(-7.0, -5.0, n)
+    return sol, dts
+
+
+def make_pairs(chem, n_pairs: int, seed: int, chunk: int = 1 << 21):
+    """(s0, s1, dt) device tensors of n_pairs cells; s1 = plain implicit solve of s0 over dt."""
+    import torch
+
+    nv = chem.nspecies + 1
+    s0 = torch.empty((nv, n_pairs), dtype=torch.float64, device="cuda")
+    s1 = torch.empty_like(s0)
+    d = torch.empty(n_pairs, dtype=torch.float64, device="cuda")
+    done, k, solve_s = 0, 0, 0.0
+    while done < n_pairs:
+        m = min(chunk, n_pairs - done)
+        sol, dts = state_batch(chem.mechanism, m, seed + 1000 * k, side=128 if m == 1 << 21 else 0)
+        s0[:, done:done + m].copy_(torch.from_numpy(sol))
+        d[done:done + m].copy_(torch.from_numpy(dts))
+        x = s0[:, done:done + m].contiguous()
+        t0 = time.perf_counter()
+        chem.substep(x, d[done:done + m], P_ATM)
+        torch.cuda.synchronize()
+        solve_s += time.perf_counter() - t0
+        s1[:, done:done + m].copy_(x)
+        done += m
+        k += 1
+    return s0, s1, d, solve_s
+
+
+def evaluate(chem, sur, n: int, seed: int, tolerances=(1.0, 2.0, 5.0, 10.0, 20.0)):
+    """The surrogate against the plain solve on n fresh cells.
+
+    Returns the timed surrogate-with-fallback substep (stats, speed-up over the plain solve) and,
+    from the fallback-free prediction of every cell, the error of the cells each consistency
+    tolerance (K) would accept, with the plain solver's share of steps those cells leave to the
+    fallback. Per-cell arrays (errors, indicator, reason, T0, dt, steps) are returned as well.
+    """
+    import torch
+
+    sol, dts = state_batch(chem.mechanism, n, seed, side=128 if n == 1 << 21 else 0)
+    s0 = torch.from_numpy(sol).cuda()
+    d = torch.from_numpy(dts).cuda()
+    ref = s0.clone()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, cnt = chem.substep(ref, d, P_ATM, cell_counts=True)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    x = s0.clone()
+    t0 = time.perf_counter()
+    st = sur.substep(x, d, P_ATM)
+    torch.cuda.synchronize()
+    t_sur = time.perf_counter() - t0
+    ns = chem.nspecies
+
+    def errors(y):
+        ry, rr = y[:ns].sum(0), ref[:ns].sum(0)
+        eT = ((y[ns] / ry - ref[ns] / rr).abs() / (ref[ns] / rr))
+        eY = ((y[:ns] / ry - ref[:ns] / rr).abs().amax(0) / (ref[:ns] / rr).amax(0))
+        return eT.cpu().numpy(), eY.cpu().numpy()
+
+    errT_run, errY_run = errors(x)
+    pred, reason, ind = sur.predict(s0, d, P_ATM)
+    eT, eY = errors(pred)
+    reason = reason.cpu().numpy()
+    ind = ind.cpu().numpy()
+    nst = cnt["nst"].cpu().numpy().astype(np.float64)
+    hard = (reason == 1) | (reason == 3)
+    curve = []
+    for tol in tolerances:
+        acc = (~hard) & (ind <= tol)
+        curve.append({"tol_K": tol, "accepted": float(acc.mean()),
+                      "max_rel_T": float(eT[acc].max()) if acc.any() else 0.0,
+                      "max_dY_over_maxY": float(eY[acc].max()) if acc.any() else 0.0,
+                      "fallback_step_share": float(nst[~acc].sum() / max(nst.sum(), 1.0))})
+    T0 = (s0[ns] / s0[:ns].sum(0)).cpu().numpy()
+    summary = {
+        "cells": n, "plain_s": t_plain, "surrogate_s": t_sur, "speedup": t_plain / t_sur,
+        "accepted": st["accepted"], "fallback": st["fallback"]["cells"], "fallback_ood": st["fallback_ood"],
+        "fallback_consistency": st["fallback_consistency"], "fallback_clip": st["fallback_clip"],
+        "max_rel_T": float(errT_run.max()), "p99_rel_T": float(np.quantile(errT_run, 0.99)),
+        "max_dY_over_maxY": float(errY_run.max()), "p99_dY_over_maxY": float(np.quantile(errY_run, 0.99)),
+        "judge_max_rel_dT": st["judge_max_rel_dT"], "judge_max_dY": st["judge_max_dY"],
+        "ms_infer": st["ms_infer"], "ms_post": st["ms_post"], "ms_fallback": st["ms_fallback"],
+        "prediction_max_rel_T": float(eT.max()), "prediction_p99_rel_T": float(np.quantile(eT, 0.99)),
+        "tolerance_curve": curve,
+    }
+    cells = {"errT": eT.astype(np.float32), "errY": eY.astype(np.float32), "ind": ind.astype(np.float32),
+             "reason": reason.astype(np.int8), "T0": T0.astype(np.float32), "dt": dts.astype(np.float32),
+             "nst": nst.astype(np.int32)}
+    return summary, cells
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--mech", default="grimech30")
+    ap.add_argument("--pairs", type=int, default=1 << 23)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--eval-cells", type=int, default=1 << 18)
+    ap.add_argument("--target-mode", type=int, default=0)
+    ap.add_argument("--post-mode", type=int, default=0)
+    ap.add_argument("--loss-T-weight", type=float, default=2.0)
+    ap.add_argument("--consist-tol", type=float, default=5.0)
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+    chem = capi.FiniteChem(a.mech, "fp64")
+    t0 = time.perf_counter()
+    s0, s1, d, solve_s = make_pairs(chem, a.pairs, a.seed)
+    t_pairs = time.perf_counter() - t0
+    sur = capi.Surrogate(chem, target_mode=a.target_mode, post_mode=a.post_mode, loss_T_weight=a.loss_T_weight,
+                         consist_tol_K=a.consist_tol)
+    t0 = time.perf_counter()
+    losses = sur.train(s0, s1, d, P_ATM, epochs=a.epochs, batch=a.batch, lr=a.lr)
+    t_train = time.perf_counter() - t0
+    del s0, s1, d
+    sur.save(a.out)
+    ev, _ = evaluate(chem, sur, a.eval_cells, a.seed + 99991)
+    log = {"mechanism": a.mech, "pairs": a.pairs, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
+           "target_mode": a.target_mode, "post_mode": a.post_mode, "loss_T_weight": a.loss_T_weight,
+           "consist_tol_K": a.consist_tol,
+           "pairs_s": t_pairs, "plain_solve_s": solve_s, "train_s": t_train,
+           "losses": [float(v) for v in losses], "eval": ev}
+    with open(a.out + ".json", "w") as f:
+        json.dump(log, f, indent=1)
+    print(json.dumps(log))
+
+
+if __name__ == "__main__":
+    main()
