@@ -2,17 +2,29 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl tiger|reference]
 
-Workloads (seeded synthetic states, built like the reference's init_flow tool):
-  gri-rates        GRI-Mech 3.0 C/H/O subset (36 species, 422 slots -- the reference's grimech30F
-                   stand-in for the 53/325 mechanism), production-rate evaluation only
-                   (finitechem_compute_rhs + PRODRATES), 128^3 = 2,097,152 cells, FP64, P = 1 atm.
+Workloads (seeded synthetic states, built like the reference's init_flow tool; the GRI-Mech
+3.0 workloads run the reference's 36-species / 422-slot grimech30F stand-in):
+
+  gri-surrogate    (default) one chemistry substep of 2,097,152 cells (a 128^3 grid) through
+                   the learned surrogate with fallback to the implicit solve: smooth seeded
+                   mixture-fraction field, CH4 / air at 300 K, progress c ~ Beta(2,2) mapped to
+                   T in [300, 2400] K, minor species log-uniform in [1e-10, 1e-3], per-cell dt
+                   log-uniform in [1e-7, 1e-5] s, P = 1 atm. The plain implicit GPU solve of the
+                   same cells (a strided subsample) is timed beside it and is the accuracy
+                   reference (max relative T error, max |dY| / max Y).
+  gri-substep      the plain implicit substep (BDF/Newton, persistent work-stealing kernel in a
+                   CUDA graph, FP64 LU) of the same 2,097,152-cell batch.
+  h2-substep       the plain implicit substep of the hydrogen mechanism on 32^3 cells, dt = 1e-6 s.
+  gri-rates        production-rate evaluation only (finitechem_compute_rhs + PRODRATES),
+                   128^3 cells, FP64.
   gri-rates-mixed  the same in mixed precision (FP32 log-space rates, FP64 reverse exponents).
 
-A step is one pass of the hot path over the whole batch. `value` is device-timed with CUDA
-events on the library's stream, inputs resident in HBM (1.24 GB per pass > 126 MB L2, so no
-L2 flush is needed); `e2e` is the same metric through the C-ABI with pinned host buffers,
-host<->device copies inside the timed region. Multi-GPU: every rank owns its own batch
-(cells are independent, no collective on the data path); the step time is the max over ranks.
+A step is one pass of the hot path over the whole batch, starting every time from the same
+initial state (restored outside the timed interval). `value` is device-timed with CUDA events
+on the library's stream, inputs resident in HBM (every batch is larger than the 126 MB L2);
+`e2e` is the same metric through the C-ABI with pinned host buffers, host<->device copies
+inside the timed region. Multi-GPU: every rank owns its own batch (cells are independent, no
+collective on the data path); the step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -30,13 +42,32 @@ sys.path.insert(0, REPO)
 
 import numpy as np  # noqa: E402
 
-WORKLOADS = {
-    "gri-rates": {"mech": "grimech30", "n": 128, "precision": "fp64", "fuel": "CH4",
-                  "desc": "GRI-Mech 3.0 C/H/O subset (36 sp, 422 slots) rates, 128^3 cells, FP64"},
-    "gri-rates-mixed": {"mech": "grimech30", "n": 128, "precision": "mixed", "fuel": "CH4",
-                        "desc": "GRI-Mech 3.0 C/H/O subset (36 sp, 422 slots) rates, 128^3 cells, mixed FP32/FP64"},
-}
 P_ATM = 101325.0
+SURROGATE_FILE = os.path.join(REPO, "tiger_nga_b200", "models", "grimech30.tngs")
+WORKLOADS = {
+    "gri-surrogate": {"kind": "surrogate", "mech": "grimech30", "side": 128, "precision": "fp64",
+                      "metric": "GRI-3.0 substep cells/s: surrogate+fallback vs plain GPU at ≤1% ΔT error",
+                      "desc": "GRI-Mech 3.0 stand-in (36 sp) substep, 128^3 cells, per-cell dt 1e-7..1e-5 s, "
+                              "surrogate (tcgen05 BF16 MLP) + implicit fallback", "steps": 5, "ref_sample": 2048},
+    "gri-substep": {"kind": "substep", "mech": "grimech30", "side": 128, "precision": "fp64",
+                    "metric": "GRI-3.0 (36-sp stand-in) implicit substep cells/s",
+                    "desc": "GRI-Mech 3.0 stand-in (36 sp) implicit substep, 128^3 cells, per-cell dt 1e-7..1e-5 s",
+                    "steps": 1, "ref_sample": 2048},
+    "h2-substep": {"kind": "substep", "mech": "hydrogen", "side": 32, "precision": "fp64",
+                   "metric": "H2 implicit substep cells/s",
+                   "desc": "hydrogen (9 sp) implicit substep, 32^3 cells, dt = 1e-6 s", "steps": 20,
+                   "ref_sample": 16384},
+    "gri-rates": {"kind": "rates", "mech": "grimech30", "side": 128, "precision": "fp64",
+                  "metric": "GRI-3.0 (36-sp stand-in) rate evaluation cells/s",
+                  "desc": "GRI-Mech 3.0 stand-in (36 sp, 422 slots) rates, 128^3 cells, FP64", "steps": 400,
+                  "ref_sample": 131072},
+    "gri-rates-mixed": {"kind": "rates", "mech": "grimech30", "side": 128, "precision": "mixed",
+                        "metric": "GRI-3.0 (36-sp stand-in) rate evaluation cells/s",
+                        "desc": "GRI-Mech 3.0 stand-in (36 sp, 422 slots) rates, 128^3 cells, mixed FP32/FP64",
+                        "steps": 400, "ref_sample": 131072},
+}
+# kernels of this library launched per step (counted from the host code of each path)
+LAUNCHES = {"rates": 1, "substep": 2, "surrogate": 8}
 
 
 def dist_env():
@@ -100,120 +131,173 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def read_traffic(profile: str):
-    """DRAM bytes per cell recorded in a committed ncu summary (line 'dram_bytes_per_cell: X')."""
+def read_profile_value(profile: str, key: str):
+    """A number recorded in a committed ncu summary (line '<key>: X')."""
     path = os.path.join(REPO, "profiles", profile)
     if not os.path.exists(path):
         return None
     for ln in open(path):
-        if ln.startswith("dram_bytes_per_cell:"):
+        if ln.startswith(key + ":"):
             return float(ln.split(":", 1)[1])
     return None
 
 
-def cpu_rhs_runner():
+def make_state(wl, rank):
+    """Seeded host state (N+1, n) and per-cell dt (or a scalar) of a workload."""
+    from tiger_nga_b200 import states
+    from tiger_nga_b200.mechanism import load
+
+    mech = load(wl["mech"])
+    n = wl["side"] ** 3
+    seed = 20261204 + rank
+    if wl["mech"] == "hydrogen":
+        sol, _ = states.h2_cube(mech, wl["side"], seed)
+        return sol, 1e-6
+    if wl["kind"] == "rates":
+        sol, _ = states.chem_state(mech, n, seed, "CH4", grid=(wl["side"],) * 3)
+        return sol, None
+    from tiger_nga_b200.train_surrogate import state_batch
+
+    return state_batch(wl["mech"], n, seed, side=wl["side"])
+
+
+# ---- host-core baselines (the oracle / transliterated reference; never the product path) ----
+def cpu_rates_runner(mech):
     """The reference's own rate arithmetic on the host cores: the transliterated Fortran
     (oracle/_ref) when it was built, else the table-driven oracle port."""
     from oracle.oracle import REF_LIB, Oracle, Reference
 
-    def make(mech):
-        if os.path.exists(REF_LIB):
-            return "reference", Reference(mech)
-        return "port", Oracle(mech)
-
-    return make
+    if os.path.exists(REF_LIB):
+        return "reference", Reference(mech)
+    return "port", Oracle(mech)
 
 
-def time_cpu(mech, sol, seconds: float, nthreads: int):
-    kind, impl = cpu_rhs_runner()(mech)
+def cpu_step(wl, impl, sol, dts, lo, m, nthreads):
+    """One bounded sample of the workload on the host cores (cells lo .. lo+m, wrapping)."""
     n = sol.shape[1]
-    chunk = min(n, 131072)
-    impl.rhs_batch(np.ascontiguousarray(sol[:, :1024]), P_ATM, nthreads)  # warm-up
+    idx = (lo + np.arange(m)) % n
+    sub = np.ascontiguousarray(sol[:, idx])
+    if wl["kind"] == "rates":
+        impl.rhs_batch(sub, P_ATM, nthreads)
+    else:
+        d = dts if np.ndim(dts) == 0 else np.ascontiguousarray(dts[idx])
+        impl.substep_batch(sub, d, P_ATM, nthreads=nthreads)
+    return m
+
+
+def cpu_impl(wl):
+    if wl["kind"] == "rates":
+        return cpu_rates_runner(wl["mech"])
+    from oracle.oracle import Oracle
+
+    return "port", Oracle(wl["mech"])
+
+
+def time_cpu(wl, sol, dts, seconds: float, nthreads: int):
+    kind, impl = cpu_impl(wl)
+    m = min(wl["ref_sample"], sol.shape[1])
+    stride = max(1, sol.shape[1] // m)
+    cpu_step(wl, impl, sol, dts, 0, min(m, 256), nthreads)  # warm-up
     done, t0, i = 0, time.perf_counter(), 0
     while True:
-        lo = (i * chunk) % n
-        sub = np.ascontiguousarray(sol[:, lo:lo + chunk])
-        impl.rhs_batch(sub, P_ATM, nthreads)
-        done += sub.shape[1]
+        done += cpu_step(wl, impl, sol, dts, (i * 7919 * stride) % sol.shape[1], m, nthreads)
         i += 1
         el = time.perf_counter() - t0
-        if el >= seconds or done >= 8 * n:
+        if el >= seconds:
             break
     return kind, done / el, done, el
 
 
-def e2e_run(chem, sol, steps, pg, dev, ncells, ws, unit):
-    """Same metric through the C-ABI host-pointer call: pinned host state in, rates out."""
+def reference_arm(args, wl, config, metric, unit):
+    """The reference's CPU implementation of the path on the host cores (rank 0 only)."""
+    sol, dts = make_state(wl, 0)
+    nthreads = os.cpu_count() or 1
+    kind, impl = cpu_impl(wl)
+    m = min(wl["ref_sample"], sol.shape[1])
+    for w in range(args.warmup):
+        cpu_step(wl, impl, sol, dts, w * m, m, nthreads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        cpu_step(wl, impl, sol, dts, (k * 7919 * m) % sol.shape[1], m, nthreads)
+    el = time.perf_counter() - t0
+    val = m * args.steps / el
+    what = ("rate evaluation (transliterated reference Fortran)" if kind == "reference" else
+            "rate evaluation (oracle port)") if wl["kind"] == "rates" else \
+        "implicit BDF/Newton substep (oracle port: the reference's CVODE is not buildable here)"
+    sample = f"{m} cells of the workload per step, {what}, OpenMP over cells"
+    print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
+                      "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+                      "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                      "data": "synthetic", "config": config,
+                      "cpu_baseline": {"value": val, "unit": unit, "cores": nthreads, "kind": kind, "sample": sample},
+                      "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        pk = json.load(open(path))
+        return pk["hbm_gbs"], pk.get("bf16_tflops"), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def max_over_ranks(pg, dev, v):
+    if not pg:
+        return v
     import torch
 
-    hin = torch.from_numpy(sol).pin_memory().numpy()
-    hout = torch.empty(sol.shape, dtype=torch.float64).pin_memory().numpy()
-    chem.compute_rhs(hin, P_ATM, out=hout)  # warm-up (staging buffers)
-    if pg:
-        pg.barrier()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        chem.compute_rhs(hin, P_ATM, out=hout)
-    e2e_s = (time.perf_counter() - t0) / steps
-    if pg:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    return {"value": ncells * ws / e2e_s, "unit": unit, "h2d_bytes_per_step": sol.nbytes * ws,
-            "d2h_bytes_per_step": sol.nbytes * ws}
+    t = torch.tensor([v], device=dev, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def solver_flops(mech, st):
+    """FP64 flops of the implicit solve that can be counted exactly from its statistics: one
+    reference-formulation RHS per Newton iteration, the LU factorisation (2/3 n^3) per Jacobian
+    and the two triangular solves (2 n^2) per Newton iteration. Jacobian assembly, error tests
+    and the Nordsieck history are left out, so this is a lower bound of the work done."""
+    from tiger_nga_b200.workcount import rhs_work
+
+    nv = mech.ns + 1
+    rf = rhs_work(mech)["flops"]
+    return st["newton_iters"] * (rf + 2 * nv * nv) + st["jacobians"] * (2.0 / 3.0) * nv ** 3
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="gri-rates", choices=sorted(WORKLOADS))
+    ap.add_argument("--steps", type=int, default=0, help="timed steps (0: the workload's default)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="gri-surrogate", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="tiger", choices=["tiger", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--n", type=int, default=0, help="cube side override (small profiling cases)")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (0: min(steps, 3))")
+    ap.add_argument("--plain-cells", type=int, default=262144,
+                    help="gri-surrogate: cells of the strided subsample solved by the plain GPU path (0 = all)")
+    ap.add_argument("--side", type=int, default=0, help="cube side override (small profiling cases)")
+    ap.add_argument("--surrogate", default=SURROGATE_FILE)
     args = ap.parse_args()
     ws, rank, local = dist_env()
     wl = dict(WORKLOADS[args.workload])
-    if args.n:
-        wl["n"] = args.n
-    from tiger_nga_b200 import states
+    if args.side:
+        wl["side"] = args.side
+    if args.steps <= 0:
+        args.steps = wl["steps"]
+    args.warmup = max(args.warmup, 3)
     from tiger_nga_b200.mechanism import load
-    from tiger_nga_b200.workcount import rhs_work
 
     mech = load(wl["mech"])
-    work = rhs_work(mech)
-    ncells = wl["n"] ** 3
+    ncells = wl["side"] ** 3
     config = {"workload": args.workload, "desc": wl["desc"], "mechanism": wl["mech"], "cells_per_gpu": ncells,
-              "pressure_pa": P_ATM, "precision": wl["precision"], "l2": "inputs larger than L2 (1.24 GB/pass)",
+              "pressure_pa": P_ATM, "precision": wl["precision"],
+              "l2": "inputs larger than L2 (no flush needed)" if ncells * (mech.ns + 1) * 8 > 126e6 else
+              "inputs smaller than L2 (state restored from a copy before every step)",
               "parallelism": f"cells sharded, {ws} independent GPU(s)"}
-    metric = "GRI-3.0 (36-sp stand-in) rate evaluation cells/s"
-    unit = "cells/s"
+    metric, unit = wl["metric"], "cells/s"
 
     if args.impl == "reference":
-        if rank != 0:
-            return 0
-        sol, _ = states.chem_state(mech, ncells, 20261204 + rank, wl["fuel"], grid=(wl["n"],) * 3)
-        nthreads = os.cpu_count() or 1
-        kind, impl = cpu_rhs_runner()(wl["mech"])
-        chunk = 131072
-        for w in range(args.warmup):
-            impl.rhs_batch(np.ascontiguousarray(sol[:, :chunk]), P_ATM, nthreads)
-        t0 = time.perf_counter()
-        for k in range(args.steps):
-            lo = (k * chunk) % ncells
-            impl.rhs_batch(np.ascontiguousarray(sol[:, lo:lo + chunk]), P_ATM, nthreads)
-        el = time.perf_counter() - t0
-        val = chunk * args.steps / el
-        sample = f"{chunk} cells of the workload per step"
-        print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
-                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
-                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                          "data": "synthetic", "config": config,
-                          "cpu_baseline": {"value": val, "unit": unit, "cores": nthreads, "kind": kind,
-                                           "sample": sample},
-                          "e2e": {"value": val, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        if rank == 0:
+            reference_arm(args, wl, config, metric, unit)
         return 0
 
     import torch
@@ -226,89 +310,219 @@ def main():
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
         pg = dist
     from tiger_nga_b200 import capi
 
-    sol, _ = states.chem_state(mech, ncells, 20261204 + rank, wl["fuel"], grid=(wl["n"],) * 3)
+    sol, dts = make_state(wl, rank)
     chem = capi.FiniteChem(wl["mech"], wl["precision"], device=local)
-    x = torch.from_numpy(sol).to(dev)
-    y = torch.empty_like(x)
     st = chem.torch_stream()
-    torch.cuda.synchronize()
-    for _ in range(max(args.warmup, 3)):
-        chem.launch_rhs(x.data_ptr(), y.data_ptr(), ncells, ncells, P_ATM)
-    chem.sync()
+    x0 = torch.from_numpy(sol).to(dev)
+    d_dev = torch.from_numpy(dts).to(dev) if dts is not None and np.ndim(dts) else dts
+    extra = {}
+    sur = None
+    if wl["kind"] == "surrogate":
+        if not os.path.exists(args.surrogate):
+            raise FileNotFoundError(f"trained surrogate weights not found: {args.surrogate}")
+        sur = capi.Surrogate(chem)
+        sur.load(args.surrogate)
+
+    work = torch.empty_like(x0)
+    out = torch.empty_like(x0)
+    stats_last = {}
+
+    def step():
+        """One timed pass; returns its device time in ms (events on the library stream)."""
+        if wl["kind"] != "rates":
+            work.copy_(x0)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        if wl["kind"] == "rates":
+            chem.launch_rhs(x0.data_ptr(), out.data_ptr(), ncells, ncells, P_ATM)
+        elif wl["kind"] == "substep":
+            r = chem.substep(work, d_dev, P_ATM, stats=True)
+            stats_last.update(r)
+        else:
+            r = sur.substep(work, d_dev, P_ATM)
+            stats_last.update(r)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    for _ in range(args.warmup):
+        step()
     if pg:
         pg.barrier()
-    torch.cuda.synchronize()
+    torch.cuda.synchronize(dev)
     uuid = str(torch.cuda.get_device_properties(dev).uuid)
     clocks = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
     clocks.start()
     time.sleep(0.3)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(args.steps):
-        chem.launch_rhs(x.data_ptr(), y.data_ptr(), ncells, ncells, P_ATM)
-    e1.record(st)
-    e1.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    if pg:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_step = ms / args.steps
-    value = ncells * ws / (ms_step * 1e-3)
-    if not bool(torch.isfinite(y).all()):
-        raise RuntimeError("non-finite rates in the benchmark output")
-
-    # ---- e2e through the C-ABI with pinned host buffers -------------------------------------
-    e2e = None
-    nbytes = sol.nbytes
-    if args.e2e_steps > 0:
-        e2e = e2e_run(chem, sol, args.e2e_steps, pg, dev, ncells, ws, unit)
-
-    # ---- roofline of the rate kernel ----------------------------------------------------------
-    hout = torch.empty(sol.shape, dtype=torch.float64).pin_memory().numpy()
-    peaks_path = os.path.join(REPO, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peaks = json.load(open(peaks_path))
-        hbm_peak, src = peaks["hbm_gbs"], "measured"
+    if wl["kind"] == "rates":
+        # back-to-back launches, one event pair around all K (the kernel is ~1 ms)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(st)
+        for _ in range(args.steps):
+            chem.launch_rhs(x0.data_ptr(), out.data_ptr(), ncells, ncells, P_ATM)
+        e1.record(st)
+        e1.synchronize()
+        ms_total = e0.elapsed_time(e1)
     else:
-        hbm_peak, src = 6650.0, "fallback"
-    alg_bytes = work["bytes"] * ncells
-    achieved = alg_bytes / (ms_step * 1e-3) / 1e9
-    fp64_peak = capi.fp64_peak_tflops(local)
-    alg_flops = work["flops"] * ncells
-    fp64_ach = alg_flops / (ms_step * 1e-3) / 1e12
-    tr = read_traffic(f"k_rhs_{wl['mech']}_{wl['precision']}.txt")
-    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-            "traffic": tr * ncells if tr else None, "peak_source": src,
-            "algorithmic_bytes_per_cell": work["bytes"],
-            "fp64_pipe": {"achieved_tflops": fp64_ach, "peak_tflops_measured": fp64_peak,
-                          "frac": fp64_ach / fp64_peak, "alg_flops_per_cell": work["flops"],
-                          "transcendentals_per_cell": work["transcendentals"],
-                          "note": "reference-formulation flops (transcendentals counted separately); "
-                                  "the kernel is FP64-pipe bound, the HBM figure is reported per schema"}}
+        ms_total = sum(step() for _ in range(args.steps))
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms_total = max_over_ranks(pg, dev, ms_total)
+    ms_step = ms_total / args.steps
+    value = ncells * ws / (ms_step * 1e-3)
+    res = out if wl["kind"] == "rates" else work
+    if not bool(torch.isfinite(res).all()):
+        raise RuntimeError("non-finite values in the benchmark output")
 
-    # ---- CPU baseline (rank 0, N = 1 only) ---------------------------------------------------
+    hbm_peak, bf16_peak, peak_src = peaks()
+    roof = None
+    if wl["kind"] == "rates":
+        from tiger_nga_b200.workcount import rhs_work
+
+        work_c = rhs_work(mech)
+        achieved = work_c["bytes"] * ncells / (ms_step * 1e-3) / 1e9
+        fp64_peak = capi.fp64_peak_tflops(local)
+        fp64_ach = work_c["flops"] * ncells / (ms_step * 1e-3) / 1e12
+        tr = read_profile_value(f"k_rhs_{wl['mech']}_{wl['precision']}.txt", "dram_bytes_per_cell")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": tr * ncells if tr else None, "peak_source": peak_src,
+                "kernel": "k_rhs", "algorithmic_bytes_per_cell": work_c["bytes"],
+                "fp64_pipe": {"achieved_tflops": fp64_ach, "peak_tflops_measured": fp64_peak,
+                              "frac": fp64_ach / fp64_peak, "alg_flops_per_cell": work_c["flops"],
+                              "transcendentals_per_cell": work_c["transcendentals"],
+                              "note": "reference-formulation flops (transcendentals counted separately); the "
+                                      "kernel is FP64-pipe bound, the HBM figure is reported per schema"}}
+    else:
+        # dominant kernel: the implicit solver (k_bdf) -- the whole substep, or the fallback cells
+        sst = stats_last if wl["kind"] == "substep" else stats_last["fallback"]
+        ms_solver = sst["ms"]
+        flops = solver_flops(mech, sst) if sst.get("newton_iters") else None
+        fp64_peak = capi.fp64_peak_tflops(local)
+        nbytes = 2 * (mech.ns + 1) * 8 * (sst["cells"] or 0)
+        if flops and ms_solver > 0:
+            ach = flops / (ms_solver * 1e-3) / 1e12
+            roof = {"bound": "hbm", "achieved": nbytes / (ms_solver * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": nbytes / (ms_solver * 1e-3) / 1e9 / hbm_peak,
+                    "traffic": read_profile_value(f"k_bdf_{wl['mech']}.txt", "dram_bytes_per_cell"),
+                    "peak_source": peak_src, "kernel": "k_bdf",
+                    "fp64_pipe": {"achieved_tflops": ach, "peak_tflops_measured": fp64_peak, "frac": ach / fp64_peak,
+                                  "counted_flops_per_launch": flops,
+                                  "note": "the implicit solve is latency bound (dependent FP64 chains, warp "
+                                          "shuffles); counted flops are a lower bound (RHS per Newton iteration, "
+                                          "LU per Jacobian, triangular solves)"}}
+        extra["solver"] = {k: sst.get(k) for k in ("cells", "cells_failed", "steps", "newton_iters", "jacobians",
+                                                   "max_steps_cell", "max_newton_cell", "passes", "ms")}
+
+    if wl["kind"] == "surrogate":
+        # the plain implicit GPU solve of a strided subsample: speed and the accuracy reference
+        m = ncells if args.plain_cells <= 0 else min(args.plain_cells, ncells)
+        idx = torch.arange(0, ncells, max(1, ncells // m), device=dev)[:m]
+        ref = x0[:, idx].contiguous()
+        dsub = d_dev[idx].contiguous()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        pst = chem.substep(ref, dsub, P_ATM, stats=True)
+        e1.record(st)
+        e1.synchronize()
+        ms_plain = e0.elapsed_time(e1)
+        plain_cps = m / (ms_plain * 1e-3)
+        got = work[:, idx]
+        ns = mech.ns
+        rg, rr = got[:ns].sum(0), ref[:ns].sum(0)
+        errT = ((got[ns] / rg - ref[ns] / rr).abs() / (ref[ns] / rr))
+        errY = ((got[:ns] / rg - ref[:ns] / rr).abs().amax(0) / (ref[:ns] / rr).amax(0))
+        extra["plain_gpu"] = {"value": plain_cps, "unit": unit, "cells": m, "ms": ms_plain,
+                              "steps": pst["steps"], "newton_iters": pst["newton_iters"]}
+        extra["speedup_vs_plain_gpu"] = value / ws / plain_cps
+        extra["accuracy_vs_plain_gpu"] = {
+            "cells": m, "max_rel_T": float(errT.max()), "p99_rel_T": float(torch.quantile(errT.float(), 0.99)),
+            "max_dY_over_maxY": float(errY.max()), "p99_dY_over_maxY": float(torch.quantile(errY.float(), 0.99)),
+            "within_1pct_T": bool(float(errT.max()) <= 0.01), "within_1e-3_dY": bool(float(errY.max()) <= 1e-3)}
+        extra["surrogate"] = {k: stats_last[k] for k in ("accepted", "fallback_ood", "fallback_consistency",
+                                                         "fallback_clip", "judged", "judge_max_rel_dT",
+                                                         "judge_max_dY", "ms_infer", "ms_post", "ms_fallback",
+                                                         "ms_total")}
+        extra["surrogate"]["fallback_fraction"] = 1.0 - stats_last["accepted"] / ncells
+        extra["surrogate"]["weights"] = os.path.relpath(args.surrogate, REPO)
+        # tensor roofline of the inference chain (reported beside the dominant solver kernel)
+        nparam_flops = 2.0 * sur.nparam  # one multiply-add per weight per cell
+        t_inf = stats_last["ms_infer"] * 1e-3
+        if t_inf > 0 and bf16_peak:
+            ach = nparam_flops * ncells / t_inf / 1e12
+            extra["inference_roofline"] = {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                                           "frac": ach / bf16_peak, "peak_source": peak_src,
+                                           "kernel": "k_mlp_infer", "flops_per_cell": nparam_flops}
+
+    # ---- e2e through the C-ABI with pinned host buffers -----------------------------------------
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 3)
+    hin = torch.from_numpy(sol).pin_memory()
+    hbuf = torch.empty_like(hin).pin_memory()
+    hd = torch.from_numpy(np.ascontiguousarray(dts)).pin_memory().numpy() if dts is not None and np.ndim(dts) else dts
+    h2d = sol.nbytes + (hd.nbytes if isinstance(hd, np.ndarray) else 0)
+    if wl["kind"] == "rates":
+        d2h = sol.nbytes
+    else:
+        d2h = sol.nbytes
+
+    def e2e_step():
+        if wl["kind"] == "rates":
+            chem.compute_rhs(hin.numpy(), P_ATM, out=hbuf.numpy())
+        else:
+            hbuf.copy_(hin)  # host restore of the initial state (outside the timed call below)
+            t0 = time.perf_counter()
+            if wl["kind"] == "substep":
+                chem.substep(hbuf.numpy(), hd, P_ATM, stats=False)
+            else:
+                sur.substep(hbuf.numpy(), hd, P_ATM)
+            return time.perf_counter() - t0
+        return None
+
+    e2e_step()  # warm-up (staging buffers)
+    if pg:
+        pg.barrier()
+    if wl["kind"] == "rates":
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+    else:
+        e2e_s = sum(e2e_step() for _ in range(e2e_steps)) / e2e_steps
+    e2e_s = max_over_ranks(pg, dev, e2e_s)
+    e2e = {"value": ncells * ws / e2e_s, "unit": unit, "h2d_bytes_per_step": h2d * ws, "d2h_bytes_per_step": d2h * ws,
+           "steps": e2e_steps}
+
+    # ---- CPU baseline (rank 0, N = 1 only) ------------------------------------------------------
     cpu = None
     if rank == 0 and ws == 1 and args.cpu_seconds > 0:
-        kind, cval, cdone, cel = time_cpu(wl["mech"], sol, args.cpu_seconds, os.cpu_count() or 1)
+        kind, cval, cdone, cel = time_cpu(wl, sol, dts, args.cpu_seconds, os.cpu_count() or 1)
+        what = "rate evaluation" if wl["kind"] == "rates" else "implicit BDF/Newton substep (no surrogate)"
         cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, OpenMP over cells"}
+               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, {what}, OpenMP over cells"}
     if rank == 0:
-        out = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64" if wl["precision"] == "fp64" else "f32/f64",
-               "data": "synthetic (seeded CH4/air states, reference init_flow recipe)", "config": config,
-               "e2e": e2e,
-               "gpu_launches": args.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
-        print(json.dumps(out))
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if wl["precision"] == "fp64" else "f32/f64",
+                "data": "synthetic (seeded CH4/air or H2/air states, reference init_flow recipe)", "config": config,
+                "e2e": e2e, "gpu_launches": LAUNCHES[wl["kind"]] * args.steps, "roofline": roof,
+                "cpu_baseline": cpu, "clocks": clk}
+        if wl["kind"] == "surrogate":
+            line["dtype"] = "bf16/f32 (network), f64 (conservation, fallback solve)"
+        line.update(extra)
+        print(json.dumps(line))
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+    if sur is not None:
+        sur.close()
     chem.close()
     return 0
 

@@ -202,11 +202,15 @@ typedef struct tng_surrogate_cfg {
   double clip_tol;        /* fallback when clipping removed more mass fraction (1e-3) */
   int judge_cells;        /* cells re-solved every call to measure the error (1024) */
   int post_mode;          /* 0: T from the enthalpy balance of the conserved Y; 1: T from the network,
-                             enthalpy held by the projection of Y (default 0) */
+                             enthalpy held by the projection of Y (default 1) */
   int target_mode;        /* training targets: 0 each output scaled by its own spread; 1 dY_k share
-                             one scale (errors weighted as the dY <= tol*max(Y) criterion) (0) */
+                             one scale (errors weighted as the dY <= tol*max(Y) criterion) (1) */
   float loss_T_weight;    /* loss weight of dT relative to one species output (0 = default 2) */
-  int reserved[5];
+  int members;            /* networks in the ensemble, trained from different initialisations; the
+                             prediction is their mean (1..4, 0 = default 2) */
+  float ens_tol_K;        /* fallback when the members' temperatures spread by more (K, 0 = default 2) */
+  float ens_tol_Y;        /* fallback when a mass fraction spreads by more (0 = default 5e-4) */
+  int reserved[2];
 } tng_surrogate_cfg;
 
 typedef struct tng_surrogate_stats {
@@ -217,6 +221,7 @@ typedef struct tng_surrogate_stats {
   double judge_max_dY;          /* max |Y_s,k - Y_p,k| / max_k Y_p,k over the sample */
   double ms_infer, ms_post, ms_fallback, ms_total;  /* device times */
   tng_substep_stats fallback;   /* the implicit solve of the fallback cells */
+  int64_t fallback_ensemble;    /* cells whose ensemble members disagreed */
 } tng_surrogate_stats;
 
 typedef struct tng_surrogate tng_surrogate;
@@ -238,8 +243,10 @@ int tng_surrogate_features(tng_surrogate* s, const double* state, int64_t n, int
                            float* X);
 /* The surrogate's prediction without fallback (device pointers): out (species-major, ld_out)
  * receives the conserved post-processed state of every cell; reason (nullable, int per cell)
- * 0 accepted / 1 out of range / 2 inconsistent / 3 clipped; indicator (nullable, double per
- * cell) the network-vs-enthalpy temperature mismatch in K. dts per cell or the scalar dt. */
+ * 0 accepted / 1 out of range / 2 inconsistent / 3 clipped / 4 ensemble disagreement;
+ * indicator (nullable, 3 doubles per cell): the network-vs-enthalpy temperature mismatch (K),
+ * the members' temperature spread (K) and their largest mass-fraction spread. dts per cell or
+ * the scalar dt. */
 int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, int64_t ncells, int64_t ld,
                           const double* dts, double dt, double p, double* out, int64_t ld_out, int* reason,
                           double* indicator);

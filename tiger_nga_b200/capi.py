@@ -52,7 +52,7 @@ class SurrogateStats(ctypes.Structure):
                 ("fallback_consistency", ctypes.c_int64), ("fallback_clip", ctypes.c_int64),
                 ("judged", ctypes.c_int64), ("judge_max_rel_dT", ctypes.c_double), ("judge_max_dY", ctypes.c_double),
                 ("ms_infer", ctypes.c_double), ("ms_post", ctypes.c_double), ("ms_fallback", ctypes.c_double),
-                ("ms_total", ctypes.c_double), ("fallback", SubstepStats)]
+                ("ms_total", ctypes.c_double), ("fallback", SubstepStats), ("fallback_ensemble", ctypes.c_int64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "fallback"}
@@ -64,7 +64,8 @@ class SurrogateCfg(ctypes.Structure):
     _fields_ = [("hidden", ctypes.c_int), ("layers", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("ood_margin", ctypes.c_double), ("consist_tol_K", ctypes.c_double), ("clip_tol", ctypes.c_double),
                 ("judge_cells", ctypes.c_int), ("post_mode", ctypes.c_int), ("target_mode", ctypes.c_int),
-                ("loss_T_weight", ctypes.c_float), ("reserved", ctypes.c_int * 5)]
+                ("loss_T_weight", ctypes.c_float), ("members", ctypes.c_int), ("ens_tol_K", ctypes.c_float),
+                ("ens_tol_Y", ctypes.c_float), ("reserved", ctypes.c_int * 2)]
 
 
 class Extent(ctypes.Structure):
@@ -601,7 +602,7 @@ class Surrogate:
                                                                         device=state.device).contiguous()
         out = torch.empty((state.shape[0], n), dtype=torch.float64, device=state.device)
         reason = torch.empty(n, dtype=torch.int32, device=state.device)
-        ind = torch.empty(n, dtype=torch.float64, device=state.device)
+        ind = torch.empty((n, 3), dtype=torch.float64, device=state.device)
         self._pre()
         _check(self.lib.tng_surrogate_predict(self.chem.h, self.h, state.data_ptr(), n, max(state.stride(0), n),
                                               dts.data_ptr() if dts is not None else None,

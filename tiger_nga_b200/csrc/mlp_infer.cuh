@@ -44,6 +44,23 @@ struct InferArgs {
   int* error;  // non-zero after a timed-out wait
 };
 
+// Raw network input i of a cell (shared by the training features, the inference kernel and the
+// range check): 0 T; 1 log P; 2 .. ns log10 Y_k; ns+1 log10 dt; ns+2 .. 2ns Y_k -- the species
+// in mechanism order without the bath gas, once on a log scale (trace radicals) and once linear
+// (heat release is linear in the mass fractions). n_in = 2 ns + 1.
+__device__ __forceinline__ float sur_raw_input(int i, int ns, int bath, const double* __restrict__ state, long long ld,
+                                               int cell, double rho, double T, double logp, double dt) {
+  if (i == 0) return (float)T;
+  if (i == 1) return (float)logp;
+  if (i == ns + 1) return (float)log10(fmax(dt, 1e-30));
+  if (i >= 2 * ns + 1) return 0.f;
+  const bool lin = i > ns + 1;
+  int k = lin ? i - ns - 2 : i - 2;
+  if (k >= bath) ++k;
+  const double y = state[(long long)k * ld + cell] / rho;
+  return lin ? (float)y : (float)log10(fmax(y, 1e-30));
+}
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -171,30 +188,26 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
     {
       const int cell = tile * kInferRows + tid;
       const bool live = cell < a.ncells;
-      float f[64];
-#pragma unroll
-      for (int i = 0; i < 64; ++i) f[i] = 0.f;
+      double rho = 1.0, T = 0.0, dt = 0.0;
       if (live) {
-        double rho = 0.0;
+        rho = 0.0;
         for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
-        const double T = a.state[(long long)a.ns * a.ld + cell] / rho;
-        const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
-        f[0] = (float)T;
-        f[1] = (float)a.logp;
-        int j = 2;
-        for (int k = 0; k < a.ns; ++k) {
-          if (k == a.bath) continue;
-          const double y = a.state[(long long)k * a.ld + cell] / rho;
-          f[j++] = (float)log10(fmax(y, 1e-30));
-        }
-        f[j] = (float)log10(fmax(dt, 1e-30));
-        for (int i = 0; i < a.n_in; ++i) f[i] = (f[i] - a.fmean[i]) * a.fistd[i];
+        T = a.state[(long long)a.ns * a.ld + cell] / rho;
+        dt = a.dts ? a.dts[cell] : a.dt_scalar;
       }
       for (int k8 = 0; k8 < a.in_pad; k8 += 8) {
-        __nv_bfloat162 p0 = __floats2bfloat162_rn(f[k8 + 0], f[k8 + 1]);
-        __nv_bfloat162 p1 = __floats2bfloat162_rn(f[k8 + 2], f[k8 + 3]);
-        __nv_bfloat162 p2 = __floats2bfloat162_rn(f[k8 + 4], f[k8 + 5]);
-        __nv_bfloat162 p3 = __floats2bfloat162_rn(f[k8 + 6], f[k8 + 7]);
+        float f[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int i = k8 + q;
+          f[q] = (live && i < a.n_in)
+                     ? (sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, rho, T, a.logp, dt) - a.fmean[i]) * a.fistd[i]
+                     : 0.f;
+        }
+        __nv_bfloat162 p0 = __floats2bfloat162_rn(f[0], f[1]);
+        __nv_bfloat162 p1 = __floats2bfloat162_rn(f[2], f[3]);
+        __nv_bfloat162 p2 = __floats2bfloat162_rn(f[4], f[5]);
+        __nv_bfloat162 p3 = __floats2bfloat162_rn(f[6], f[7]);
         uint4 v;
         v.x = *reinterpret_cast<uint32_t*>(&p0);
         v.y = *reinterpret_cast<uint32_t*>(&p1);

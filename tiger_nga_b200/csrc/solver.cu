@@ -305,6 +305,10 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
     if (e != cudaSuccess) return cuda_error(e, "solver graph instantiate");
     s->key[slot] = key;
   }
+  if (stats && list) {
+    // cells outside the list keep older counters: clear them so the statistics cover the list only
+    for (int* q : {nst, nni, (int*)s->nje.ptr, sts}) cudaMemsetAsync(q, 0, ncells * sizeof(int), h->stream);
+  }
   cudaEventRecord(s->ev0, h->stream);
   if ((e = cudaGraphLaunch(s->graph[slot], h->stream)) != cudaSuccess) return cuda_error(e, "solver graph launch");
   cudaEventRecord(s->ev1, h->stream);
@@ -313,25 +317,20 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
                           cudaMemcpyDeviceToHost, h->stream);
     if (e != cudaSuccess) return cuda_error(e, "state device->host");
   }
-  if (stats && list) {
-    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_error(e, "implicit substep");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-    stats->passes = passes;
-    stats->ms = ms;
-  } else if (stats) {
+  if (stats) {
     unsigned long long* acc = (unsigned long long*)s->stats.ptr;
     cudaMemsetAsync(acc, 0, 32 * sizeof(unsigned long long), h->stream);
     k_stats<<<std::min<int64_t>(1184, (ncells + 255) / 256), 256, 0, h->stream>>>(nst, nni, (int*)s->nje.ptr, sts,
                                                                                   ncells, acc);
     unsigned long long hacc[32];
-    int hc[4];
+    int hc[4], hlist = 0;
     cudaMemcpyAsync(hacc, acc, sizeof(hacc), cudaMemcpyDeviceToHost, h->stream);
     cudaMemcpyAsync(hc, s->counters.ptr, sizeof(hc), cudaMemcpyDeviceToHost, h->stream);
+    if (list) cudaMemcpyAsync(&hlist, nlist, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return cuda_error(e, "implicit substep");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, s->ev0, s->ev1);
-    stats->cells = ncells;
+    stats->cells = list ? hlist : ncells;
     stats->steps = (int64_t)hacc[0];
     stats->newton_iters = (int64_t)hacc[1];
     stats->jacobians = (int64_t)hacc[2];

@@ -40,13 +40,16 @@ struct SurPost {
   const double* th;  // ns x 24 NASA (hi 12, lo 12)
   double tmid;
   int post_mode;     // 0: T from the enthalpy balance; 1: T from the network, enthalpy in the projection
+  int members;       // ensemble members; outputs of member i at out + i * member_stride
+  long long member_stride;
+  double ens_tol_K, ens_tol_Y;
   int* fb_list;      // fallback cells
   int* fb_count;
-  unsigned long long* cnt;  // [accepted, ood, consistency, clip]
+  unsigned long long* cnt;  // [accepted, ood, consistency, clip, ensemble]
   double* out_state;  // predict mode: every cell's post-processed state here (state untouched, no list)
   long long ld_out;
   int* reason_out;    // per cell, nullable
-  double* ind_out;    // per cell, nullable
+  double* ind_out;    // per cell 3 values, nullable
 };
 
 __device__ __forceinline__ void nasa(const double* th, double tmid, int k, double T, double* h, double* cp) {
@@ -61,23 +64,17 @@ __device__ __forceinline__ int raw_features(const double* state, long long ld, i
   double rho = 0.0;
   for (int k = 0; k < ns; ++k) rho += state[(long long)k * ld + cell];
   const double T = state[(long long)ns * ld + cell] / rho;
-  f[0] = (float)T;
-  f[1] = (float)logp;
-  int j = 2;
-  for (int k = 0; k < ns; ++k) {
-    if (k == bath) continue;
-    f[j++] = (float)log10(fmax(state[(long long)k * ld + cell] / rho, 1e-30));
-  }
-  f[j++] = (float)log10(fmax(dt, 1e-30));
+  const int n_in = 2 * ns + 1;
+  for (int i = 0; i < n_in; ++i) f[i] = sur_raw_input(i, ns, bath, state, ld, cell, rho, T, logp, dt);
   *rho_out = rho;
   *T_out = T;
-  return j;
+  return n_in;
 }
 
 __global__ void k_sur_features(const double* __restrict__ state, long long ld, int n, const double* __restrict__ dts,
                                double logp, int ns, int bath, int in_pad, float* __restrict__ X) {
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < n; cell += gridDim.x * blockDim.x) {
-    float f[kMaxNs + 4];
+    float f[2 * kMaxNs + 2];
     double rho, T;
     const int nf = raw_features(state, ld, cell, ns, bath, logp, dts[cell], f, &rho, &T);
     for (int i = 0; i < in_pad; ++i) X[(size_t)cell * in_pad + i] = i < nf ? f[i] : 0.f;
@@ -94,7 +91,8 @@ __global__ void k_sur_targets(const double* __restrict__ s0, const double* __res
       r1 += s1[(long long)k * ld + cell];
     }
     float* t = Tt + (size_t)cell * out_pad;
-    t[0] = (float)(s1[(long long)ns * ld + cell] / r1 - s0[(long long)ns * ld + cell] / r0);
+    const double T0 = s0[(long long)ns * ld + cell] / r0;
+    t[0] = (float)((s1[(long long)ns * ld + cell] / r1 - T0) / T0);  // relative: the accuracy criterion's unit
     for (int k = 0; k < ns; ++k)
       t[1 + k] = (float)(s1[(long long)k * ld + cell] / r1 - s0[(long long)k * ld + cell] / r0);
     for (int i = ns + 1; i < out_pad; ++i) t[i] = 0.f;
@@ -163,24 +161,40 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 __device__ bool project(const SurPost& a, const double* Y0, double* dY, double* D, const double* hrow, double hrhs) {
   const int nc = a.nel + (hrow ? 1 : 0);
   auto A = [&](int e, int k) { return e < a.nel ? a.E[e * a.ns + k] : hrow[k]; };
-  for (int pass = 0; pass < 4; ++pass) {
-    double G[kMaxEl + 1][kMaxEl + 1], r[kMaxEl + 1];
+  for (int pass = 0; pass < 8; ++pass) {
+    double G[kMaxEl + 1][kMaxEl + 1], r[kMaxEl + 1], scale[kMaxEl + 1];
     for (int e = 0; e < nc; ++e) {
       r[e] = e < a.nel ? 0.0 : -hrhs;
-      for (int k = 0; k < a.ns; ++k) r[e] += A(e, k) * dY[k];
+      scale[e] = e < a.nel ? 0.0 : fabs(hrhs);
+      for (int k = 0; k < a.ns; ++k) {
+        r[e] += A(e, k) * dY[k];
+        scale[e] += fabs(A(e, k)) * (Y0[k] + fabs(dY[k]));
+      }
       for (int g = 0; g <= e; ++g) {
         double sg = 0.0;
         for (int k = 0; k < a.ns; ++k) sg += A(e, k) * D[k] * A(g, k);
         G[e][g] = G[g][e] = sg;
       }
     }
+    // A constraint whose carriers are all pinned (or absent) has G_ee = 0 exactly: it holds
+    // already when its residual is zero (e.g. an element no species of the cell carries), and
+    // cannot be met otherwise. It leaves the system; the others are solved without it.
+    bool act[kMaxEl + 1];
+    for (int e = 0; e < nc; ++e) {
+      act[e] = G[e][e] > 0.0;
+      if (!act[e] && !(fabs(r[e]) <= 1e-13 * scale[e] + 1e-300)) return false;
+    }
     double Lc[kMaxEl + 1][kMaxEl + 1];
     for (int i = 0; i < nc; ++i)
       for (int j = 0; j <= i; ++j) {
+        if (!act[i] || !act[j]) {
+          Lc[i][j] = (i == j) ? 1.0 : 0.0;
+          continue;
+        }
         double sg = G[i][j];
         for (int q = 0; q < j; ++q) sg -= Lc[i][q] * Lc[j][q];
         if (i == j) {
-          if (!(sg > 0.0)) return false;
+          if (!(sg > 1e-14 * G[i][i])) return false;  // dependent constraints
           Lc[i][i] = sqrt(sg);
         } else {
           Lc[i][j] = sg / Lc[j][j];
@@ -188,7 +202,7 @@ __device__ bool project(const SurPost& a, const double* Y0, double* dY, double* 
       }
     double lam[kMaxEl + 1];
     for (int i = 0; i < nc; ++i) {
-      double sg = r[i];
+      double sg = act[i] ? r[i] : 0.0;
       for (int q = 0; q < i; ++q) sg -= Lc[i][q] * lam[q];
       lam[i] = sg / Lc[i][i];
     }
@@ -211,7 +225,7 @@ __device__ bool project(const SurPost& a, const double* Y0, double* dY, double* 
     }
     if (!pinned) return true;
   }
-  return false;  // still pinning species after four passes: leave the cell to the implicit solve
+  return false;  // still pinning species after eight passes: leave the cell to the implicit solve
 }
 
 // temperature with sum Y_k h_k(T) = h0 (Newton from T)
@@ -234,7 +248,7 @@ __device__ double enthalpy_T(const SurPost& a, const double* Y, double h0, doubl
 __global__ void k_sur_post(const SurPost a) {
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells; cell += gridDim.x * blockDim.x) {
     const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
-    float f[kMaxNs + 4];
+    float f[2 * kMaxNs + 2];
     double rho, T0;
     raw_features(a.state, a.ld, cell, a.ns, a.bath, a.logp, dt, f, &rho, &T0);
     int reason = 0;
@@ -243,12 +257,27 @@ __global__ void k_sur_post(const SurPost a) {
       if (f[i] < a.fmin[i] - a.margin * span || f[i] > a.fmax[i] + a.margin * span) reason = 1;
     }
     double Y0[kMaxNs], dY[kMaxNs], D[kMaxNs];
+    // the ensemble: mean prediction, and the spread of the members as an error indicator
     const float* o = a.out + (size_t)cell * a.out_pad;
-    const double Tnet = fmin(fmax(T0 + ((double)o[0] * a.tstd[0] + a.tmean[0]), 200.0), 6000.0);
+    double rT = 0.0, tlo = 1e300, thi = -1e300, sY = 0.0;
+    for (int i = 0; i < a.members; ++i) {
+      const double v = (double)o[i * a.member_stride] * a.tstd[0] + a.tmean[0];
+      rT += v;
+      tlo = fmin(tlo, v), thi = fmax(thi, v);
+    }
+    const double Tnet = fmin(fmax(T0 * (1.0 + rT / a.members), 200.0), 6000.0);
+    const double sT = T0 * (thi - tlo);
     double neg = 0.0;  // negative mass fraction the network predicted (clip test)
     for (int k = 0; k < a.ns; ++k) {
       Y0[k] = a.state[(long long)k * a.ld + cell] / rho;
-      dY[k] = (double)o[1 + k] * a.tstd[1 + k] + a.tmean[1 + k];
+      double m = 0.0, lo = 1e300, hi = -1e300;
+      for (int i = 0; i < a.members; ++i) {
+        const double v = (double)o[i * a.member_stride + 1 + k] * a.tstd[1 + k] + a.tmean[1 + k];
+        m += v;
+        lo = fmin(lo, v), hi = fmax(hi, v);
+      }
+      dY[k] = m / a.members;
+      sY = fmax(sY, hi - lo);
       D[k] = fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12;
       if (Y0[k] + dY[k] < 0.0) neg -= Y0[k] + dY[k];
     }
@@ -294,8 +323,13 @@ __global__ void k_sur_post(const SurPost a) {
     if (!reason && !(ind <= a.consist_tol)) reason = 2;
     if (!reason && !(neg <= a.clip_tol)) reason = 3;
     if (!reason && !(isfinite(T1) && ok)) reason = 2;
+    if (!reason && !(sT <= a.ens_tol_K && sY <= a.ens_tol_Y)) reason = 4;
     if (a.reason_out) a.reason_out[cell] = reason;
-    if (a.ind_out) a.ind_out[cell] = ok ? ind : INFINITY;
+    if (a.ind_out) {
+      a.ind_out[3 * (size_t)cell] = ok ? ind : INFINITY;
+      a.ind_out[3 * (size_t)cell + 1] = sT;
+      a.ind_out[3 * (size_t)cell + 2] = sY;
+    }
     if (a.out_state) {
       for (int k = 0; k < a.ns; ++k) a.out_state[(long long)k * a.ld_out + cell] = rho * Y1[k];
       a.out_state[(long long)a.ns * a.ld_out + cell] = rho * T1;
@@ -344,10 +378,16 @@ __global__ void k_judge(const double* __restrict__ state, long long ld, int ns, 
 
 using namespace tng;
 
+constexpr int kMaxMembers = 4;
+
 struct tng_surrogate {
   tng_chem* h = nullptr;
   tng_surrogate_cfg cfg{};
-  Mlp m;
+  Mlp m;                         // member 0 (also the member of the single-network tools)
+  Mlp mx[kMaxMembers - 1];       // members 1 ..
+  int members = 1;
+  Mlp& member(int i) { return i == 0 ? m : mx[i - 1]; }
+  const Mlp& member(int i) const { return i == 0 ? m : mx[i - 1]; }
   int ns = 0, bath = 0, n_in = 0, n_out = 0, nel = 0;
   std::vector<double> fmean, fstd, fmin, fmax, tmean, tstd;  // host copies
   bool trained = false;
@@ -355,7 +395,7 @@ struct tng_surrogate {
   float* d_fnorm = nullptr;  // fmean (in_pad), fistd (in_pad), fmin (in_pad), fmax (in_pad)
   double* d_tnorm = nullptr;  // tmean (out_pad), tstd (out_pad)
   double* d_E = nullptr;
-  __nv_bfloat16* d_wpack = nullptr;
+  __nv_bfloat16* d_wpack[kMaxMembers] = {};
   long long w_off[kMaxLayers] = {};
   DevBuf out, fb, cnt, judge_state, judge_dts, judge_idx, work;
   cudaEvent_t ev[5] = {};
@@ -382,18 +422,21 @@ static int sur_upload_norm(tng_surrogate* s) {
 }
 
 static int sur_pack(tng_surrogate* s) {
-  long long off = 0;
-  for (int l = 0; l < s->m.nlin; ++l) {
-    s->w_off[l] = off;
-    const int fo = s->m.fan_out[l], fi = s->m.fan_in[l];
-    k_pack_weights<<<256, 256, 0, s->m.stream>>>(s->m.params + s->m.w_off[l], fo, fi, s->d_wpack + off);
-    off += (long long)fo * fi;
+  for (int i = 0; i < s->members; ++i) {
+    long long off = 0;
+    Mlp& mi = s->member(i);
+    for (int l = 0; l < mi.nlin; ++l) {
+      s->w_off[l] = off;
+      const int fo = mi.fan_out[l], fi = mi.fan_in[l];
+      k_pack_weights<<<256, 256, 0, s->m.stream>>>(mi.params + mi.w_off[l], fo, fi, s->d_wpack[i] + off);
+      off += (long long)fo * fi;
+    }
   }
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate weight packing");
 }
 
-static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
+static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double* dstate, int64_t ncells, int64_t dld,
                         const double* ddts, double dt, double p, float* out, int* err) {
   InferArgs ia{};
   ia.state = dstate;
@@ -411,12 +454,12 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int
   ia.nlin = s->m.nlin;
   ia.fmean = s->d_fnorm;
   ia.fistd = s->d_fnorm + s->m.in_pad;
-  ia.wpack = s->d_wpack;
+  ia.wpack = s->d_wpack[member];
   for (int l = 0; l < s->m.nlin; ++l) {
     ia.w_off[l] = s->w_off[l];
     ia.b_off[l] = (int)s->m.b_off[l];
   }
-  ia.bias = s->m.params;
+  ia.bias = s->member(member).params;
   ia.out = out;
   ia.error = err;
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
@@ -453,6 +496,10 @@ static SurPost post_args(tng_chem* h, tng_surrogate* s, double* state, int64_t l
   pa.consist_tol = s->cfg.consist_tol_K;
   pa.clip_tol = s->cfg.clip_tol;
   pa.post_mode = s->cfg.post_mode;
+  pa.members = s->members;
+  pa.member_stride = (long long)ncells * s->m.out_pad;
+  pa.ens_tol_K = s->cfg.ens_tol_K;
+  pa.ens_tol_Y = s->cfg.ens_tol_Y;
   pa.E = s->d_E;
   solver_thermo(h, &pa.th, &pa.tmid);
   return pa;
@@ -471,6 +518,11 @@ void tng_surrogate_default_cfg(tng_surrogate_cfg* c) {
   c->consist_tol_K = 5.0;
   c->clip_tol = 1e-3;
   c->judge_cells = 1024;
+  c->post_mode = 1;
+  c->target_mode = 1;
+  c->members = 2;
+  c->ens_tol_K = 2.f;
+  c->ens_tol_Y = 5e-4f;
 }
 
 int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogate** out) {
@@ -481,6 +533,11 @@ int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogat
     c = *cfg;
   else
     tng_surrogate_default_cfg(&c);
+  if (c.members == 0) c.members = 2;
+  if (!(c.ens_tol_K > 0.f)) c.ens_tol_K = 2.f;
+  if (!(c.ens_tol_Y > 0.f)) c.ens_tol_Y = 5e-4f;
+  if (c.members < 1 || c.members > kMaxMembers)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_create: 1..%d ensemble members", kMaxMembers);
   if (c.hidden != 256 || c.layers < 1 || c.layers > kMaxLayers - 1)
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: hidden width must be 256 (the tensor-core tile), 1..%d layers",
                      kMaxLayers - 1);
@@ -494,22 +551,27 @@ int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogat
   s->bath = 0;
   for (int k = 0; k < o->ns; ++k)
     if (std::strcmp(o->species[k], "N2") == 0) s->bath = k;
-  s->n_in = o->ns + 2;  // T, log P, ns-1 species, log dt
+  s->n_in = 2 * o->ns + 1;  // T, log P, ns-1 species (log), log dt, ns-1 species (linear)
   s->n_out = o->ns + 1;
   s->nel = o->nelem;
-  int rc = mlp_init(&s->m, h->cfg.device, h->stream, s->n_in, s->n_out, c.hidden, c.layers, c.seed);
+  s->members = c.members;
+  int rc = TNG_OK;
+  for (int i = 0; i < s->members && !rc; ++i)
+    rc = mlp_init(&s->member(i), h->cfg.device, h->stream, s->n_in, s->n_out, c.hidden, c.layers,
+                  c.seed + 7919ULL * i);
   if (rc) {
+    for (int i = 0; i < s->members; ++i) mlp_free(&s->member(i));
     delete s;
     return rc;
   }
   if (s->m.in_pad > 256 || s->m.out_pad > 256 || s->m.in_pad % 16 || s->m.out_pad % 16) {
-    mlp_free(&s->m);
+    for (int i = 0; i < s->members; ++i) mlp_free(&s->member(i));
     delete s;
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: unsupported layer widths");
   }
   cudaMalloc(&s->d_fnorm, sizeof(float) * 4 * s->m.in_pad);
   cudaMalloc(&s->d_tnorm, sizeof(double) * 2 * s->m.out_pad);
-  cudaMalloc(&s->d_wpack, sizeof(__nv_bfloat16) * s->m.nparam);
+  for (int i = 0; i < s->members; ++i) cudaMalloc(&s->d_wpack[i], sizeof(__nv_bfloat16) * s->m.nparam);
   // element matrix per kg: a_ek / W_k (reference literal kinds of W_k)
   std::vector<double> E(s->nel * s->ns);
   const double* wm = o->wmol[h->cfg.literal_mode];
@@ -535,11 +597,12 @@ int tng_surrogate_destroy(tng_surrogate* s) {
   if (!s) return TNG_OK;
   DeviceGuard g(s->m.device);
   cudaStreamSynchronize(s->m.stream);
-  mlp_free(&s->m);
+  for (int i = 0; i < s->members; ++i) mlp_free(&s->member(i));
   if (s->d_fnorm) cudaFree(s->d_fnorm);
   if (s->d_tnorm) cudaFree(s->d_tnorm);
   if (s->d_E) cudaFree(s->d_E);
-  if (s->d_wpack) cudaFree(s->d_wpack);
+  for (auto* w : s->d_wpack)
+    if (w) cudaFree(w);
   for (DevBuf* b : {&s->out, &s->fb, &s->cnt, &s->judge_state, &s->judge_dts, &s->judge_idx, &s->work}) b->release();
   for (auto& ev : s->ev)
     if (ev) cudaEventDestroy(ev);
@@ -604,7 +667,15 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
   float* dw;
   if ((e = cudaMalloc(&dw, sizeof(float) * op)) != cudaSuccess) return cuda_error(e, "loss weights");
   cudaMemcpyAsync(dw, w.data(), sizeof(float) * op, cudaMemcpyHostToDevice, st);
-  rc = mlp_train(&s->m, X, T, dw, n, epochs, batch, (float)lr, s->cfg.seed + 1, losses);
+  // every member on the same normalised pairs, from its own initialisation and shuffling order;
+  // the reported loss is the members' mean per epoch
+  std::vector<float> lm(epochs > 0 ? epochs : 1);
+  if (losses) std::fill(losses, losses + epochs, 0.f);
+  for (int i = 0; i < s->members && !rc; ++i) {
+    rc = mlp_train(&s->member(i), X, T, dw, n, epochs, batch, (float)lr, s->cfg.seed + 1 + 104729ULL * i, lm.data());
+    if (losses)
+      for (int ep = 0; ep < epochs; ++ep) losses[ep] += lm[ep] / s->members;
+  }
   cudaStreamSynchronize(st);
   cudaFree(dw);
   if (rc) return rc;
@@ -616,16 +687,18 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
 int tng_surrogate_save(const tng_surrogate* s, const char* path) {
   if (!s || !path) return set_error(TNG_ERR_ARG, "tng_surrogate_save: null argument");
   if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_save: surrogate not trained");
-  std::vector<float> params(s->m.nparam);
+  std::vector<float> params(s->m.nparam * s->members);
   DeviceGuard g(s->m.device);
   cudaStreamSynchronize(s->m.stream);
-  cudaMemcpy(params.data(), s->m.params, sizeof(float) * s->m.nparam, cudaMemcpyDeviceToHost);
+  for (int i = 0; i < s->members; ++i)
+    cudaMemcpy(params.data() + i * s->m.nparam, s->member(i).params, sizeof(float) * s->m.nparam,
+               cudaMemcpyDeviceToHost);
   FILE* f = std::fopen(path, "wb");
   if (!f) return set_error(TNG_ERR_ARG, "tng_surrogate_save: cannot open %s", path);
-  char magic[8] = {'T', 'N', 'G', 'S', 'U', 'R', '1', 0};
+  char magic[8] = {'T', 'N', 'G', 'S', 'U', 'R', '2', 0};
   char mech[32] = {};
   std::snprintf(mech, sizeof(mech), "%s", s->h->ops->name);
-  int hdr[8] = {s->ns, s->n_in, s->n_out, s->cfg.hidden, s->cfg.layers, s->bath, s->h->cfg.literal_mode, 0};
+  int hdr[8] = {s->ns, s->n_in, s->n_out, s->cfg.hidden, s->cfg.layers, s->bath, s->h->cfg.literal_mode, s->members};
   int64_t np = s->m.nparam;
   bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(mech, 1, 32, f) == 32 && std::fwrite(hdr, 4, 8, f) == 8 &&
             std::fwrite(&np, 8, 1, f) == 1;
@@ -645,7 +718,7 @@ int tng_surrogate_load(tng_surrogate* s, const char* path) {
   int64_t np = 0;
   bool ok = std::fread(magic, 1, 8, f) == 8 && std::fread(mech, 1, 32, f) == 32 && std::fread(hdr, 4, 8, f) == 8 &&
             std::fread(&np, 8, 1, f) == 1;
-  if (!ok || std::memcmp(magic, "TNGSUR1", 8) != 0) {
+  if (!ok || std::memcmp(magic, "TNGSUR2", 8) != 0) {
     std::fclose(f);
     return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is not a surrogate file", path);
   }
@@ -655,14 +728,20 @@ int tng_surrogate_load(tng_surrogate* s, const char* path) {
     std::fclose(f);
     return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s was trained for %s with other sizes", path, mech);
   }
+  if (hdr[7] != s->members) {
+    std::fclose(f);
+    return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s holds %d ensemble members, the surrogate was created with %d",
+                     path, hdr[7], s->members);
+  }
   for (std::vector<double>* v : {&s->fmean, &s->fstd, &s->fmin, &s->fmax, &s->tmean, &s->tstd})
     ok = ok && std::fread(v->data(), 8, v->size(), f) == v->size();
-  std::vector<float> params(np);
-  ok = ok && std::fread(params.data(), 4, np, f) == (size_t)np;
+  std::vector<float> params(np * s->members);
+  ok = ok && std::fread(params.data(), 4, params.size(), f) == params.size();
   std::fclose(f);
   if (!ok) return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is truncated", path);
   DeviceGuard g(s->m.device);
-  cudaMemcpy(s->m.params, params.data(), sizeof(float) * np, cudaMemcpyHostToDevice);
+  for (int i = 0; i < s->members; ++i)
+    cudaMemcpy(s->member(i).params, params.data() + i * np, sizeof(float) * np, cudaMemcpyHostToDevice);
   int rc = sur_upload_norm(s);
   if (rc) return rc;
   if ((rc = sur_pack(s))) return rc;
@@ -737,7 +816,7 @@ int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_
   if (!s->cnt.reserve(16 * sizeof(unsigned long long))) return set_error(TNG_ERR_CUDA, "scratch");
   int* err = (int*)((unsigned long long*)s->cnt.ptr + 8);
   cudaMemsetAsync(err, 0, sizeof(int), s->m.stream);
-  int rc = launch_infer(s->h, s, state, n, ld, dts, dt, p, out, err);
+  int rc = launch_infer(s->h, s, 0, state, n, ld, dts, dt, p, out, err);
   if (rc) return rc;
   int herr = 0;
   cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s->m.stream);
@@ -778,7 +857,7 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
     }
   }
   const int J = (int)std::min<int64_t>(ncells, std::max(0, s->cfg.judge_cells));
-  bool ok = s->out.reserve((size_t)ncells * s->m.out_pad * sizeof(float)) && s->fb.reserve((ncells + 1) * sizeof(int)) &&
+  bool ok = s->out.reserve((size_t)ncells * s->m.out_pad * s->members * sizeof(float)) && s->fb.reserve((ncells + 1) * sizeof(int)) &&
             s->cnt.reserve(16 * sizeof(unsigned long long)) &&
             (J == 0 || (s->judge_state.reserve((size_t)J * nv * sizeof(double)) &&
                         s->judge_dts.reserve((size_t)J * sizeof(double)) && s->judge_idx.reserve(J * sizeof(int))));
@@ -804,7 +883,9 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   s->calls++;
   // inference on the tensor cores
   cudaEventRecord(s->ev[0], st);
-  rc = launch_infer(h, s, dstate, ncells, dld, ddts, dt, p, (float*)s->out.ptr, (int*)(cnt + 8));
+  for (int i = 0; i < s->members && !rc; ++i)
+    rc = launch_infer(h, s, i, dstate, ncells, dld, ddts, dt, p,
+                      (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad, (int*)(cnt + 8));
   if (rc) return rc;
   cudaEventRecord(s->ev[1], st);
   // post-processing and fallback list
@@ -856,7 +937,8 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
       cudaEventElapsedTime(&d, s->ev[0], s->ev[3]);
       stats->ms_infer = a, stats->ms_post = b, stats->ms_fallback = c, stats->ms_total = d;
       stats->fallback = fst;
-      stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3]);
+      stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3] + hc[4]);
+      stats->fallback_ensemble = (int64_t)hc[4];
     }
   }
   return TNG_OK;
@@ -874,13 +956,15 @@ int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, in
     return set_error(TNG_ERR_ARG, "tng_surrogate_predict: bad argument");
   DeviceGuard g(h->cfg.device);
   cudaStream_t st = h->stream;
-  if (!s->out.reserve((size_t)ncells * s->m.out_pad * sizeof(float)) || !s->cnt.reserve(16 * sizeof(unsigned long long)))
+  if (!s->out.reserve((size_t)ncells * s->m.out_pad * s->members * sizeof(float)) || !s->cnt.reserve(16 * sizeof(unsigned long long)))
     return set_error(TNG_ERR_CUDA, "tng_surrogate_predict: scratch allocation failed");
   int rc = solver_prepare(h);
   if (rc) return rc;
   unsigned long long* cnt = (unsigned long long*)s->cnt.ptr;
   cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), st);
-  rc = launch_infer(h, s, state, ncells, ld, dts, dt, p, (float*)s->out.ptr, (int*)(cnt + 8));
+  for (int i = 0; i < s->members && !rc; ++i)
+    rc = launch_infer(h, s, i, state, ncells, ld, dts, dt, p, (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad,
+                      (int*)(cnt + 8));
   if (rc) return rc;
   SurPost pa = post_args(h, s, const_cast<double*>(state), ld, ncells, dts, dt, p);
   pa.out_state = out;

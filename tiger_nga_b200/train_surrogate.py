@@ -63,13 +63,14 @@ def make_pairs(chem, n_pairs: int, seed: int, chunk: int = 1 << 21):
     return s0, s1, d, solve_s
 
 
-def evaluate(chem, sur, n: int, seed: int, tolerances=(1.0, 2.0, 5.0, 10.0, 20.0)):
+def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.0, 2.0, 4.0),
+             ens_Y=(1e-4, 2e-4, 5e-4, 1e-3)):
     """The surrogate against the plain solve on n fresh cells.
 
     Returns the timed surrogate-with-fallback substep (stats, speed-up over the plain solve) and,
     from the fallback-free prediction of every cell, the error of the cells each consistency
-    tolerance (K) would accept, with the plain solver's share of steps those cells leave to the
-    fallback. Per-cell arrays (errors, indicator, reason, T0, dt, steps) are returned as well.
+    tolerance (K) and ensemble-spread tolerances (K, mass fraction) would accept, with the plain
+    solver's share of steps those cells leave to the fallback. Per-cell arrays (errors, indicator, reason, T0, dt, steps) are returned as well.
     """
     import torch
 
@@ -104,16 +105,19 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(1.0, 2.0, 5.0, 10.0, 20.0
     hard = (reason == 1) | (reason == 3)
     curve = []
     for tol in tolerances:
-        acc = (~hard) & (ind <= tol)
-        curve.append({"tol_K": tol, "accepted": float(acc.mean()),
-                      "max_rel_T": float(eT[acc].max()) if acc.any() else 0.0,
-                      "max_dY_over_maxY": float(eY[acc].max()) if acc.any() else 0.0,
-                      "fallback_step_share": float(nst[~acc].sum() / max(nst.sum(), 1.0))})
+        for ek in ens_K:
+            for ey in ens_Y:
+                acc = (~hard) & (ind[:, 0] <= tol) & (ind[:, 1] <= ek) & (ind[:, 2] <= ey)
+                curve.append({"tol_K": tol, "ens_tol_K": ek, "ens_tol_Y": ey, "accepted": float(acc.mean()),
+                              "max_rel_T": float(eT[acc].max()) if acc.any() else 0.0,
+                              "max_dY_over_maxY": float(eY[acc].max()) if acc.any() else 0.0,
+                              "fallback_step_share": float(nst[~acc].sum() / max(nst.sum(), 1.0))})
     T0 = (s0[ns] / s0[:ns].sum(0)).cpu().numpy()
     summary = {
         "cells": n, "plain_s": t_plain, "surrogate_s": t_sur, "speedup": t_plain / t_sur,
         "accepted": st["accepted"], "fallback": st["fallback"]["cells"], "fallback_ood": st["fallback_ood"],
         "fallback_consistency": st["fallback_consistency"], "fallback_clip": st["fallback_clip"],
+        "fallback_ensemble": st["fallback_ensemble"],
         "max_rel_T": float(errT_run.max()), "p99_rel_T": float(np.quantile(errT_run, 0.99)),
         "max_dY_over_maxY": float(errY_run.max()), "p99_dY_over_maxY": float(np.quantile(errY_run, 0.99)),
         "judge_max_rel_dT": st["judge_max_rel_dT"], "judge_max_dY": st["judge_max_dY"],
@@ -121,7 +125,8 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(1.0, 2.0, 5.0, 10.0, 20.0
         "prediction_max_rel_T": float(eT.max()), "prediction_p99_rel_T": float(np.quantile(eT, 0.99)),
         "tolerance_curve": curve,
     }
-    cells = {"errT": eT.astype(np.float32), "errY": eY.astype(np.float32), "ind": ind.astype(np.float32),
+    cells = {"errT": eT.astype(np.float32), "errY": eY.astype(np.float32), "ind": ind[:, 0].astype(np.float32),
+             "ensT": ind[:, 1].astype(np.float32), "ensY": ind[:, 2].astype(np.float32),
              "reason": reason.astype(np.int8), "T0": T0.astype(np.float32), "dt": dts.astype(np.float32),
              "nst": nst.astype(np.int32)}
     return summary, cells
@@ -131,31 +136,36 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--mech", default="grimech30")
     ap.add_argument("--pairs", type=int, default=1 << 23)
-    ap.add_argument("--epochs", type=int, default=40)
-    ap.add_argument("--batch", type=int, default=8192)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--batch", type=int, default=16384)
+    ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--eval-cells", type=int, default=1 << 18)
-    ap.add_argument("--target-mode", type=int, default=0)
-    ap.add_argument("--post-mode", type=int, default=0)
+    ap.add_argument("--target-mode", type=int, default=1)
+    ap.add_argument("--post-mode", type=int, default=1)
+    ap.add_argument("--members", type=int, default=2)
     ap.add_argument("--loss-T-weight", type=float, default=2.0)
     ap.add_argument("--consist-tol", type=float, default=5.0)
     ap.add_argument("--out", required=True)
+    ap.add_argument("--cells-out", default="", help="write the per-cell evaluation arrays (.npz) here")
     a = ap.parse_args(argv)
     chem = capi.FiniteChem(a.mech, "fp64")
     t0 = time.perf_counter()
     s0, s1, d, solve_s = make_pairs(chem, a.pairs, a.seed)
     t_pairs = time.perf_counter() - t0
     sur = capi.Surrogate(chem, target_mode=a.target_mode, post_mode=a.post_mode, loss_T_weight=a.loss_T_weight,
-                         consist_tol_K=a.consist_tol)
+                         consist_tol_K=a.consist_tol, members=a.members)
     t0 = time.perf_counter()
     losses = sur.train(s0, s1, d, P_ATM, epochs=a.epochs, batch=a.batch, lr=a.lr)
     t_train = time.perf_counter() - t0
     del s0, s1, d
     sur.save(a.out)
-    ev, _ = evaluate(chem, sur, a.eval_cells, a.seed + 99991)
+    ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991)
+    if a.cells_out:
+        np.savez_compressed(a.cells_out, **cells)
     log = {"mechanism": a.mech, "pairs": a.pairs, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
            "target_mode": a.target_mode, "post_mode": a.post_mode, "loss_T_weight": a.loss_T_weight,
+           "members": a.members,
            "consist_tol_K": a.consist_tol,
            "pairs_s": t_pairs, "plain_solve_s": solve_s, "train_s": t_train,
            "losses": [float(v) for v in losses], "eval": ev}
