@@ -49,8 +49,10 @@ def test_tensor_core_chain_matches_fp32_forward(trained):
     Y32 = sur.forward_f32(X)
     torch.cuda.synchronize()
     a, b = Y_tc.cpu().numpy()[:, :sur.n_out], Y32.cpu().numpy()[:, :sur.n_out]
-    # BF16 operands, FP32 accumulation: agreement at the BF16 rounding level
-    scale = np.abs(b).max(axis=0) + 1e-3
+    # BF16 operands, FP32 accumulation: agreement at the BF16 rounding level of the layer
+    # activations, which are O(1) (outputs whose own range is smaller -- trace species under the
+    # shared output scale -- are compared against 1)
+    scale = np.maximum(np.abs(b).max(axis=0), 1.0)
     assert np.isfinite(a).all()
     assert np.max(np.abs(a - b) / scale) < 0.05
     assert np.median(np.abs(a - b) / scale) < 0.005
