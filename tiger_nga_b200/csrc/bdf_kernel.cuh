@@ -129,7 +129,10 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
     if (!(dt > 0.0)) goto finish;
     ewt[0] = h0 ? 1.0 / (rtol * fabs(u0) + atol) : 0.0;
     ewt[1] = h1 ? 1.0 / (rtol * fabs(u1) + atol) : 0.0;
-    rhs_warp(t, w, u0, u1, p, f[0], f[1], lane);
+    {
+      const double2 r = rhs_call(t, w, u0, u1, p, lane);
+      f[0] = r.x, f[1] = r.y;
+    }
     if (!warp_all_finite(f[0], f[1], nv, lane)) {
       status = ST_NONFINITE;
       goto finish;
@@ -149,8 +152,8 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
         hnew = hlb;
       } else {
         for (int it = 0; it < 4; ++it) {
-          double g0, g1;
-          rhs_warp(t, w, u0 + hg * f[0], u1 + hg * f[1], p, g0, g1, lane);
+          const double2 gg = rhs_call(t, w, u0 + hg * f[0], u1 + hg * f[1], p, lane);
+          const double g0 = gg.x, g1 = gg.y;
           const double ydd = wrms2((g0 - f[0]) / hg, (g1 - f[1]) / hg, ewt[0], ewt[1], nv, lane);
           hnew = (ydd * hub * hub > 2.0) ? sqrt(2.0 / ydd) : sqrt(hg * hub);
           if (!isfinite(hnew)) hnew = hg;
@@ -220,15 +223,17 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
         bool conv_fail = false;
         bool jcur = false;
         if (need_j || nst >= nst_lu + msbp || fabs(gamma / gamma_lu - 1.0) > dgmax) {
-          rhs_warp(t, w, z[0][0], z[0][1], p, f[0], f[1], lane);
-          jac_warp(t, w, rs, z[0][0], z[0][1], f[0], f[1], p, lane);
+          {
+            const double2 r = rhs_call(t, w, z[0][0], z[0][1], p, lane);
+            f[0] = r.x, f[1] = r.y;
+          }
+          jac_call(t, w, rs, z[0][0], z[0][1], f[0], f[1], p, lane);
           ++nje;
           for (int e = lane; e < nv * rs; e += 32) w.mat[e] = -gamma * w.mat[e];
           __syncwarp();
           for (int i = lane; i < nv; i += 32) w.mat[i * rs + i] += 1.0;
           __syncwarp();
-          const int sing = lu_warp(w.mat, nv, rs, w.piv, lane);
-          lu_finish(w.mat, nv, rs, w.piv, w.perm, w.cb, lane);
+          const int sing = lu_call(w.mat, nv, rs, w.piv, w.perm, w.cb, lane);
           gamma_lu = gamma;
           nst_lu = nst;
           jcur = true;
@@ -243,7 +248,10 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
           y[1] = z[0][1];
           conv_fail = true;
           for (int it = 0; it < maxcor; ++it) {
-            rhs_warp(t, w, y[0], y[1], p, f[0], f[1], lane);
+            {
+              const double2 r = rhs_call(t, w, y[0], y[1], p, lane);
+              f[0] = r.x, f[1] = r.y;
+            }
             ++nni;
             x[0] = h * f[0] - z[1][0] - acor[0];
             x[1] = h * f[1] - z[1][1] - acor[1];
@@ -300,7 +308,10 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
           if (nef >= 3 && q > 1) {
             h *= 0.1;
             q = 1;
-            rhs_warp(t, w, z[0][0], z[0][1], p, f[0], f[1], lane);
+            {
+              const double2 r = rhs_call(t, w, z[0][0], z[0][1], p, lane);
+              f[0] = r.x, f[1] = r.y;
+            }
             z[1][0] = h * f[0];
             z[1][1] = h * f[1];
             qwait = 2;
@@ -441,12 +452,12 @@ __global__ void __launch_bounds__(WARPS * 32)
   for (int cell = blockIdx.x * WARPS + warp; cell < n; cell += gridDim.x * WARPS) {
     const double y0 = lane < nv ? state[(long long)lane * ld + cell] : 0.0;
     const double y1 = lane + 32 < nv ? state[(long long)(lane + 32) * ld + cell] : 0.0;
-    double f0, f1;
-    rhs_warp(t, w, y0, y1, p, f0, f1, lane);
+    const double2 r = rhs_call(t, w, y0, y1, p, lane);
+    const double f0 = r.x, f1 = r.y;
     if (lane < nv) rhs[(long long)lane * ld + cell] = f0;
     if (lane + 32 < nv) rhs[(long long)(lane + 32) * ld + cell] = f1;
     if (jac) {
-      jac_warp(t, w, rs, y0, y1, f0, f1, p, lane);
+      jac_call(t, w, rs, y0, y1, f0, f1, p, lane);
       for (int e = lane; e < nv * nv; e += 32) jac[(long long)cell * nv * nv + e] = w.mat[(e / nv) * rs + e % nv];
       __syncwarp();
     }

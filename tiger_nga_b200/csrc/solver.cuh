@@ -301,6 +301,16 @@ __device__ __forceinline__ void rhs_warp(const SvDev& t, const WarpMem& w, const
   __syncwarp();
 }
 
+// One out-of-line copy of the right-hand side. The solver evaluates it from several places;
+// inlined at each of them, the kernel's code outgrows the instruction cache and the warps stall
+// on instruction fetch.
+static __device__ __noinline__ double2 rhs_call(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+                                                const double p, const int lane) {
+  double f0, f1;
+  rhs_warp(t, w, y0, y1, p, f0, f1, lane);
+  return make_double2(f0, f1);
+}
+
 // Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
 // row stride rs). Uses one extra right-hand side for the temperature column.
 __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const double y0,
@@ -399,8 +409,8 @@ __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const
   const double dlt = 1.4901161193847656e-08 * fmax(fabs(yN), 1e-30);
   const double yNp = yN + dlt;
   const double idl = 1.0 / (yNp - yN);
-  double g0, g1;
-  rhs_warp(t, w, lane == ns ? yNp : y0, lane + 32 == ns ? yNp : y1, p, g0, g1, lane);
+  const double2 gg = rhs_call(t, w, lane == ns ? yNp : y0, lane + 32 == ns ? yNp : y1, p, lane);
+  const double g0 = gg.x, g1 = gg.y;
   if (lane < nv) w.mat[lane * rs + ns] = (g0 - f0) * idl;
   if (lane + 32 < nv) w.mat[(lane + 32) * rs + ns] = (g1 - f1) * idl;
   __syncwarp();
@@ -515,6 +525,20 @@ __device__ __forceinline__ void lu_finish(const double* a, const int n, const in
   }
   for (int i = lane; i < n; i += 32) dinv[i] = 1.0 / a[i * rs + i];
   __syncwarp();
+}
+
+// Out-of-line Jacobian and factorisation (one copy each, as rhs_call).
+static __device__ __noinline__ void jac_call(const SvDev& t, const WarpMem& w, const int rs, const double y0,
+                                             const double y1, const double f0, const double f1, const double p,
+                                             const int lane) {
+  jac_warp(t, w, rs, y0, y1, f0, f1, p, lane);
+}
+
+static __device__ __noinline__ int lu_call(double* a, const int n, const int rs, int* piv, int* perm, double* dinv,
+                                           const int lane) {
+  const int sing = lu_warp(a, n, rs, piv, lane);
+  lu_finish(a, n, rs, piv, perm, dinv, lane);
+  return sing;
 }
 
 // Solve (LU) x = b with b and x two entries per lane in registers: permutation by one gather,
