@@ -198,7 +198,7 @@ typedef struct tng_surrogate_cfg {
   int layers;             /* hidden layers (default 4) */
   uint64_t seed;          /* weight initialisation */
   double ood_margin;      /* allowed excursion beyond the training range, fraction of the range (0.02) */
-  double consist_tol_K;   /* fallback when network and enthalpy temperatures differ by more (K, 2) */
+  double consist_tol_K;   /* fallback when network and enthalpy temperatures differ by more (K, 5) */
   double clip_tol;        /* fallback when clipping removed more mass fraction (1e-3) */
   int judge_cells;        /* cells re-solved every call to measure the error (1024) */
   int post_mode;          /* 0: T from the enthalpy balance of the conserved Y; 1: T from the network,
@@ -208,8 +208,8 @@ typedef struct tng_surrogate_cfg {
   float loss_T_weight;    /* loss weight of dT relative to one species output (0 = default 2) */
   int members;            /* networks in the ensemble, trained from different initialisations; the
                              prediction is their mean (1..4, 0 = default 2) */
-  float ens_tol_K;        /* fallback when the members' temperatures spread by more (K, 0 = default 1) */
-  float ens_tol_Y;        /* fallback when a mass fraction spreads by more (0 = default 1e-4) */
+  float ens_tol_K;        /* fallback when the members' temperatures spread by more (K, 0 = default 2) */
+  float ens_tol_Y;        /* fallback when a mass fraction spreads by more (0 = default 5e-4) */
   int reserved[2];
 } tng_surrogate_cfg;
 

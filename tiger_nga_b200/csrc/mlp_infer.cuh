@@ -21,7 +21,7 @@ namespace tng {
 
 constexpr int kInferRows = 128;
 constexpr int kInferThreads = 128;
-constexpr int kWChunkK = 64;  // K width of one streamed weight chunk
+constexpr int kWChunkK = 32;  // K width of one streamed weight chunk
 constexpr int kMaxLayers = 9;
 
 struct InferArgs {
@@ -154,12 +154,13 @@ __device__ __forceinline__ float gelu_fast(float x) {
 }
 
 // shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), two weight stages of
-// 256 x 64 bf16 (32 KB each), barriers and the TMEM address.
+// 256 x 32 bf16 (16 KB each), barriers and the TMEM address: 96 KB, two CTAs per SM (their
+// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns.
 constexpr int kSmemA = kInferRows * 256 * 2;
 constexpr int kSmemStage = 256 * kWChunkK * 2;
 constexpr int kInferSmem = kSmemA + 2 * kSmemStage + 128;
 
-__global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs a) {
+__global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* sA = sm;
   uint8_t* sW = sm + kSmemA;
@@ -181,7 +182,27 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
   const uint32_t tmem = *tmem_slot;
   uint32_t ph_full[2] = {0, 0}, ph_free[2] = {0, 0}, ph_done = 0;
   int stage_busy[2] = {0, 0};  // thread 0 only: a commit to stage_free is pending
+  int inflight[2] = {0, 0};    // thread 0 only: a weight copy into the stage has not been waited for
+  int gc = 0;                  // thread 0 only: weight chunks issued so far (stage = gc & 1)
+  int pre = 0, pre_base = 0;   // thread 0 only: chunk 0 of the coming layer already issued at gc = pre_base
   int err = 0;
+  // issue the bulk copy of weight chunk c of layer l into the next stage (thread 0)
+  auto issue = [&](int l, int c) {
+    const int K = l == 0 ? a.in_pad : a.hidden;
+    const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
+    const int s = gc & 1;
+    ++gc;
+    if (stage_busy[s]) {  // wait for the MMAs that read this stage
+      if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
+      ph_free[s] ^= 1;
+      stage_busy[s] = 0;
+    }
+    const int kc = min(kWChunkK, K - c * kWChunkK);
+    const uint32_t bytes = (uint32_t)N * kc * 2;
+    mbar_expect_tx(&bars[s], bytes);
+    bulk_g2s(sW + s * kSmemStage, a.wpack + a.w_off[l] + (long long)c * N * kWChunkK, bytes, &bars[s]);
+    inflight[s] = 1;
+  };
   const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
   for (int tile = blockIdx.x; tile < ntiles && !err; tile += gridDim.x) {
     // ---- 1. features of the tile's cells into A (K = in_pad)
@@ -191,6 +212,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
       double rho = 1.0, T = 0.0, dt = 0.0;
       if (live) {
         rho = 0.0;
+#pragma unroll 4
         for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
         T = a.state[(long long)a.ns * a.ld + cell] / rho;
         dt = a.dts ? a.dts[cell] : a.dt_scalar;
@@ -226,22 +248,19 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
       const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
       const int nchunk = (K + kWChunkK - 1) / kWChunkK;
       if (tid == 0) {
-        const __nv_bfloat16* wl = a.wpack + a.w_off[l];
         const uint32_t idesc = umma_idesc(kInferRows, N);
         const uint32_t a_sbo = (uint32_t)K * 16;
+        // chunk c sits in stage (base + c) & 1; chunk c + 1 is in flight while chunk c multiplies
+        const int base = pre ? pre_base : gc;
+        if (!pre) issue(l, 0);
+        pre = 0;
         for (int c = 0; c < nchunk && !err; ++c) {
-          const int s = c & 1;
+          if (c + 1 < nchunk) issue(l, c + 1);
+          const int s = (base + c) & 1;
           const int kc = min(kWChunkK, K - c * kWChunkK);
-          const uint32_t bytes = (uint32_t)N * kc * 2;
-          if (stage_busy[s]) {  // wait for the MMAs that read this stage
-            if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
-            ph_free[s] ^= 1;
-            stage_busy[s] = 0;
-          }
-          mbar_expect_tx(&bars[s], bytes);
-          bulk_g2s(sW + s * kSmemStage, wl + (long long)c * N * kWChunkK, bytes, &bars[s]);
           if (!mbar_wait(&bars[s], ph_full[s])) err = 1;
           ph_full[s] ^= 1;
+          inflight[s] = 0;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t wbase = smem_u32(sW + s * kSmemStage);
           const uint32_t abase = smem_u32(sA);
@@ -261,6 +280,15 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
       ph_done ^= 1;
       if (!ok) err = 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // the next layer's (or the next tile's first layer's) first weight chunk loads during the epilogue
+      if (tid == 0 && !err) {
+        const bool more = l + 1 < a.nlin || tile + (int)gridDim.x < ntiles;
+        if (more) {
+          pre_base = gc;
+          issue(l + 1 < a.nlin ? l + 1 : 0, 0);
+          pre = 1;
+        }
+      }
       const float* bl = a.bias + a.b_off[l];
       const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
       const bool last = l == a.nlin - 1;
@@ -300,13 +328,16 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_mlp_infer(const InferArgs 
       err = __syncthreads_or(err);
     }
   }
-  // drain: the last commits on the stage barriers must complete before the CTA exits
-  if (tid == 0 && !err) {
-    for (int s = 0; s < 2; ++s)
+  // drain: weight copies still in flight (after an error) and the last commits on the stage
+  // barriers must complete before the CTA exits; every wait is bounded
+  if (tid == 0) {
+    for (int s = 0; s < 2; ++s) {
+      if (inflight[s] && !mbar_wait(&bars[s], ph_full[s])) err = 1;
       if (stage_busy[s]) {
         if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
         ph_free[s] ^= 1;
       }
+    }
   }
   if (err && tid == 0 && a.error) atomicExch(a.error, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

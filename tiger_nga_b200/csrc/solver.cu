@@ -141,20 +141,40 @@ static int configure_kernel(tng_chem* h, int warps, int* blocks_out) {
   return TNG_OK;
 }
 
+// Totals of the per-cell counters: per-thread partials, warp sums, one global atomic per warp
+// (one atomic per cell and counter serialised on the same addresses).
 static __global__ void k_stats(const int* nst, const int* nni, const int* nje, const int* status, int64_t n,
                                unsigned long long* acc /* 5 + 2 + 16 */) {
+  __shared__ unsigned long long hist[16];
+  if (threadIdx.x < 16) hist[threadIdx.x] = 0;
+  __syncthreads();
+  unsigned long long s0 = 0, s1 = 0, s2 = 0, s3 = 0, m0 = 0, m1 = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int a = nst[i], b = nni[i], c = nje[i];
-    atomicAdd(&acc[0], (unsigned long long)a);
-    atomicAdd(&acc[1], (unsigned long long)b);
-    atomicAdd(&acc[2], (unsigned long long)c);
-    if (status[i] != 0) atomicAdd(&acc[3], 1ULL);
-    atomicMax(&acc[4], (unsigned long long)a);
-    atomicMax(&acc[5], (unsigned long long)b);
+    s0 += a, s1 += b, s2 += c, s3 += status[i] != 0;
+    m0 = max(m0, (unsigned long long)a), m1 = max(m1, (unsigned long long)b);
     int bin = 0;
     for (int v = b; v > 0 && bin < 15; v >>= 1) ++bin;
-    atomicAdd(&acc[8 + bin], 1ULL);
+    atomicAdd(&hist[bin], 1ULL);
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    m0 = max(m0, __shfl_xor_sync(0xffffffffu, m0, o));
+    m1 = max(m1, __shfl_xor_sync(0xffffffffu, m1, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (s0) atomicAdd(&acc[0], s0);
+    if (s1) atomicAdd(&acc[1], s1);
+    if (s2) atomicAdd(&acc[2], s2);
+    if (s3) atomicAdd(&acc[3], s3);
+    atomicMax(&acc[4], m0);
+    atomicMax(&acc[5], m1);
+  }
+  __syncthreads();
+  if (threadIdx.x < 16 && hist[threadIdx.x]) atomicAdd(&acc[8 + threadIdx.x], hist[threadIdx.x]);
 }
 
 int solver_prepare(tng_chem* h) {

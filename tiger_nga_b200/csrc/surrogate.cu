@@ -464,7 +464,7 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double*
   ia.error = err;
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
   if (e != cudaSuccess) return cuda_error(e, "inference shared memory");
-  const int grid = (int)std::min<int64_t>(h->sm_count, (ncells + kInferRows - 1) / kInferRows);
+  const int grid = (int)std::min<int64_t>(2 * h->sm_count, (ncells + kInferRows - 1) / kInferRows);
   k_mlp_infer<<<grid, kInferThreads, kInferSmem, h->stream>>>(ia);
   e = cudaGetLastError();
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "tensor-core inference");
@@ -515,14 +515,14 @@ void tng_surrogate_default_cfg(tng_surrogate_cfg* c) {
   c->layers = 4;
   c->seed = 20261203;
   c->ood_margin = 0.02;
-  c->consist_tol_K = 2.0;
+  c->consist_tol_K = 5.0;
   c->clip_tol = 1e-3;
   c->judge_cells = 1024;
   c->post_mode = 1;
   c->target_mode = 1;
   c->members = 2;
-  c->ens_tol_K = 1.f;
-  c->ens_tol_Y = 1e-4f;
+  c->ens_tol_K = 2.f;
+  c->ens_tol_Y = 5e-4f;
 }
 
 int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogate** out) {
@@ -534,8 +534,8 @@ int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogat
   else
     tng_surrogate_default_cfg(&c);
   if (c.members == 0) c.members = 2;
-  if (!(c.ens_tol_K > 0.f)) c.ens_tol_K = 1.f;
-  if (!(c.ens_tol_Y > 0.f)) c.ens_tol_Y = 1e-4f;
+  if (!(c.ens_tol_K > 0.f)) c.ens_tol_K = 2.f;
+  if (!(c.ens_tol_Y > 0.f)) c.ens_tol_Y = 5e-4f;
   if (c.members < 1 || c.members > kMaxMembers)
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: 1..%d ensemble members", kMaxMembers);
   if (c.hidden != 256 || c.layers < 1 || c.layers > kMaxLayers - 1)

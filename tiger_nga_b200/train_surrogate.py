@@ -145,7 +145,7 @@ def main(argv=None):
     ap.add_argument("--post-mode", type=int, default=1)
     ap.add_argument("--members", type=int, default=2)
     ap.add_argument("--loss-T-weight", type=float, default=2.0)
-    ap.add_argument("--consist-tol", type=float, default=2.0)
+    ap.add_argument("--consist-tol", type=float, default=5.0)
     ap.add_argument("--out", required=True)
     ap.add_argument("--cells-out", default="", help="write the per-cell evaluation arrays (.npz) here")
     a = ap.parse_args(argv)
