@@ -18,6 +18,12 @@ Workloads (seeded synthetic states, built like the reference's init_flow tool; t
   gri-rates        production-rate evaluation only (finitechem_compute_rhs + PRODRATES),
                    128^3 cells, FP64.
   gri-rates-mixed  the same in mixed precision (FP32 log-space rates, FP64 reverse exponents).
+  dme-sweep        the DME39 mechanism on a 256x192x192 temporal mixing layer (DME at 400 K above air
+                   at 300 K, tanh mixture-fraction profile plus seeded Fourier perturbations of
+                   amplitude 0.1, seeded burning fraction), 100 consecutive substeps of dt = 2e-6 s
+                   with the state resident on the device, through the surrogate with fallback;
+                   reports the hit rate, the fallback cost and the p50/p99 substep latency, and the
+                   accuracy after all substeps against the plain solve of a strided subsample.
 
 A step is one pass of the hot path over the whole batch, starting every time from the same
 initial state (restored outside the timed interval). `value` is device-timed with CUDA events
@@ -43,12 +49,17 @@ sys.path.insert(0, REPO)
 import numpy as np  # noqa: E402
 
 P_ATM = 101325.0
-SURROGATE_FILE = os.path.join(REPO, "tiger_nga_b200", "models", "grimech30.tngs")
+MODELS = os.path.join(REPO, "tiger_nga_b200", "models")
 WORKLOADS = {
     "gri-surrogate": {"kind": "surrogate", "mech": "grimech30", "side": 128, "precision": "fp64",
                       "metric": "GRI-3.0 substep cells/s: surrogate+fallback vs plain GPU at ≤1% ΔT error",
                       "desc": "GRI-Mech 3.0 stand-in (36 sp) substep, 128^3 cells, per-cell dt 1e-7..1e-5 s, "
                               "surrogate (tcgen05 BF16 MLP) + implicit fallback", "steps": 5, "ref_sample": 2048},
+    "dme-sweep": {"kind": "sweep", "mech": "dme39", "shape": (256, 192, 192), "precision": "fp64",
+                  "metric": "DME39 mixing-layer sweep cell-substeps/s (surrogate+fallback, 100 substeps resident)",
+                  "desc": "DME39 temporal mixing layer 256x192x192, dt = 2e-6 s, 100 consecutive substeps on the "
+                          "device through the surrogate with implicit fallback", "steps": 100, "ref_sample": 2048,
+                  "weights": "dme39.tngs"},
     "gri-substep": {"kind": "substep", "mech": "grimech30", "side": 128, "precision": "fp64",
                     "metric": "GRI-3.0 (36-sp stand-in) implicit substep cells/s",
                     "desc": "GRI-Mech 3.0 stand-in (36 sp) implicit substep, 128^3 cells, per-cell dt 1e-7..1e-5 s",
@@ -67,7 +78,7 @@ WORKLOADS = {
                         "steps": 400, "ref_sample": 131072},
 }
 # kernels of this library launched per step (counted from the host code of each path)
-LAUNCHES = {"rates": 1, "substep": 2, "surrogate": 8}
+LAUNCHES = {"rates": 1, "substep": 2, "surrogate": 8, "sweep": 8}
 
 
 def dist_env():
@@ -148,8 +159,11 @@ def make_state(wl, rank):
     from tiger_nga_b200.mechanism import load
 
     mech = load(wl["mech"])
-    n = wl["side"] ** 3
     seed = 20261204 + rank
+    if wl["kind"] == "sweep":
+        sol, _ = states.mixing_layer(mech, shape=wl["shape"], seed=20261205 + rank)
+        return sol, 2e-6
+    n = wl["side"] ** 3
     if wl["mech"] == "hydrogen":
         sol, _ = states.h2_cube(mech, wl["side"], seed)
         return sol, 1e-6
@@ -263,6 +277,143 @@ def solver_flops(mech, st):
     return st["newton_iters"] * (rf + 2 * nv * nv) + st["jacobians"] * (2.0 / 3.0) * nv ** 3
 
 
+def run_sweep(args, wl, config, metric, unit, ws, rank, local, dev, pg):
+    """K consecutive substeps of a resident state through the surrogate with fallback."""
+    import torch
+
+    from tiger_nga_b200 import capi
+    from tiger_nga_b200.mechanism import load
+
+    mech = load(wl["mech"])
+    sol, dt = make_state(wl, rank)
+    ncells = sol.shape[1]
+    chem = capi.FiniteChem(wl["mech"], wl["precision"], device=local)
+    st = chem.torch_stream()
+    if not os.path.exists(args.surrogate):
+        raise FileNotFoundError(f"trained surrogate weights not found: {args.surrogate}")
+    sur = capi.Surrogate(chem)
+    sur.load(args.surrogate)
+    x0 = torch.from_numpy(sol).to(dev)
+    work = x0.clone()
+    for _ in range(args.warmup):
+        sur.substep(work, dt, P_ATM)
+    work.copy_(x0)
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    clocks = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
+    clocks.start()
+    time.sleep(0.3)
+    per, acc, fb, fb_ms, inf_ms, post_ms, judgeT, judgeY = [], 0, 0, 0.0, 0.0, 0.0, 0.0, 0.0
+    solver_tot = {"steps": 0, "newton_iters": 0, "jacobians": 0, "cells": 0}
+    solver_ms = 0.0
+    t_wall = time.perf_counter()
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        r = sur.substep(work, dt, P_ATM)
+        e1.record(st)
+        e1.synchronize()
+        per.append(e0.elapsed_time(e1))
+        acc += r["accepted"]
+        fb += r["fallback"]["cells"]
+        fb_ms += r["ms_fallback"]
+        inf_ms += r["ms_infer"]
+        post_ms += r["ms_post"]
+        judgeT = max(judgeT, r["judge_max_rel_dT"])
+        judgeY = max(judgeY, r["judge_max_dY"])
+        for k in solver_tot:
+            solver_tot[k] += r["fallback"][k]
+        solver_ms += r["fallback"]["ms"]
+    t_wall = time.perf_counter() - t_wall
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms_total = max_over_ranks(pg, dev, sum(per))
+    ms_step = ms_total / args.steps
+    value = ncells * ws / (ms_step * 1e-3)
+    if not bool(torch.isfinite(work).all()):
+        raise RuntimeError("non-finite values after the sweep")
+    # accuracy after all substeps: the plain implicit solve of a strided subsample, substep by substep
+    m = min(16384, ncells)
+    idx = torch.arange(0, ncells, max(1, ncells // m), device=dev)[:m]
+    ref = x0[:, idx].contiguous()
+    for _ in range(args.steps):
+        chem.substep(ref, dt, P_ATM, stats=False)
+    torch.cuda.synchronize(dev)
+    got = work[:, idx]
+    ns = mech.ns
+    rg, rr = got[:ns].sum(0), ref[:ns].sum(0)
+    errT = ((got[ns] / rg - ref[ns] / rr).abs() / (ref[ns] / rr))
+    errY = ((got[:ns] / rg - ref[:ns] / rr).abs().amax(0) / (ref[:ns] / rr).amax(0))
+    pa = np.array(per)
+    extra = {
+        "substep_latency_ms": {"p50": float(np.percentile(pa, 50)), "p99": float(np.percentile(pa, 99)),
+                               "max": float(pa.max()), "min": float(pa.min())},
+        "surrogate": {"hit_rate": acc / (ncells * args.steps), "fallback_cells_per_substep": fb / args.steps,
+                      "fallback_ms_per_substep": fb_ms / args.steps, "infer_ms_per_substep": inf_ms / args.steps,
+                      "post_ms_per_substep": post_ms / args.steps, "fallback_share_of_time": fb_ms / sum(per),
+                      "judge_max_rel_dT": judgeT, "judge_max_dY": judgeY,
+                      "weights": os.path.relpath(args.surrogate, REPO)},
+        "accuracy_vs_plain_gpu_after_all_substeps": {
+            "cells": m, "substeps": args.steps, "max_rel_T": float(errT.max()),
+            "p99_rel_T": float(torch.quantile(errT.float(), 0.99)), "max_dY_over_maxY": float(errY.max()),
+            "p99_dY_over_maxY": float(torch.quantile(errY.float(), 0.99))},
+        "solver": dict(solver_tot, ms=solver_ms),
+    }
+    hbm_peak, bf16_peak, peak_src = peaks()
+    roof = None
+    flops = solver_flops(mech, solver_tot) if solver_tot["newton_iters"] else None
+    if flops and solver_ms > 0:
+        fp64_peak = capi.fp64_peak_tflops(local)
+        ach = flops / (solver_ms * 1e-3) / 1e12
+        nbytes = 2 * (mech.ns + 1) * 8 * solver_tot["cells"]
+        roof = {"bound": "hbm", "achieved": nbytes / (solver_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": nbytes / (solver_ms * 1e-3) / 1e9 / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "kernel": "k_bdf",
+                "fp64_pipe": {"achieved_tflops": ach, "peak_tflops_measured": fp64_peak, "frac": ach / fp64_peak,
+                              "counted_flops": flops}}
+    if inf_ms > 0 and bf16_peak:
+        ach = 2.0 * sur.nparam * ncells * args.steps / (inf_ms * 1e-3) / 1e12
+        extra["inference_roofline"] = {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
+                                       "frac": ach / bf16_peak, "peak_source": peak_src, "kernel": "k_mlp_infer"}
+    # e2e: substeps through the host-pointer call (state copied in and out every substep)
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else 1
+    hin = torch.from_numpy(sol).pin_memory()
+    hbuf = hin.clone().pin_memory()
+    sur.substep(hbuf.numpy(), dt, P_ATM)  # warm-up
+    hbuf.copy_(hin)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sur.substep(hbuf.numpy(), dt, P_ATM)
+    e2e_s = max_over_ranks(pg, dev, (time.perf_counter() - t0) / e2e_steps)
+    e2e = {"value": ncells * ws / e2e_s, "unit": unit, "h2d_bytes_per_step": sol.nbytes * ws,
+           "d2h_bytes_per_step": sol.nbytes * ws, "steps": e2e_steps}
+    cpu = None
+    if rank == 0 and ws == 1 and args.cpu_seconds > 0:
+        kind, cval, cdone, cel = time_cpu(wl, sol, dt, args.cpu_seconds, os.cpu_count() or 1)
+        cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
+               "sample": f"{cdone} cells ({cel:.1f} s) of the initial mixing layer, one implicit BDF/Newton "
+                         "substep each (no surrogate), OpenMP over cells"}
+    if rank == 0:
+        line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16/f32 (network), f64 (conservation, fallback solve)",
+                "data": "synthetic (seeded DME/air temporal mixing layer)", "config": config, "e2e": e2e,
+                "gpu_launches": LAUNCHES["sweep"] * args.steps, "roofline": roof, "cpu_baseline": cpu,
+                "clocks": clk, "wall_s": t_wall}
+        line.update(extra)
+        print(json.dumps(line))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    sur.close()
+    chem.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -275,19 +426,24 @@ def main():
     ap.add_argument("--plain-cells", type=int, default=262144,
                     help="gri-surrogate: cells of the strided subsample solved by the plain GPU path (0 = all)")
     ap.add_argument("--side", type=int, default=0, help="cube side override (small profiling cases)")
-    ap.add_argument("--surrogate", default=SURROGATE_FILE)
+    ap.add_argument("--surrogate", default="", help="weights file (default: the workload's trained model)")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     wl = dict(WORKLOADS[args.workload])
     if args.side:
-        wl["side"] = args.side
+        if wl["kind"] == "sweep":
+            wl["shape"] = (args.side, args.side * 3 // 4, args.side * 3 // 4)
+        else:
+            wl["side"] = args.side
+    if not args.surrogate:
+        args.surrogate = os.path.join(MODELS, wl.get("weights", "grimech30.tngs"))
     if args.steps <= 0:
         args.steps = wl["steps"]
     args.warmup = max(args.warmup, 3)
     from tiger_nga_b200.mechanism import load
 
     mech = load(wl["mech"])
-    ncells = wl["side"] ** 3
+    ncells = int(np.prod(wl["shape"])) if wl["kind"] == "sweep" else wl["side"] ** 3
     config = {"workload": args.workload, "desc": wl["desc"], "mechanism": wl["mech"], "cells_per_gpu": ncells,
               "pressure_pa": P_ATM, "precision": wl["precision"],
               "l2": "inputs larger than L2 (no flush needed)" if ncells * (mech.ns + 1) * 8 > 126e6 else
@@ -314,6 +470,8 @@ def main():
         pg = dist
     from tiger_nga_b200 import capi
 
+    if wl["kind"] == "sweep":
+        return run_sweep(args, wl, config, metric, unit, ws, rank, local, dev, pg)
     sol, dts = make_state(wl, rank)
     chem = capi.FiniteChem(wl["mech"], wl["precision"], device=local)
     st = chem.torch_stream()

@@ -121,11 +121,12 @@ def adiabatic_T(mech: Mechanism, Yu, Tu, Yb, iters: int = 40) -> np.ndarray:
 
 def chem_state(mech: Mechanism, ncells: int, seed: int, fuel: str, T_fuel: float = 300.0, T_air: float = 300.0,
                minor=(1e-10, 1e-3), minor_species=None, progress: str = "uniform", T_range=None,
-               grid=None, p: float = P_ATM, z=None):
+               grid=None, p: float = P_ATM, z=None, c=None):
     """Seeded state batch. Returns (sol (N+1, ncells), info dict with Y, T, rho, Z, c).
 
     progress: 'uniform' (c ~ U[0,1]) or 'beta22' (c ~ Beta(2,2)); with T_range=(lo, hi) the
-    temperature is lo + c (hi - lo) instead of the burnt/unburnt blend.
+    temperature is lo + c (hi - lo) instead of the burnt/unburnt blend. z and c, when given,
+    are the mixture fraction and progress of every cell.
     """
     rng = np.random.default_rng(seed + 7919)
     if z is None:
@@ -143,7 +144,9 @@ def chem_state(mech: Mechanism, ncells: int, seed: int, fuel: str, T_fuel: float
     Yut = yf[:, None] * zt[None, :] + ya[:, None] * (1.0 - zt[None, :])
     Tbt = adiabatic_T(mech, Yut, T_fuel * zt + T_air * (1.0 - zt), burnt(mech, fuel, Yut))
     Tb = np.interp(Z, zt, Tbt)
-    if progress == "uniform":
+    if c is not None:
+        c = np.asarray(c, dtype=np.float64).reshape(-1)
+    elif progress == "uniform":
         c = rng.uniform(0.0, 1.0, ncells)
     elif progress == "beta22":
         c = rng.beta(2.0, 2.0, ncells)
@@ -182,3 +185,29 @@ def ch4_cube(mech: Mechanism, n: int = 128, seed: int = 20261204, progress: str 
     """CH4/air, n^3 cells, minor species log-uniform in [1e-10, 1e-3]."""
     return chem_state(mech, n ** 3, seed, "CH4", minor=(1e-10, 1e-3), grid=(n, n, n), progress=progress,
                       T_range=T_range)
+
+
+def mixing_layer(mech: Mechanism, shape=(256, 192, 192), seed: int = 20261205, fuel: str = "CH3OCH3",
+                 T_fuel: float = 400.0, T_air: float = 300.0, thickness: float = 0.08, amp: float = 0.1,
+                 minor=(1e-10, 1e-3), p: float = P_ATM, chunk: int = 1 << 20):
+    """Temporal mixing layer on a (nx, ny, nz) grid: fuel above air along y.
+
+    Z = (1 + tanh((y - 1/2) / thickness)) / 2 + amp * (2 F - 1), clipped to [0, 1], with F a seeded
+    smooth Fourier field in [0, 1]; the burning fraction c is a second seeded smooth field, which
+    blends the unburnt mixture with its complete-combustion products (T up to adiabatic); minor
+    species log-uniform in ``minor``. Built in chunks of cells (memory bounded). Returns
+    (sol (N+1, ncells) C-ordered over (x, y, z), info with Z and c).
+    """
+    nx, ny, nz = shape
+    y = (np.arange(ny, dtype=np.float64) + 0.5) / ny
+    prof = 0.5 * (1.0 + np.tanh((y - 0.5) / thickness))
+    Z = np.clip(prof[None, :, None] + amp * (2.0 * fourier_field(shape, seed) - 1.0), 0.0, 1.0).reshape(-1)
+    c = fourier_field(shape, seed + 1).reshape(-1)
+    n = Z.size
+    sol = np.empty((mech.ns + 1, n))
+    for k, lo in enumerate(range(0, n, chunk)):
+        hi = min(n, lo + chunk)
+        part, _ = chem_state(mech, hi - lo, seed + 101 * (k + 1), fuel, T_fuel=T_fuel, T_air=T_air, minor=minor,
+                             p=p, z=Z[lo:hi], c=c[lo:hi])
+        sol[:, lo:hi] = part
+    return sol, {"Z": Z, "c": c, "shape": shape}

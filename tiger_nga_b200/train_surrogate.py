@@ -3,11 +3,13 @@
     python -m tiger_nga_b200.train_surrogate --mech grimech30 --pairs 8388608 \\
         --out tiger_nga_b200/models/grimech30.tngs
 
-Pairs: seeded states of the uneven-stiffness batch -- 128^3 grids of a smooth Fourier-mode
+Pairs (--dist uneven, the default): seeded states of the uneven-stiffness batch -- 128^3 grids of a smooth Fourier-mode
 mixture-fraction field (CH4 fuel / air at 300 K for GRI-Mech, DME at 400 K for DME39),
 progress c ~ Beta(2,2) mapped to T in [300, 2400] K, minor species log-uniform in
 [1e-10, 1e-3], dt log-uniform in [1e-7, 1e-5] s per cell, P = 1 atm -- each advanced by
-tng_substep_batch. The network is trained by the library's own CUDA kernels
+tng_substep_batch. With --dist mixing-layer the pairs are taken along 100-substep
+(dt = 2e-6 s) trajectories of temporal mixing layers (fuel above air, seeded burning fraction)
+instead. The network is trained by the library's own CUDA kernels
 (tng_surrogate_train: FP32 forward/backward, Adam, cosine learning rate), then evaluated
 on fresh cells against the plain solve (accepted fraction, max relative error of T, max
 species error over max Y). Writes the weights file and a JSON log beside it.
@@ -63,8 +65,46 @@ def make_pairs(chem, n_pairs: int, seed: int, chunk: int = 1 << 21):
     return s0, s1, d, solve_s
 
 
+def make_trajectory_pairs(chem, n_pairs: int, seed: int, dt: float = 2e-6, substeps: int = 100,
+                          shape=(64, 48, 48), grids: int = 2):
+    """(s0, s1, dt) pairs along implicit-solver trajectories of temporal mixing layers.
+
+    Each of ``grids`` seeded mixing layers (fuel above air, seeded burning fraction) is advanced
+    ``substeps`` times by dt with tng_substep_batch; every substep contributes a random subset of
+    its cells, so the pairs cover the states a 100-substep run visits, not only the first.
+    """
+    import torch
+
+    m = load(chem.mechanism)
+    fuel, t_fuel = FUEL[chem.mechanism]
+    nv = chem.nspecies + 1
+    per = -(-n_pairs // (grids * substeps))
+    s0 = torch.empty((nv, n_pairs), dtype=torch.float64, device="cuda")
+    s1 = torch.empty_like(s0)
+    done, solve_s = 0, 0.0
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    for g in range(grids):
+        sol, _ = states.mixing_layer(m, shape=shape, seed=seed + 7 * g, fuel=fuel, T_fuel=t_fuel)
+        x = torch.from_numpy(sol).cuda()
+        for k in range(substeps):
+            take = min(per, n_pairs - done, x.shape[1])
+            if take <= 0:
+                break
+            idx = torch.randperm(x.shape[1], device="cuda", generator=gen)[:take]
+            s0[:, done:done + take] = x[:, idx]
+            t0 = time.perf_counter()
+            chem.substep(x, dt, P_ATM)
+            torch.cuda.synchronize()
+            solve_s += time.perf_counter() - t0
+            s1[:, done:done + take] = x[:, idx]
+            done += take
+    d = torch.full((done,), dt, dtype=torch.float64, device="cuda")
+    return s0[:, :done].contiguous(), s1[:, :done].contiguous(), d, solve_s
+
+
 def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.0, 2.0, 4.0),
-             ens_Y=(1e-4, 2e-4, 5e-4, 1e-3)):
+             ens_Y=(1e-4, 2e-4, 5e-4, 1e-3), dist: str = "uneven"):
     """The surrogate against the plain solve on n fresh cells.
 
     Returns the timed surrogate-with-fallback substep (stats, speed-up over the plain solve) and,
@@ -74,7 +114,13 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.
     """
     import torch
 
-    sol, dts = state_batch(chem.mechanism, n, seed, side=128 if n == 1 << 21 else 0)
+    if dist == "mixing-layer":
+        fuel, t_fuel = FUEL[chem.mechanism]
+        sol, _ = states.mixing_layer(load(chem.mechanism), shape=(64, 48, 48), seed=seed, fuel=fuel, T_fuel=t_fuel)
+        dts = np.full(sol.shape[1], 2e-6)
+        n = sol.shape[1]
+    else:
+        sol, dts = state_batch(chem.mechanism, n, seed, side=128 if n == 1 << 21 else 0)
     s0 = torch.from_numpy(sol).cuda()
     d = torch.from_numpy(dts).cuda()
     ref = s0.clone()
@@ -135,6 +181,8 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--mech", default="grimech30")
+    ap.add_argument("--dist", default="uneven", choices=["uneven", "mixing-layer"],
+                    help="pairs from the uneven-stiffness batch, or along 100-substep mixing-layer trajectories")
     ap.add_argument("--pairs", type=int, default=1 << 23)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=16384)
@@ -151,7 +199,10 @@ def main(argv=None):
     a = ap.parse_args(argv)
     chem = capi.FiniteChem(a.mech, "fp64")
     t0 = time.perf_counter()
-    s0, s1, d, solve_s = make_pairs(chem, a.pairs, a.seed)
+    if a.dist == "mixing-layer":
+        s0, s1, d, solve_s = make_trajectory_pairs(chem, a.pairs, a.seed)
+    else:
+        s0, s1, d, solve_s = make_pairs(chem, a.pairs, a.seed)
     t_pairs = time.perf_counter() - t0
     sur = capi.Surrogate(chem, target_mode=a.target_mode, post_mode=a.post_mode, loss_T_weight=a.loss_T_weight,
                          consist_tol_K=a.consist_tol, members=a.members)
@@ -160,10 +211,10 @@ def main(argv=None):
     t_train = time.perf_counter() - t0
     del s0, s1, d
     sur.save(a.out)
-    ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991)
+    ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991, dist=a.dist)
     if a.cells_out:
         np.savez_compressed(a.cells_out, **cells)
-    log = {"mechanism": a.mech, "pairs": a.pairs, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
+    log = {"mechanism": a.mech, "dist": a.dist, "pairs": a.pairs, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
            "target_mode": a.target_mode, "post_mode": a.post_mode, "loss_T_weight": a.loss_T_weight,
            "members": a.members,
            "consist_tol_K": a.consist_tol,
