@@ -20,7 +20,8 @@
 namespace tng {
 
 constexpr int kInferRows = 128;
-constexpr int kInferThreads = 128;
+constexpr int kInferThreads = 256;  // 8 warps: two per TMEM lane quarter
+constexpr int kInferMaxBias = 8 * 256 + 256;  // biases of every layer staged in shared memory
 constexpr int kWChunkK = 32;  // K width of one streamed weight chunk
 constexpr int kMaxLayers = 9;
 
@@ -168,6 +169,12 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   // bars[0..1]: stage full, bars[2..3]: stage free, bars[4]: layer done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 6);
   const int tid = threadIdx.x, warp = tid >> 5;
+  __shared__ float s_bias[kInferMaxBias];
+  __shared__ double s_rho[kInferRows], s_T[kInferRows];
+  {
+    const int nb = a.b_off[a.nlin - 1] + a.out_pad;
+    for (int i = tid; i < nb && i < kInferMaxBias; i += kInferThreads) s_bias[i] = a.bias[i];
+  }
   if (tid == 0) {
     for (int i = 0; i < 5; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -205,19 +212,29 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   };
   const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
   for (int tile = blockIdx.x; tile < ntiles && !err; tile += gridDim.x) {
-    // ---- 1. features of the tile's cells into A (K = in_pad)
+    // ---- 1. features of the tile's cells into A (K = in_pad): thread t serves row t % 128 and
+    // one half of the 8-wide input groups; density and temperature are formed once per row
     {
-      const int cell = tile * kInferRows + tid;
+      const int row = tid & (kInferRows - 1), part = tid >> 7;
+      const int cell = tile * kInferRows + row;
       const bool live = cell < a.ncells;
-      double rho = 1.0, T = 0.0, dt = 0.0;
-      if (live) {
-        rho = 0.0;
+      if (part == 0) {
+        double rho = 1.0, T = 0.0;
+        if (live) {
+          rho = 0.0;
 #pragma unroll 4
-        for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
-        T = a.state[(long long)a.ns * a.ld + cell] / rho;
-        dt = a.dts ? a.dts[cell] : a.dt_scalar;
+          for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
+          T = a.state[(long long)a.ns * a.ld + cell] / rho;
+        }
+        s_rho[row] = rho;
+        s_T[row] = T;
       }
-      for (int k8 = 0; k8 < a.in_pad; k8 += 8) {
+      __syncthreads();
+      const double rho = s_rho[row], T = s_T[row];
+      const double dt = live ? (a.dts ? a.dts[cell] : a.dt_scalar) : 0.0;
+      const int ng = a.in_pad / 8, g0 = part == 0 ? 0 : (ng + 1) / 2, g1 = part == 0 ? (ng + 1) / 2 : ng;
+      for (int g = g0; g < g1; ++g) {
+        const int k8 = 8 * g;
         float f[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -235,7 +252,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         v.y = *reinterpret_cast<uint32_t*>(&p1);
         v.z = *reinterpret_cast<uint32_t*>(&p2);
         v.w = *reinterpret_cast<uint32_t*>(&p3);
-        *reinterpret_cast<uint4*>(sA + canon_off(tid, k8, a.in_pad)) = v;
+        *reinterpret_cast<uint4*>(sA + canon_off(row, k8, a.in_pad)) = v;
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -289,25 +306,27 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
           pre = 1;
         }
       }
-      const float* bl = a.bias + a.b_off[l];
-      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+      // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
+      const float* bl = s_bias + a.b_off[l];
+      const int row = (warp & 3) * 32 + (tid & 31);
+      const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
       const bool last = l == a.nlin - 1;
-      const int cell = tile * kInferRows + tid;
-      for (int c0 = 0; c0 < N; c0 += 32) {
+      const int cell = tile * kInferRows + row;
+      for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 64) {
         float v[32];
         tmem_ld32(trow + (uint32_t)c0, v);
         if (last) {
           if (cell < a.ncells) {
             float* o = a.out + (long long)cell * a.out_pad + c0;
             const int nc = min(32, N - c0);
-            for (int i = 0; i < nc; ++i) o[i] = v[i] + __ldg(bl + c0 + i);
+            for (int i = 0; i < nc; ++i) o[i] = v[i] + bl[c0 + i];
           }
         } else {
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             float x[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) x[i] = gelu_fast(v[q * 8 + i] + __ldg(bl + c0 + q * 8 + i));
+            for (int i = 0; i < 8; ++i) x[i] = gelu_fast(v[q * 8 + i] + bl[c0 + q * 8 + i]);
             __nv_bfloat162 p0 = __floats2bfloat162_rn(x[0], x[1]);
             __nv_bfloat162 p1 = __floats2bfloat162_rn(x[2], x[3]);
             __nv_bfloat162 p2 = __floats2bfloat162_rn(x[4], x[5]);
@@ -317,7 +336,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
             u.y = *reinterpret_cast<uint32_t*>(&p1);
             u.z = *reinterpret_cast<uint32_t*>(&p2);
             u.w = *reinterpret_cast<uint32_t*>(&p3);
-            *reinterpret_cast<uint4*>(sA + canon_off(tid, c0 + q * 8, a.hidden)) = u;
+            *reinterpret_cast<uint4*>(sA + canon_off(row, c0 + q * 8, a.hidden)) = u;
           }
         }
       }

@@ -153,69 +153,104 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 }
 
 // prediction -> state with conservation; fallback cells keep their state and are listed
-// Smallest change of dY in the metric sum dY'^2/D_k that satisfies the linear constraints
-// A dY = b (rows: the nel element rows of E, then optionally one enthalpy row), by the normal
-// equations (Cholesky). Species driven below zero are pinned at zero (dY = -Y0, weight 0) and
-// the projection repeated over the rest (an active set), so clipping keeps the constraints.
-// Returns false when the constraints cannot be met (no free carrier of some constraint).
-__device__ bool project(const SurPost& a, const double* Y0, double* dY, double* D, const double* hrow, double hrhs) {
-  const int nc = a.nel + (hrow ? 1 : 0);
-  auto A = [&](int e, int k) { return e < a.nel ? a.E[e * a.ns + k] : hrow[k]; };
+constexpr int kPostNs = 48;  // species of a cell held by the post-processing thread
+
+// Column k of the constraint matrix: the nel element rows (atoms per kg, a_ek / W_k), then, when
+// NC > nel, the enthalpy row h_k(Th) * hsc.
+template <int NC>
+__device__ __forceinline__ void constraint_col(const SurPost& a, int k, double Th, double hsc, double (&c)[NC]) {
+#pragma unroll
+  for (int e = 0; e < NC; ++e) {
+    if (e < a.nel) {
+      c[e] = a.E[e * a.ns + k];
+    } else {
+      double hk, cpk;
+      nasa(a.th, a.tmid, k, Th, &hk, &cpk);
+      c[e] = hk * hsc;
+    }
+  }
+}
+
+// Smallest change of dY in the metric sum dY'^2/D_k that satisfies the NC linear constraints
+// A dY = b (b = 0 for the element rows, hrhs for the enthalpy row), by the normal equations
+// G = A D A^T, G lam = A dY - b (Cholesky; NC is a compile-time count, so G and its factor stay
+// in registers). Species driven below zero are pinned at zero (dY = -Y0, weight 0) and the
+// projection repeated over the rest (an active set), so clipping keeps the constraints. A
+// constraint whose carriers are all pinned or absent (G_ee = 0) holds already when its residual
+// is zero and is then left out; otherwise, or when the active set does not settle, the cell is
+// rejected (returns false).
+template <int NC>
+__device__ bool project_t(const SurPost& a, const double* Y0, double* dY, double* D, double Th, double hsc,
+                          double hrhs) {
   for (int pass = 0; pass < 8; ++pass) {
-    double G[kMaxEl + 1][kMaxEl + 1], r[kMaxEl + 1], scale[kMaxEl + 1];
-    for (int e = 0; e < nc; ++e) {
+    double G[NC][NC], r[NC], sc[NC];
+#pragma unroll
+    for (int e = 0; e < NC; ++e) {
       r[e] = e < a.nel ? 0.0 : -hrhs;
-      scale[e] = e < a.nel ? 0.0 : fabs(hrhs);
-      for (int k = 0; k < a.ns; ++k) {
-        r[e] += A(e, k) * dY[k];
-        scale[e] += fabs(A(e, k)) * (Y0[k] + fabs(dY[k]));
-      }
-      for (int g = 0; g <= e; ++g) {
-        double sg = 0.0;
-        for (int k = 0; k < a.ns; ++k) sg += A(e, k) * D[k] * A(g, k);
-        G[e][g] = G[g][e] = sg;
+      sc[e] = e < a.nel ? 0.0 : fabs(hrhs);
+#pragma unroll
+      for (int g = 0; g < NC; ++g) G[e][g] = 0.0;
+    }
+    for (int k = 0; k < a.ns; ++k) {
+      double c[NC];
+      constraint_col<NC>(a, k, Th, hsc, c);
+#pragma unroll
+      for (int e = 0; e < NC; ++e) {
+        r[e] = fma(c[e], dY[k], r[e]);
+        sc[e] += fabs(c[e]) * (Y0[k] + fabs(dY[k]));
+        const double cd = c[e] * D[k];
+#pragma unroll
+        for (int g = 0; g <= e; ++g) G[e][g] = fma(cd, c[g], G[e][g]);
       }
     }
-    // A constraint whose carriers are all pinned (or absent) has G_ee = 0 exactly: it holds
-    // already when its residual is zero (e.g. an element no species of the cell carries), and
-    // cannot be met otherwise. It leaves the system; the others are solved without it.
-    bool act[kMaxEl + 1];
-    for (int e = 0; e < nc; ++e) {
+    bool act[NC];
+#pragma unroll
+    for (int e = 0; e < NC; ++e) {
       act[e] = G[e][e] > 0.0;
-      if (!act[e] && !(fabs(r[e]) <= 1e-13 * scale[e] + 1e-300)) return false;
+      if (!act[e] && !(fabs(r[e]) <= 1e-13 * sc[e] + 1e-300)) return false;
     }
-    double Lc[kMaxEl + 1][kMaxEl + 1];
-    for (int i = 0; i < nc; ++i)
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+#pragma unroll
       for (int j = 0; j <= i; ++j) {
         if (!act[i] || !act[j]) {
-          Lc[i][j] = (i == j) ? 1.0 : 0.0;
+          G[i][j] = (i == j) ? 1.0 : 0.0;
           continue;
         }
         double sg = G[i][j];
-        for (int q = 0; q < j; ++q) sg -= Lc[i][q] * Lc[j][q];
+#pragma unroll
+        for (int q = 0; q < j; ++q) sg -= G[i][q] * G[j][q];
         if (i == j) {
           if (!(sg > 1e-14 * G[i][i])) return false;  // dependent constraints
-          Lc[i][i] = sqrt(sg);
+          G[i][i] = sqrt(sg);
         } else {
-          Lc[i][j] = sg / Lc[j][j];
+          G[i][j] = sg / G[j][j];
         }
       }
-    double lam[kMaxEl + 1];
-    for (int i = 0; i < nc; ++i) {
-      double sg = act[i] ? r[i] : 0.0;
-      for (int q = 0; q < i; ++q) sg -= Lc[i][q] * lam[q];
-      lam[i] = sg / Lc[i][i];
     }
-    for (int i = nc - 1; i >= 0; --i) {
+    double lam[NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) {
+      double sg = act[i] ? r[i] : 0.0;
+#pragma unroll
+      for (int q = 0; q < i; ++q) sg -= G[i][q] * lam[q];
+      lam[i] = sg / G[i][i];
+    }
+#pragma unroll
+    for (int i = NC - 1; i >= 0; --i) {
       double sg = lam[i];
-      for (int q = i + 1; q < nc; ++q) sg -= Lc[q][i] * lam[q];
-      lam[i] = sg / Lc[i][i];
+#pragma unroll
+      for (int q = i + 1; q < NC; ++q) sg -= G[q][i] * lam[q];
+      lam[i] = sg / G[i][i];
     }
     bool pinned = false;
     for (int k = 0; k < a.ns; ++k) {
       if (D[k] == 0.0) continue;
+      double c[NC];
+      constraint_col<NC>(a, k, Th, hsc, c);
       double corr = 0.0;
-      for (int e = 0; e < nc; ++e) corr += A(e, k) * lam[e];
+#pragma unroll
+      for (int e = 0; e < NC; ++e) corr = fma(c[e], lam[e], corr);
       dY[k] -= D[k] * corr;
       if (Y0[k] + dY[k] < 0.0) {
         dY[k] = -Y0[k];
@@ -228,15 +263,37 @@ __device__ bool project(const SurPost& a, const double* Y0, double* dY, double* 
   return false;  // still pinning species after eight passes: leave the cell to the implicit solve
 }
 
-// temperature with sum Y_k h_k(T) = h0 (Newton from T)
-__device__ double enthalpy_T(const SurPost& a, const double* Y, double h0, double T) {
+// the projection for the run-time constraint count nc = nel (+1 with the enthalpy row)
+__device__ bool project(const SurPost& a, int nc, const double* Y0, double* dY, double* D, double Th, double hsc,
+                        double hrhs) {
+  switch (nc) {
+    case 1: return project_t<1>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 2: return project_t<2>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 3: return project_t<3>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 4: return project_t<4>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 5: return project_t<5>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 6: return project_t<6>(a, Y0, dY, D, Th, hsc, hrhs);
+    case 7: return project_t<7>(a, Y0, dY, D, Th, hsc, hrhs);
+    default: return project_t<8>(a, Y0, dY, D, Th, hsc, hrhs);
+  }
+}
+
+// mass fractions after the projection: max(Y0 + dY, 0) renormalised to sum 1
+__device__ __forceinline__ double y_new(const double* Y0, const double* dY, int k, double inv_sum) {
+  return fmax(Y0[k] + dY[k], 0.0) * inv_sum;
+}
+
+// temperature with sum Y_k h_k(T) = h0 (Newton from T), Y = y_new(...)
+__device__ double enthalpy_T(const SurPost& a, const double* Y0, const double* dY, double inv_sum, double h0,
+                             double T) {
   for (int it = 0; it < 12; ++it) {
     double hh = 0.0, cp = 0.0;
     for (int k = 0; k < a.ns; ++k) {
       double hk, cpk;
       nasa(a.th, a.tmid, k, T, &hk, &cpk);
-      hh += Y[k] * hk;
-      cp += Y[k] * cpk;
+      const double y = y_new(Y0, dY, k, inv_sum);
+      hh = fma(y, hk, hh);
+      cp = fma(y, cpk, cp);
     }
     const double step = (hh - h0) / cp;
     T -= step;
@@ -245,18 +302,20 @@ __device__ double enthalpy_T(const SurPost& a, const double* Y, double h0, doubl
   return T;
 }
 
-__global__ void k_sur_post(const SurPost a) {
+// prediction -> state with conservation; fallback cells keep their state and are listed
+__global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
   for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < a.ncells; cell += gridDim.x * blockDim.x) {
     const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
-    float f[2 * kMaxNs + 2];
-    double rho, T0;
-    raw_features(a.state, a.ld, cell, a.ns, a.bath, a.logp, dt, f, &rho, &T0);
+    double rho = 0.0;
+    for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
+    const double T0 = a.state[(long long)a.ns * a.ld + cell] / rho;
     int reason = 0;
     for (int i = 0; i < a.n_in && !reason; ++i) {
+      const float f = sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, rho, T0, a.logp, dt);
       const float span = a.fmax[i] - a.fmin[i];
-      if (f[i] < a.fmin[i] - a.margin * span || f[i] > a.fmax[i] + a.margin * span) reason = 1;
+      if (f < a.fmin[i] - a.margin * span || f > a.fmax[i] + a.margin * span) reason = 1;
     }
-    double Y0[kMaxNs], dY[kMaxNs], D[kMaxNs];
+    double Y0[kPostNs], dY[kPostNs], D[kPostNs];
     // the ensemble: mean prediction, and the spread of the members as an error indicator
     const float* o = a.out + (size_t)cell * a.out_pad;
     double rT = 0.0, tlo = 1e300, thi = -1e300, sY = 0.0;
@@ -267,7 +326,7 @@ __global__ void k_sur_post(const SurPost a) {
     }
     const double Tnet = fmin(fmax(T0 * (1.0 + rT / a.members), 200.0), 6000.0);
     const double sT = T0 * (thi - tlo);
-    double neg = 0.0;  // negative mass fraction the network predicted (clip test)
+    double neg = 0.0, h0 = 0.0;  // negative mass fraction the network predicted (clip test)
     for (int k = 0; k < a.ns; ++k) {
       Y0[k] = a.state[(long long)k * a.ld + cell] / rho;
       double m = 0.0, lo = 1e300, hi = -1e300;
@@ -280,45 +339,33 @@ __global__ void k_sur_post(const SurPost a) {
       sY = fmax(sY, hi - lo);
       D[k] = fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12;
       if (Y0[k] + dY[k] < 0.0) neg -= Y0[k] + dY[k];
-    }
-    double h0 = 0.0;
-    for (int k = 0; k < a.ns; ++k) {
       double hk, cpk;
       nasa(a.th, a.tmid, k, T0, &hk, &cpk);
-      h0 += Y0[k] * hk;
+      h0 = fma(Y0[k], hk, h0);
     }
     // element conservation, then the temperature the conserved Y implies
-    bool ok = project(a, Y0, dY, D, nullptr, 0.0);
-    double Y1[kMaxNs], sum = 0.0;
-    for (int k = 0; k < a.ns; ++k) {
-      Y1[k] = fmax(Y0[k] + dY[k], 0.0);
-      sum += Y1[k];
-    }
-    for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
-    double T1 = enthalpy_T(a, Y1, h0, Tnet);
+    bool ok = project(a, a.nel, Y0, dY, D, 0.0, 0.0, 0.0);
+    double sum = 0.0;
+    for (int k = 0; k < a.ns; ++k) sum += fmax(Y0[k] + dY[k], 0.0);
+    double inv_sum = 1.0 / sum;
+    double T1 = enthalpy_T(a, Y0, dY, inv_sum, h0, Tnet);
     const double ind = fabs(T1 - Tnet);
     if (ok && a.post_mode == 1) {
-      // keep the network's temperature: move Y (elements held) until h(Y, Tnet) = h0
-      double hrow[kMaxNs], cpm = 0.0, hy = 0.0;
+      // keep the network's temperature: move Y (elements held) until h(Y, Tnet) = h0; the
+      // enthalpy row is scaled by 1 / (cp T)
+      double cpm = 0.0, hy = 0.0;
       for (int k = 0; k < a.ns; ++k) {
         double hk, cpk;
         nasa(a.th, a.tmid, k, Tnet, &hk, &cpk);
-        hrow[k] = hk;
-        cpm += Y1[k] * cpk;
+        cpm = fma(y_new(Y0, dY, k, inv_sum), cpk, cpm);
+        hy = fma(hk, Y0[k], hy);
       }
-      const double sc = 1.0 / (cpm * Tnet);  // enthalpy row in units of cp*T
-      for (int k = 0; k < a.ns; ++k) {
-        hrow[k] *= sc;
-        hy += hrow[k] * Y0[k];
-      }
-      ok = project(a, Y0, dY, D, hrow, h0 * sc - hy);
+      const double hsc = 1.0 / (cpm * Tnet);
+      ok = project(a, a.nel + 1, Y0, dY, D, Tnet, hsc, (h0 - hy) * hsc);
       sum = 0.0;
-      for (int k = 0; k < a.ns; ++k) {
-        Y1[k] = fmax(Y0[k] + dY[k], 0.0);
-        sum += Y1[k];
-      }
-      for (int k = 0; k < a.ns; ++k) Y1[k] /= sum;
-      T1 = enthalpy_T(a, Y1, h0, Tnet);  // one correction for the renormalisation
+      for (int k = 0; k < a.ns; ++k) sum += fmax(Y0[k] + dY[k], 0.0);
+      inv_sum = 1.0 / sum;
+      T1 = enthalpy_T(a, Y0, dY, inv_sum, h0, Tnet);  // one correction for the renormalisation
     }
     if (!reason && !(ind <= a.consist_tol)) reason = 2;
     if (!reason && !(neg <= a.clip_tol)) reason = 3;
@@ -331,14 +378,14 @@ __global__ void k_sur_post(const SurPost a) {
       a.ind_out[3 * (size_t)cell + 2] = sY;
     }
     if (a.out_state) {
-      for (int k = 0; k < a.ns; ++k) a.out_state[(long long)k * a.ld_out + cell] = rho * Y1[k];
+      for (int k = 0; k < a.ns; ++k) a.out_state[(long long)k * a.ld_out + cell] = rho * y_new(Y0, dY, k, inv_sum);
       a.out_state[(long long)a.ns * a.ld_out + cell] = rho * T1;
     } else if (reason) {
       const int slot = atomicAdd(a.fb_count, 1);
       a.fb_list[slot] = cell;
       atomicAdd(&a.cnt[reason], 1ULL);
     } else {
-      for (int k = 0; k < a.ns; ++k) a.state[(long long)k * a.ld + cell] = rho * Y1[k];
+      for (int k = 0; k < a.ns; ++k) a.state[(long long)k * a.ld + cell] = rho * y_new(Y0, dY, k, inv_sum);
       a.state[(long long)a.ns * a.ld + cell] = rho * T1;
       atomicAdd(&a.cnt[0], 1ULL);
     }
@@ -542,7 +589,9 @@ int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogat
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: hidden width must be 256 (the tensor-core tile), 1..%d layers",
                      kMaxLayers - 1);
   const MechOps* o = h->ops;
-  if (o->ns + 3 > kMaxNs || o->nelem > kMaxEl) return set_error(TNG_ERR_ARG, "tng_surrogate_create: mechanism too large");
+  if (o->ns > kPostNs || 2 * o->ns + 1 > 2 * kMaxNs || o->nelem > kMaxEl)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_create: mechanism too large (at most %d species, %d elements)",
+                     kPostNs, kMaxEl);
   DeviceGuard g(h->cfg.device);
   tng_surrogate* s = new tng_surrogate();
   s->h = h;
