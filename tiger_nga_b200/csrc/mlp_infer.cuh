@@ -171,9 +171,11 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   const int tid = threadIdx.x, warp = tid >> 5;
   __shared__ float s_bias[kInferMaxBias];
   __shared__ double s_rho[kInferRows], s_T[kInferRows];
-  {
-    const int nb = a.b_off[a.nlin - 1] + a.out_pad;
-    for (int i = tid; i < nb && i < kInferMaxBias; i += kInferThreads) s_bias[i] = a.bias[i];
+  // biases, compact: layer l at s_bias[l * hidden] (hidden entries; out_pad for the last layer);
+  // b_off[l] is the offset of layer l's bias inside the parameter array
+  for (int l = 0; l < a.nlin; ++l) {
+    const int nl = l == a.nlin - 1 ? a.out_pad : a.hidden;
+    for (int i = tid; i < nl; i += kInferThreads) s_bias[l * a.hidden + i] = a.bias[a.b_off[l] + i];
   }
   if (tid == 0) {
     for (int i = 0; i < 5; ++i) mbar_init(&bars[i], 1);
@@ -307,7 +309,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         }
       }
       // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
-      const float* bl = s_bias + a.b_off[l];
+      const float* bl = s_bias + l * a.hidden;
       const int row = (warp & 3) * 32 + (tid & 31);
       const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
       const bool last = l == a.nlin - 1;

@@ -509,6 +509,8 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double*
   ia.bias = s->member(member).params;
   ia.out = out;
   ia.error = err;
+  if ((s->m.nlin - 1) * s->m.hidden + s->m.out_pad > kInferMaxBias)
+    return set_error(TNG_ERR_ARG, "inference: the biases do not fit the kernel's shared-memory stage");
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
   if (e != cudaSuccess) return cuda_error(e, "inference shared memory");
   const int grid = (int)std::min<int64_t>(2 * h->sm_count, (ncells + kInferRows - 1) / kInferRows);
@@ -589,7 +591,7 @@ int tng_surrogate_create(tng_chem* h, const tng_surrogate_cfg* cfg, tng_surrogat
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: hidden width must be 256 (the tensor-core tile), 1..%d layers",
                      kMaxLayers - 1);
   const MechOps* o = h->ops;
-  if (o->ns > kPostNs || 2 * o->ns + 1 > 2 * kMaxNs || o->nelem > kMaxEl)
+  if (o->ns > kPostNs || 2 * o->ns + 1 > 2 * kMaxNs || o->nelem + 1 > kMaxEl)
     return set_error(TNG_ERR_ARG, "tng_surrogate_create: mechanism too large (at most %d species, %d elements)",
                      kPostNs, kMaxEl);
   DeviceGuard g(h->cfg.device);
