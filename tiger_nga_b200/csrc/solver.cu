@@ -90,6 +90,8 @@ static int ensure_tables(tng_chem* h) {
   }
   const MechOps* o = h->ops;
   const SvLayout& L = *o->sv_layout;
+  if (L.size[SZ_NV] > 64)  // the warp holds a cell's state two entries per lane
+    return set_error(TNG_ERR_ARG, "implicit solver: at most 63 species (%s has %d)", o->name, L.size[SZ_NS]);
   cudaError_t e;
   if ((e = cudaMalloc(&s->d_int, sizeof(int) * (L.nhi + L.nci))) != cudaSuccess) return cuda_error(e, "solver tables");
   if ((e = cudaMalloc(&s->d_dbl, sizeof(double) * L.nhd)) != cudaSuccess) return cuda_error(e, "solver tables");
