@@ -396,23 +396,11 @@ __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const
     const int* gi = t.c(CI_G_I);
     const int* gm = t.c(CI_G_M);
     const double* eff = t.d(HD_EFF);
-    // the pairs are sorted by row i: accumulate a row's contributions, one read-modify-write
-    for (int j = lane; j < ns; j += 32) {
-      int cur = -1;
-      double acc = 0.0;
+    for (int j = lane; j < ns; j += 32)
       for (int g = 0; g < ng; ++g) {
         const double v = w.G[g];
-        if (v == 0.0) continue;
-        const int i = gi[g];
-        if (i != cur) {
-          if (cur >= 0) w.mat[cur * rs + j] += acc;
-          cur = i;
-          acc = 0.0;
-        }
-        acc = fma(v, eff[gm[g] * ns + j], acc);
+        if (v != 0.0) w.mat[gi[g] * rs + j] = fma(v, eff[gm[g] * ns + j], w.mat[gi[g] * rs + j]);
       }
-      if (cur >= 0) w.mat[cur * rs + j] += acc;
-    }
   }
   __syncwarp();
   // temperature column: forward difference (one right-hand side)
@@ -513,21 +501,9 @@ __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int
     }
     for (int i = k + 1 + lane; i < n; i += 32) a[i * rs + k] = a[i * rs + k] / d;
     __syncwarp();
-    // rank-1 update of the trailing block, lanes as a 4 x 8 grid: the pivot-row values of the
-    // lane's columns are read once, and the up to 8 elements of a row are independent (fixed
-    // offsets from one row pointer), so their loads overlap
-    {
-      const int j0 = k + 1 + lc;
-      double prow[8];
-#pragma unroll
-      for (int m = 0; m < 8; ++m) prow[m] = j0 + 8 * m < n ? a[k * rs + j0 + 8 * m] : 0.0;
-      for (int i = k + 1 + lr; i < n; i += 4) {
-        double* row = a + i * rs;
-        const double l = row[k];
-#pragma unroll
-        for (int m = 0; m < 8; ++m)
-          if (j0 + 8 * m < n) row[j0 + 8 * m] = fma(-l, prow[m], row[j0 + 8 * m]);
-      }
+    for (int i = k + 1 + lr; i < n; i += 4) {
+      const double l = a[i * rs + k];
+      for (int j = k + 1 + lc; j < n; j += 8) a[i * rs + j] = fma(-l, a[k * rs + j], a[i * rs + j]);
     }
     __syncwarp();
   }
