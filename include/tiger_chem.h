@@ -219,8 +219,10 @@ typedef struct tng_surrogate_stats {
   int64_t judged;               /* sampled cells solved twice */
   double judge_max_rel_dT;      /* max |T_s - T_p| / T_p over the sample (surrogate vs implicit) */
   double judge_max_dY;          /* max |Y_s,k - Y_p,k| / max_k Y_p,k over the sample */
-  double ms_infer, ms_post, ms_fallback, ms_total;  /* device times */
-  tng_substep_stats fallback;   /* the implicit solve of the fallback cells */
+  double ms_infer, ms_post, ms_fallback, ms_total;  /* device times; with a judged sample, ms_fallback
+                                   covers the joint implicit solve of the fallback cells and the sample */
+  tng_substep_stats fallback;   /* the implicit solve of the fallback cells (cells: their number; the
+                                   step and iteration counts include the judged sample, solved jointly) */
   int64_t fallback_ensemble;    /* cells whose ensemble members disagreed */
 } tng_surrogate_stats;
 

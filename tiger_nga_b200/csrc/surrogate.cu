@@ -393,29 +393,57 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
 }
 
 __global__ void k_gather_cells(const double* __restrict__ src, long long ld, int nv, const int* __restrict__ idx, int m,
-                               double* __restrict__ dst, const double* __restrict__ dts, double dt,
+                               double* __restrict__ dst, long long dst_ld, const double* __restrict__ dts, double dt,
                                double* __restrict__ dts_out) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
-    for (int v = 0; v < nv; ++v) dst[(long long)v * m + j] = src[(long long)v * ld + idx[j]];
+    for (int v = 0; v < nv; ++v) dst[(long long)v * dst_ld + j] = src[(long long)v * ld + idx[j]];
     dts_out[j] = dts ? dts[idx[j]] : dt;
   }
 }
 
+// The fallback cells listed by the post-processing (count on the device) into columns J, J+1, ...
+// of the joint batch, whose first J columns hold the judged sample; n_out = J + count.
+__global__ void k_gather_list(const double* __restrict__ src, long long ld, int nv, const int* __restrict__ list,
+                              const int* __restrict__ count, int J, double* __restrict__ dst, long long dst_ld,
+                              const double* __restrict__ dts, double dt, double* __restrict__ dts_out,
+                              int* __restrict__ n_out) {
+  const int n = *count;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const int c = list[j];
+    for (int v = 0; v < nv; ++v) dst[(long long)v * dst_ld + J + j] = src[(long long)v * ld + c];
+    dts_out[J + j] = dts ? dts[c] : dt;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = J + n;
+}
+
+// the solved fallback cells back into the state
+__global__ void k_scatter_list(double* __restrict__ dst, long long ld, int nv, const int* __restrict__ list,
+                               const int* __restrict__ count, int J, const double* __restrict__ src, long long src_ld) {
+  const int n = *count;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    for (int v = 0; v < nv; ++v) dst[(long long)v * ld + list[j]] = src[(long long)v * src_ld + J + j];
+}
+
+__global__ void k_iota(int* __restrict__ a, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] = (int)i;
+}
+
 // surrogate(+fallback) result vs implicit result on the judged cells
 __global__ void k_judge(const double* __restrict__ state, long long ld, int ns, const int* __restrict__ idx, int m,
-                        const double* __restrict__ ref, double* __restrict__ out) {
+                        const double* __restrict__ ref, long long ref_ld, double* __restrict__ out) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
     const int c = idx[j];
     double rs = 0.0, rr = 0.0, ymax = 0.0;
     for (int k = 0; k < ns; ++k) {
       rs += state[(long long)k * ld + c];
-      rr += ref[(long long)k * m + j];
+      rr += ref[(long long)k * ref_ld + j];
     }
-    for (int k = 0; k < ns; ++k) ymax = fmax(ymax, ref[(long long)k * m + j] / rr);
-    const double Ts = state[(long long)ns * ld + c] / rs, Tp = ref[(long long)ns * m + j] / rr;
+    for (int k = 0; k < ns; ++k) ymax = fmax(ymax, ref[(long long)k * ref_ld + j] / rr);
+    const double Ts = state[(long long)ns * ld + c] / rs, Tp = ref[(long long)ns * ref_ld + j] / rr;
     double dy = 0.0;
     for (int k = 0; k < ns; ++k)
-      dy = fmax(dy, fabs(state[(long long)k * ld + c] / rs - ref[(long long)k * m + j] / rr));
+      dy = fmax(dy, fabs(state[(long long)k * ld + c] / rs - ref[(long long)k * ref_ld + j] / rr));
     atomic_max_pos(&out[0], fabs(Ts - Tp) / Tp);
     atomic_max_pos(&out[1], dy / ymax);
   }
@@ -444,7 +472,7 @@ struct tng_surrogate {
   double* d_E = nullptr;
   __nv_bfloat16* d_wpack[kMaxMembers] = {};
   long long w_off[kMaxLayers] = {};
-  DevBuf out, fb, cnt, judge_state, judge_dts, judge_idx, work;
+  DevBuf out, fb, cnt, judge_state, judge_dts, judge_idx, work, joint;
   cudaEvent_t ev[5] = {};
   int calls = 0;
 };
@@ -654,7 +682,8 @@ int tng_surrogate_destroy(tng_surrogate* s) {
   if (s->d_E) cudaFree(s->d_E);
   for (auto* w : s->d_wpack)
     if (w) cudaFree(w);
-  for (DevBuf* b : {&s->out, &s->fb, &s->cnt, &s->judge_state, &s->judge_dts, &s->judge_idx, &s->work}) b->release();
+  for (DevBuf* b : {&s->out, &s->fb, &s->cnt, &s->judge_state, &s->judge_dts, &s->judge_idx, &s->work, &s->joint})
+    b->release();
   for (auto& ev : s->ev)
     if (ev) cudaEventDestroy(ev);
   if (s->h) s->h->dependents--;
@@ -912,6 +941,22 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
             s->cnt.reserve(16 * sizeof(unsigned long long)) &&
             (J == 0 || (s->judge_state.reserve((size_t)J * nv * sizeof(double)) &&
                         s->judge_dts.reserve((size_t)J * sizeof(double)) && s->judge_idx.reserve(J * sizeof(int))));
+  // With statistics requested the judged sample and the fallback cells are solved in ONE launch of
+  // the implicit solver (a joint batch: the sample in columns 0..J-1, the fallback cells after
+  // it), so the two tails overlap instead of adding up.
+  const bool joint = J > 0 && stats;
+  const int64_t ldc = J + ncells;
+  double* comp = nullptr;
+  double* comp_dts = nullptr;
+  int* comp_iota = nullptr;
+  int* comp_n = nullptr;
+  if (ok && joint) {
+    ok = s->joint.reserve((size_t)ldc * (nv + 1) * sizeof(double) + (size_t)(ldc + 4) * sizeof(int));
+    comp = (double*)s->joint.ptr;
+    comp_dts = comp + (size_t)nv * ldc;
+    comp_iota = (int*)(comp_dts + ldc);
+    comp_n = comp_iota + ldc;
+  }
   if (!ok) return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: scratch allocation failed");
   int rc = solver_prepare(h);  // the solver tables (thermo for the enthalpy balance) on the device
   if (rc) return rc;
@@ -927,9 +972,13 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
     const int64_t off = (int64_t)(s->calls * 7919) % stride;
     for (int j = 0; j < J; ++j) idx[j] = (int)((off + (int64_t)j * stride) % ncells);
     cudaMemcpyAsync(s->judge_idx.ptr, idx.data(), sizeof(int) * J, cudaMemcpyHostToDevice, st);
-    k_gather_cells<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, nv, (const int*)s->judge_idx.ptr, J,
-                                                    (double*)s->judge_state.ptr, ddts, dt,
-                                                    (double*)s->judge_dts.ptr);
+    if (joint)
+      k_gather_cells<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, nv, (const int*)s->judge_idx.ptr, J, comp, ldc,
+                                                      ddts, dt, comp_dts);
+    else
+      k_gather_cells<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, nv, (const int*)s->judge_idx.ptr, J,
+                                                      (double*)s->judge_state.ptr, J, ddts, dt,
+                                                      (double*)s->judge_dts.ptr);
   }
   s->calls++;
   // inference on the tensor cores
@@ -947,19 +996,25 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   k_sur_post<<<(int)std::min<int64_t>(4096, (ncells + 127) / 128), 128, 0, st>>>(pa);
   cudaEventRecord(s->ev[2], st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "surrogate kernels");
-  // implicit fallback on the listed cells, in place
   tng_substep_stats fst;
-  rc = substep_run(h, dstate, ncells, dld, ddts, dt, p, TNG_DEVICE_PTRS, fb_list, fb_count, nullptr, nullptr, nullptr,
-                   stats ? &fst : nullptr);
-  if (rc) return rc;
-  cudaEventRecord(s->ev[3], st);
-  // judge: the implicit solve of the sample, compared with the surrogate(+fallback) result
-  if (J > 0 && stats) {
-    rc = substep_run(h, (double*)s->judge_state.ptr, J, J, (const double*)s->judge_dts.ptr, 0.0, p, TNG_DEVICE_PTRS,
-                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+  if (joint) {
+    // fallback cells and the judged sample in one implicit solve, then the fallback cells back
+    k_gather_list<<<1184, 128, 0, st>>>(dstate, dld, nv, fb_list, fb_count, J, comp, ldc, ddts, dt, comp_dts, comp_n);
+    k_iota<<<(int)std::min<int64_t>(4096, (ldc + 255) / 256), 256, 0, st>>>(comp_iota, ldc);
+    rc = substep_run(h, comp, ldc, ldc, comp_dts, 0.0, p, TNG_DEVICE_PTRS, comp_iota, comp_n, nullptr, nullptr, nullptr,
+                     &fst);
     if (rc) return rc;
-    k_judge<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, s->ns, (const int*)s->judge_idx.ptr, J,
-                                             (const double*)s->judge_state.ptr, (double*)(cnt + 10));
+    k_scatter_list<<<1184, 128, 0, st>>>(dstate, dld, nv, fb_list, fb_count, J, comp, ldc);
+    cudaEventRecord(s->ev[3], st);
+    // judge: the implicit solve of the sample against the surrogate(+fallback) result
+    k_judge<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, s->ns, (const int*)s->judge_idx.ptr, J, comp, ldc,
+                                             (double*)(cnt + 10));
+  } else {
+    // implicit fallback on the listed cells, in place
+    rc = substep_run(h, dstate, ncells, dld, ddts, dt, p, TNG_DEVICE_PTRS, fb_list, fb_count, nullptr, nullptr,
+                     nullptr, stats ? &fst : nullptr);
+    if (rc) return rc;
+    cudaEventRecord(s->ev[3], st);
   }
   cudaEventRecord(s->ev[4], st);
   if (flags == TNG_HOST_PTRS)
