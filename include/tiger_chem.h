@@ -98,6 +98,27 @@ int tng_prodrates_batch_rates(tng_chem* h, const double* sol, double* rhs, doubl
 /* Wait for the handle's stream; returns the first asynchronous error, if any. */
 int tng_chem_sync(tng_chem* h);
 
+/* ---- autotuning (no counterpart in the reference: its kernels are the compiler's) ----------- */
+#define TNG_TUNE_MAX 24
+typedef struct tng_tune_result {
+  int n, best;           /* candidates timed; index of the kept one */
+  int a[TNG_TUNE_MAX];   /* rates: kernel variant; substep: cells (warps) per block */
+  int b[TNG_TUNE_MAX];   /* rates: block size; substep: pass budget (0 = one pass, no recompaction) */
+  double ms[TNG_TUNE_MAX];
+} tng_tune_result;
+/* Set the tunable launch parameters of a handle (as tng_cfg: rate_variant -1..2, block_size 0 =
+ * default, solver_warps 0/2/4/8, pass_budget >= 0). */
+int tng_chem_set_tuning(tng_chem* h, int rate_variant, int block_size, int solver_warps, int pass_budget);
+/* Time the rate kernel's variants x block sizes on the caller's cells (device pointers) and keep
+ * the fastest in the handle. */
+int tng_rates_autotune(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p,
+                       tng_tune_result* out);
+/* Time the implicit solver's cells-per-block x pass-budget (recompaction) choices on a strided
+ * sample of at most `sample` of the caller's cells (device pointers; 0 = 65536) and keep the
+ * fastest. Results per cell do not depend on the choice. */
+int tng_substep_autotune(tng_chem* h, const double* state, int64_t ncells, int64_t ld, const double* dts, double dt,
+                         double p, int64_t sample, tng_tune_result* out);
+
 /* Statistics of one implicit substep. */
 typedef struct tng_substep_stats {
   int64_t cells;         /* cells integrated */

@@ -68,6 +68,14 @@ class SurrogateCfg(ctypes.Structure):
                 ("ens_tol_Y", ctypes.c_float), ("reserved", ctypes.c_int * 2)]
 
 
+class TuneResult(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("best", ctypes.c_int), ("a", ctypes.c_int * 24), ("b", ctypes.c_int * 24),
+                ("ms", ctypes.c_double * 24)]
+
+    def as_list(self):
+        return [(self.a[i], self.b[i], self.ms[i]) for i in range(self.n)]
+
+
 class Extent(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in ("imino", "imaxo", "jmino", "jmaxo", "kmino", "kmaxo", "imin", "imax",
                                             "jmin", "jmax", "kmin", "kmax", "nscalar", "isc_sc", "isc_T",
@@ -107,6 +115,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
         "tng_substep_batch_static": (I, [V, V, L, L, V, D, D, ctypes.POINTER(I)]),
+        "tng_chem_set_tuning": (I, [V, I, I, I, I]),
+        "tng_rates_autotune": (I, [V, V, L, L, D, ctypes.POINTER(TuneResult)]),
+        "tng_substep_autotune": (I, [V, V, L, L, V, D, D, L, ctypes.POINTER(TuneResult)]),
         "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
         "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
         "tng_mlp_destroy": (I, [V]),
@@ -183,6 +194,7 @@ class FiniteChem:
         _check(self.lib.tng_chem_create(mechanism.encode(), ctypes.byref(cfg), ctypes.byref(h)), "tng_chem_create")
         self.h = h
         self.mechanism = mechanism
+        self.precision = precision
         self.device = device
         ns, nr, nm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(self.lib.tng_chem_sizes(h, ctypes.byref(ns), ctypes.byref(nr), ctypes.byref(nm)), "tng_chem_sizes")
@@ -408,6 +420,70 @@ def _substep_static(self, state, dt, p: float) -> int:
     return failed.value
 
 
+def _tuning_key(self, kind: str) -> str:
+    import torch
+
+    return f"{kind}/{self.mechanism}/{self.precision}/{torch.cuda.get_device_name()}"
+
+
+def _autotune(self, state, dt=None, p: float = 101325.0, kind: str = "substep", sample: int = 65536,
+              cache: str | None = None):
+    """Run the project's autotuner on ``state`` (a CUDA tensor of the caller's cells) and keep the
+    fastest launch configuration in the handle. kind 'rates' times the rate kernel's variants x
+    block sizes; 'substep' times the implicit solver's cells-per-block x pass budget on a sample.
+    With ``cache`` (a JSON file) a stored choice for this mechanism, precision and GPU is applied
+    without timing, and a new one is stored. Returns {"best": (a, b), "candidates": [(a, b, ms)]}."""
+    import json
+    import os
+
+    import torch
+
+    key = self._tuning_key(kind)
+    store = {}
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            store = json.load(f)
+        if key in store:
+            a, b = store[key]["best"]
+            if kind == "rates":
+                _check(self.lib.tng_chem_set_tuning(self.h, a, b, self.cfg.solver_warps, self.cfg.pass_budget),
+                       "tng_chem_set_tuning")
+                self.cfg.rate_variant, self.cfg.block_size = a, b
+            else:
+                _check(self.lib.tng_chem_set_tuning(self.h, self.cfg.rate_variant, self.cfg.block_size, a, b),
+                       "tng_chem_set_tuning")
+                self.cfg.solver_warps, self.cfg.pass_budget = a, b
+            return store[key]
+    n = state.shape[1]
+    ld = max(state.stride(0), n)
+    res = TuneResult()
+    sst = self.torch_stream()
+    sst.wait_stream(torch.cuda.current_stream(state.device))
+    if kind == "rates":
+        _check(self.lib.tng_rates_autotune(self.h, state.data_ptr(), n, ld, float(p), ctypes.byref(res)),
+               "tng_rates_autotune")
+    else:
+        dts = None
+        if dt is not None and not isinstance(dt, (float, int)):
+            dts = torch.as_tensor(dt, dtype=torch.float64, device=state.device).contiguous()
+        _check(self.lib.tng_substep_autotune(self.h, state.data_ptr(), n, ld, dts.data_ptr() if dts is not None else None,
+                                             0.0 if dts is not None else float(dt), float(p), int(sample),
+                                             ctypes.byref(res)), "tng_substep_autotune")
+    a, b = res.a[res.best], res.b[res.best]
+    if kind == "rates":
+        self.cfg.rate_variant, self.cfg.block_size = a, b
+    else:
+        self.cfg.solver_warps, self.cfg.pass_budget = a, b
+    out = {"best": (a, b), "candidates": res.as_list()}
+    if cache:
+        store[key] = out
+        with open(cache, "w") as f:
+            json.dump(store, f, indent=1)
+    return out
+
+
+FiniteChem._tuning_key = _tuning_key
+FiniteChem.autotune = _autotune
 FiniteChem.source_chemistry = _source_chemistry
 FiniteChem.substep_static = _substep_static
 FiniteChem.substep = _substep
