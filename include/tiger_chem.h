@@ -54,7 +54,9 @@ typedef struct tng_cfg {
   int solver_warps; /* cells (warps) per block of the implicit solver: 2, 4 or 8; 0 = tuned */
   int pass_budget;  /* internal steps per cell and solver pass before the cell is re-queued; 0 = no limit */
   int max_passes;   /* passes captured in the solver's CUDA graph (the last one has no budget) */
-  int reserved[4];
+  int solver_occupancy; /* solver blocks per SM targeted by its launch bounds (with 8 warps): 1, or 2
+                           (registers capped at 128, some spilled); 0 = 1 */
+  int reserved[3];
 } tng_cfg;
 
 typedef struct tng_chem tng_chem;
@@ -107,13 +109,14 @@ typedef struct tng_tune_result {
   double ms[TNG_TUNE_MAX];
 } tng_tune_result;
 /* Set the tunable launch parameters of a handle (as tng_cfg: rate_variant -1..2, block_size 0 =
- * default, solver_warps 0/2/4/8, pass_budget >= 0). */
+ * default, solver_warps 0/2/4/8, or 16 for 8 warps with solver_occupancy 2; pass_budget >= 0). */
 int tng_chem_set_tuning(tng_chem* h, int rate_variant, int block_size, int solver_warps, int pass_budget);
 /* Time the rate kernel's variants x block sizes on the caller's cells (device pointers) and keep
  * the fastest in the handle. */
 int tng_rates_autotune(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p,
                        tng_tune_result* out);
-/* Time the implicit solver's cells-per-block x pass-budget (recompaction) choices on a strided
+/* Time the implicit solver's cells-per-block (2, 4, 8, 16 = 8 at two blocks per SM) x pass-budget
+ * (recompaction) choices on a strided
  * sample of at most `sample` of the caller's cells (device pointers; 0 = 65536) and keep the
  * fastest. Results per cell do not depend on the choice. */
 int tng_substep_autotune(tng_chem* h, const double* state, int64_t ncells, int64_t ld, const double* dts, double dt,

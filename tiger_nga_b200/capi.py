@@ -32,7 +32,7 @@ class TngCfg(ctypes.Structure):
                 ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_steps", ctypes.c_int),
                 ("max_newton", ctypes.c_int), ("block_size", ctypes.c_int), ("rate_variant", ctypes.c_int),
                 ("solver_warps", ctypes.c_int), ("pass_budget", ctypes.c_int), ("max_passes", ctypes.c_int),
-                ("reserved", ctypes.c_int * 4)]
+                ("solver_occupancy", ctypes.c_int), ("reserved", ctypes.c_int * 3)]
 
 
 class SubstepStats(ctypes.Structure):  # noqa: E302
@@ -452,7 +452,8 @@ def _autotune(self, state, dt=None, p: float = 101325.0, kind: str = "substep", 
             else:
                 _check(self.lib.tng_chem_set_tuning(self.h, self.cfg.rate_variant, self.cfg.block_size, a, b),
                        "tng_chem_set_tuning")
-                self.cfg.solver_warps, self.cfg.pass_budget = a, b
+                self.cfg.solver_warps, self.cfg.solver_occupancy = (8, 2) if a == 16 else (a, 1)
+                self.cfg.pass_budget = b
             return store[key]
     n = state.shape[1]
     ld = max(state.stride(0), n)
@@ -473,7 +474,8 @@ def _autotune(self, state, dt=None, p: float = 101325.0, kind: str = "substep", 
     if kind == "rates":
         self.cfg.rate_variant, self.cfg.block_size = a, b
     else:
-        self.cfg.solver_warps, self.cfg.pass_budget = a, b
+        self.cfg.solver_warps, self.cfg.solver_occupancy = (8, 2) if a == 16 else (a, 1)
+        self.cfg.pass_budget = b
     out = {"best": (a, b), "candidates": res.as_list()}
     if cache:
         store[key] = out

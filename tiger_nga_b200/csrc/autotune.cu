@@ -41,11 +41,13 @@ using namespace tng;
 extern "C" int tng_chem_set_tuning(tng_chem* h, int rate_variant, int block_size, int solver_warps, int pass_budget) {
   if (!h) return set_error(TNG_ERR_ARG, "tng_chem_set_tuning: null handle");
   if (rate_variant < -1 || rate_variant > 2 || block_size < 0 || block_size > 1024 ||
-      !(solver_warps == 0 || solver_warps == 2 || solver_warps == 4 || solver_warps == 8) || pass_budget < 0)
+      !(solver_warps == 0 || solver_warps == 2 || solver_warps == 4 || solver_warps == 8 || solver_warps == 16) ||
+      pass_budget < 0)
     return set_error(TNG_ERR_ARG, "tng_chem_set_tuning: value out of range");
   h->cfg.rate_variant = rate_variant;
   h->cfg.block_size = block_size;
-  h->cfg.solver_warps = solver_warps;
+  h->cfg.solver_warps = solver_warps == 16 ? 8 : solver_warps;  // 16: 8 warps, two blocks per SM
+  h->cfg.solver_occupancy = solver_warps == 16 ? 2 : 1;
   h->cfg.pass_budget = pass_budget;
   return TNG_OK;
 }
@@ -115,14 +117,16 @@ extern "C" int tng_substep_autotune(tng_chem* h, const double* state, int64_t nc
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const int warps[3] = {2, 4, 8}, budgets[3] = {0, 32, 128};
+  // warps per block; 16 stands for 8 warps with launch bounds for two blocks per SM
+  const int warps[4] = {2, 4, 8, 16}, budgets[3] = {0, 32, 128};
   double best = 1e300;
   int bw = 8, bb = 0;
   const tng_cfg saved = h->cfg;
   int rc = TNG_OK;
   for (int w : warps)
     for (int b : budgets) {
-      h->cfg.solver_warps = w;
+      h->cfg.solver_warps = w == 16 ? 8 : w;
+      h->cfg.solver_occupancy = w == 16 ? 2 : 1;
       h->cfg.pass_budget = b;
       // first run builds the pass graph of this configuration; the second is timed
       for (int rep = 0; rep < 2 && !rc; ++rep) {
@@ -146,7 +150,8 @@ extern "C" int tng_substep_autotune(tng_chem* h, const double* state, int64_t nc
   h->cfg = saved;
   if (rc) return rc;
   if (e != cudaSuccess) return cuda_error(e, "tng_substep_autotune");
-  h->cfg.solver_warps = bw;
+  h->cfg.solver_warps = bw == 16 ? 8 : bw;
+  h->cfg.solver_occupancy = bw == 16 ? 2 : 1;
   h->cfg.pass_budget = bb;
   if (out) {
     for (int i = 0; i < out->n; ++i)

@@ -422,8 +422,8 @@ finish:
 __host__ __device__ inline int hot_smem_doubles(const SvLayout& L) { return (hot_smem_bytes(L) + 15) / 16 * 2; }
 
 // One block per SM of WARPS warps (the staged tables are shared by the block's warps).
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 1) k_bdf(const BdfLaunch P) {
+template <int WARPS, int MINB = 1>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_bdf(const BdfLaunch P) {
   extern __shared__ __align__(16) double smem[];
   const SvDev t = stage_tables(P.a.tab, smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

@@ -40,7 +40,7 @@ struct SubstepKey {
   const int* nlist;
   const double* dts;
   double dt, p;
-  int warps, budget, passes;
+  int warps, occ, budget, passes;
   int* nst;
   int* nni;
   int* status;
@@ -59,7 +59,7 @@ struct SolverState {
   cudaGraphExec_t graph[kGraphs] = {};
   SubstepKey key[kGraphs] = {};
   int next_slot = 0;
-  int warps = 0, blocks = 0;
+  int warps = 0, occ = 0, blocks = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -114,7 +114,9 @@ static int ensure_tables(tng_chem* h) {
 
 typedef void (*BdfKernel)(const BdfLaunch);
 
-static BdfKernel bdf_kernel(int warps) {
+// occ 2 (with 8 warps): launch bounds for two blocks per SM (registers capped at 128)
+static BdfKernel bdf_kernel(int warps, int occ = 1) {
+  if (warps == 8 && occ == 2) return k_bdf<8, 2>;
   switch (warps) {
     case 2:
       return k_bdf<2>;
@@ -129,10 +131,10 @@ static size_t block_smem(const SolverState* s, int warps) {
   return ((size_t)hot_smem_doubles(s->dev.L) + (size_t)warps * s->smem_warp) * sizeof(double);
 }
 
-static int configure_kernel(tng_chem* h, int warps, int* blocks_out) {
+static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   SolverState* s = h->solver;
   const size_t smem = block_smem(s, warps);
-  BdfKernel k = bdf_kernel(warps);
+  BdfKernel k = bdf_kernel(warps, occ);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   int per_sm = 0;
@@ -251,6 +253,7 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
   const int budget = h->cfg.pass_budget > 0 ? h->cfg.pass_budget : 0x7fffffff;
   const int passes = budget == 0x7fffffff ? 1 : std::max(2, h->cfg.max_passes > 0 ? h->cfg.max_passes : 8);
   const int warps = (h->cfg.solver_warps == 2 || h->cfg.solver_warps == 4) ? h->cfg.solver_warps : 8;
+  const int occ = (warps == 8 && h->cfg.solver_occupancy == 2) ? 2 : 1;
   const int save_stride = ((kQmax + 2) * nv + 16 + 3) & ~3;
   bool ok = s->counters.reserve(64 * sizeof(int)) && s->queue[0].reserve(ncells * sizeof(int)) &&
             s->queue[1].reserve(ncells * sizeof(int)) && s->resume.reserve(ncells * sizeof(int)) &&
@@ -259,15 +262,16 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
             s->stats.reserve(32 * sizeof(unsigned long long));
   if (ok && passes > 1) ok = s->save.reserve((size_t)ncells * save_stride * sizeof(double));
   if (!ok) return set_error(TNG_ERR_CUDA, "tng_substep_batch: scratch allocation for %lld cells failed", (long long)ncells);
-  if (s->warps != warps) {
-    if ((rc = configure_kernel(h, warps, &s->blocks))) return rc;
+  if (s->warps != warps || s->occ != occ) {
+    if ((rc = configure_kernel(h, warps, occ, &s->blocks))) return rc;
     s->warps = warps;
+    s->occ = occ;
   }
   int* nst = cell_nst ? cell_nst : (int*)s->nst.ptr;
   int* nni = cell_nni ? cell_nni : (int*)s->nni.ptr;
   int* sts = cell_status ? cell_status : (int*)s->status.ptr;
   if (list && flags != TNG_DEVICE_PTRS) return set_error(TNG_ERR_ARG, "substep: cell lists need device pointers");
-  SubstepKey key{dstate, ncells, dld, list, nlist, ddts, dt, p, warps, budget, passes, nst, nni, sts};
+  SubstepKey key{dstate, ncells, dld, list, nlist, ddts, dt, p, warps, occ, budget, passes, nst, nni, sts};
   int slot = -1;
   for (int i = 0; i < SolverState::kGraphs; ++i)
     if (s->graph[i] && s->key[i] == key) slot = i;
@@ -317,7 +321,7 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
       a.n_in = (int)ncells;
       L.n_in_dev = pass == 0 ? nlist : cnt + 2 + (cur ^ 1);
       a.budget = pass == passes - 1 ? 0x7fffffff : budget;
-      bdf_kernel(warps)<<<s->blocks, warps * 32, smem, st>>>(L);
+      bdf_kernel(warps, occ)<<<s->blocks, warps * 32, smem, st>>>(L);
     }
     cudaGraph_t graph;
     e = cudaStreamEndCapture(st, &graph);

@@ -23,7 +23,8 @@ module tiger_chem_gpu
     real(c_double) :: rtol, atol
     integer(c_int) :: max_steps, max_newton, block_size, rate_variant
     integer(c_int) :: solver_warps, pass_budget, max_passes
-    integer(c_int) :: reserved(4)
+    integer(c_int) :: solver_occupancy
+    integer(c_int) :: reserved(3)
   end type tng_cfg
 
   type, bind(C) :: tng_extent
