@@ -14,6 +14,7 @@ Workloads (seeded synthetic states, built like the reference's init_flow tool; t
                    reference (max relative T error, max |dY| / max Y).
   gri-substep      the plain implicit substep (BDF/Newton, persistent work-stealing kernel in a
                    CUDA graph, FP64 LU) of the same 2,097,152-cell batch.
+  gri-substep-mixed the same with the rate-constant exponentials on the FP32 unit (precision split).
   h2-substep       the plain implicit substep of the hydrogen mechanism on 32^3 cells, dt = 1e-6 s.
   gri-rates        production-rate evaluation only (finitechem_compute_rhs + PRODRATES),
                    128^3 cells, FP64.
@@ -64,6 +65,11 @@ WORKLOADS = {
                     "metric": "GRI-3.0 (36-sp stand-in) implicit substep cells/s",
                     "desc": "GRI-Mech 3.0 stand-in (36 sp) implicit substep, 128^3 cells, per-cell dt 1e-7..1e-5 s",
                     "steps": 1, "ref_sample": 2048},
+    "gri-substep-mixed": {"kind": "substep", "mech": "grimech30", "side": 128, "precision": "mixed",
+                          "metric": "GRI-3.0 (36-sp stand-in) implicit substep cells/s",
+                          "desc": "GRI-Mech 3.0 stand-in implicit substep, 128^3 cells, per-cell dt 1e-7..1e-5 s, "
+                                  "rate-constant exponentials in FP32 (exponents, LU, Newton in FP64)",
+                          "steps": 1, "ref_sample": 2048},
     "h2-substep": {"kind": "substep", "mech": "hydrogen", "side": 32, "precision": "fp64",
                    "metric": "H2 implicit substep cells/s",
                    "desc": "hydrogen (9 sp) implicit substep, 32^3 cells, dt = 1e-6 s", "steps": 20,

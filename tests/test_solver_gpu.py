@@ -122,3 +122,26 @@ def test_substep_status_codes():
     x1 = x0.clone()
     chem.substep(x1, 0.0, P)
     assert torch.equal(x0, x1)
+
+
+@pytest.mark.parametrize("mech", ["grimech30", "dme39"])
+def test_mixed_precision_substep_against_fp64(mech):
+    """Precision split: rate-constant exponentials on the FP32 unit (exponents, LU, Newton and the
+    error test in FP64). Stated error against the FP64 path of the same solver at rtol 1e-6."""
+    sol = batch(mech, 1024, seed=9, progress="beta22", T_range=(300.0, 2400.0))
+    rng = np.random.default_rng(5)
+    dts = torch.from_numpy(10 ** rng.uniform(-7, -5, sol.shape[1])).cuda()
+    a = torch.from_numpy(sol).cuda()
+    b = a.clone()
+    s64 = capi.FiniteChem(mech, "fp64").substep(a, dts, P)
+    smx = capi.FiniteChem(mech, "mixed").substep(b, dts, P)
+    assert s64["cells_failed"] == 0 and smx["cells_failed"] == 0
+    dT, dY = close_at_tolerance(b.cpu().numpy(), a.cpu().numpy())
+    assert dT < 1e-4 and dY < 1e-5, (dT, dY)
+    # the right-hand side itself: relative error of the rate constants ~3e-7, normwise
+    chem = capi.FiniteChem(mech, "mixed")
+    x = torch.from_numpy(sol).cuda()
+    r_mx, _ = chem.solver_rhs_jac(x, P, jacobian=False)
+    r_64, _ = capi.FiniteChem(mech, "fp64").solver_rhs_jac(x, P, jacobian=False)
+    scale = r_64.abs().amax(dim=1, keepdim=True) + 1e-300
+    assert float(((r_mx - r_64).abs() / scale).max()) < 1e-5

@@ -102,6 +102,7 @@ static int ensure_tables(tng_chem* h) {
   s->dev.hi = s->d_int;
   s->dev.ci = s->d_int + L.nhi;
   s->dev.L = L;
+  s->dev.mixed = h->cfg.precision == TNG_MIXED;
   const int nv = L.size[SZ_NV];
   s->rs = (nv % 2 == 0) ? nv + 1 : nv;
   s->smem_warp = warp_mem_doubles(L, s->rs);

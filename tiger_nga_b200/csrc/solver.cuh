@@ -26,6 +26,7 @@
 #include <stdint.h>
 
 #include "solver_layout.h"
+#include "tng_device.cuh"
 
 namespace tng {
 
@@ -39,6 +40,7 @@ struct SvDev {
   const int* __restrict__ hi;     // hot ints (shared memory once staged)
   const int* __restrict__ ci;     // cold ints (global, read through L1)
   SvLayout L;
+  int mixed;  // rate-constant exponentials on the FP32 special-function unit (see rexp)
   __device__ __forceinline__ const double* d(int k) const { return hd + L.hd[k]; }
   __device__ __forceinline__ const int* i(int k) const { return hi + L.hi[k]; }
   __device__ __forceinline__ const int* c(int k) const { return ci + L.ci[k]; }
@@ -151,6 +153,18 @@ __device__ __forceinline__ double expo(const double lnA, const double E, const d
 
 __device__ __forceinline__ int nu_of(const int term) { return (int)(int8_t)(term & 0xFF); }
 
+// exp of a rate-constant exponent in the handle's precision: FP64, or in mixed precision 2^x
+// split into an exact power of two (FP64 scaling) and a fraction in [0, 1) evaluated by the FP32
+// ex2 unit, relative error about 3e-7. The exponent itself (ln A + n ln T - E/RT, where the
+// reverse rates' cancellations sit) is always formed in FP64.
+__device__ __forceinline__ double rexp(const SvDev& t, const double e) {
+  if (!t.mixed) return exp(e);
+  const double x = e * 1.4426950408889634;
+  const double n = floor(x);
+  if (!(n > -1100.0)) return 0.0;
+  return ldexp((double)tng_ex2f((float)(x - n)), (int)fmin(n, 1100.0));
+}
+
 // Per-cell thermochemical state shared by the rate and Jacobian evaluations.
 struct CellPrep {
   double rho, T, LT, invRT, invT, irho;
@@ -222,16 +236,16 @@ __device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, c
     const double lki = expo(par[3], par[4], par[5], (fw >> 4) & 15, c.LT, c.invRT);
     const double lpr = lk0 + w.lcm[fw >> 16] - fmax(lki, sc[SC_LNKMIN]);
     if (lpr_out) *lpr_out = lpr;
-    const double pr = exp(lpr);
+    const double pr = rexp(t, lpr);
     const int fid = ((fw >> 8) & 255) - 1;
-    if (fid < 0) return exp(lki) * pr / (1.0 + pr);
+    if (fid < 0) return rexp(t, lki) * pr / (1.0 + pr);
     const double lg = lpr * sc[SC_INVLN10] + w.fc[3 * fid + 2];
     const double ff = lg / (w.fc[3 * fid + 1] - sc[SC_TD] * lg);
-    return exp(lki + w.fc[3 * fid] / (ff * ff + 1.0)) * pr / (1.0 + pr);
+    return rexp(t, lki + w.fc[3 * fid] / (ff * ff + 1.0)) * pr / (1.0 + pr);
   }
   const double* sd = t.d(HD_SLOT) + 4 * p;
   if (fl & 8) return sd[0];
-  return exp(expo(sd[0], sd[1], sd[2], fl, c.LT, c.invRT));
+  return rexp(t, expo(sd[0], sd[1], sd[2], fl, c.LT, c.invRT));
 }
 
 // finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
@@ -380,7 +394,7 @@ __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const
           if (Mf > 0.0) {
             double lpr;
             rate_const(t, w, c, pp, w0, w1, &lpr);
-            const double pr = exp(lpr);
+            const double pr = rexp(t, lpr);
             const int mw = w1 & 127;
             val = w.W[pp] / (Mf * (1.0 + pr)) * prodC * (mw != kNone7 ? w.Ms[mw] : 1.0);
           }

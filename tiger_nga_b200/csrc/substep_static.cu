@@ -134,6 +134,7 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   a.tab.hi = tab_i;
   a.tab.ci = tab_i + L.nhi;
   a.tab.L = L;
+  a.tab.mixed = h->cfg.precision == TNG_MIXED;
   const int nv = L.size[SZ_NV];
   a.rs = (nv % 2 == 0) ? nv + 1 : nv;
   a.smem_warp = (warp_mem_doubles(L, a.rs) + 3) & ~3;
