@@ -22,7 +22,8 @@ namespace tng {
 constexpr int kInferRows = 128;
 constexpr int kInferThreads = 256;  // 8 warps: two per TMEM lane quarter
 constexpr int kInferMaxBias = 8 * 256 + 256;  // biases of every layer staged in shared memory
-constexpr int kWChunkK = 32;  // K width of one streamed weight chunk
+constexpr int kWChunkK = 32;   // K width of one streamed weight chunk (two MMAs)
+constexpr int kWStages = 2;    // weight stages: one chunk in flight ahead of the MMA
 constexpr int kMaxLayers = 9;
 
 struct InferArgs {
@@ -156,18 +157,22 @@ __device__ __forceinline__ float gelu_fast(float x) {
 
 // shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), two weight stages of
 // 256 x 32 bf16 (16 KB each), barriers and the TMEM address: 96 KB, two CTAs per SM (their
-// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns.
+// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns. (Four stages of 16-wide
+// chunks measured slower: the per-chunk issue and wait overhead outweighs the deeper prefetch.)
 constexpr int kSmemA = kInferRows * 256 * 2;
 constexpr int kSmemStage = 256 * kWChunkK * 2;
-constexpr int kInferSmem = kSmemA + 2 * kSmemStage + 128;
+constexpr int kInferSmem = kSmemA + kWStages * kSmemStage + 128;
 
 __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
   uint8_t* sA = sm;
   uint8_t* sW = sm + kSmemA;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kSmemA + 2 * kSmemStage);
-  // bars[0..1]: stage full, bars[2..3]: stage free, bars[4]: layer done
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 6);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kSmemA + kWStages * kSmemStage);
+  // bars[0..S): stage full, bars[S..2S): stage free, bars[2S]: layer done
+  uint64_t* bar_full = bars;
+  uint64_t* bar_free = bars + kWStages;
+  uint64_t* bar_done = bars + 2 * kWStages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kWStages + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
   __shared__ float s_bias[kInferMaxBias];
   __shared__ double s_rho[kInferRows], s_T[kInferRows];
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
     for (int i = tid; i < nl; i += kInferThreads) s_bias[l * a.hidden + i] = a.bias[a.b_off[l] + i];
   }
   if (tid == 0) {
-    for (int i = 0; i < 5; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < 2 * kWStages + 1; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -189,27 +194,27 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  uint32_t ph_full[2] = {0, 0}, ph_free[2] = {0, 0}, ph_done = 0;
-  int stage_busy[2] = {0, 0};  // thread 0 only: a commit to stage_free is pending
-  int inflight[2] = {0, 0};    // thread 0 only: a weight copy into the stage has not been waited for
-  int gc = 0;                  // thread 0 only: weight chunks issued so far (stage = gc & 1)
-  int pre = 0, pre_base = 0;   // thread 0 only: chunk 0 of the coming layer already issued at gc = pre_base
+  // thread 0 only: parities, pending commits and copies per stage; chunks issued so far (stage =
+  // gc % kWStages); chunks of the coming layer already issued (pre) from gc = pre_base
+  uint32_t ph_full[kWStages] = {}, ph_free[kWStages] = {}, ph_done = 0;
+  int stage_busy[kWStages] = {}, inflight[kWStages] = {};
+  int gc = 0, pre = 0, pre_base = 0;
   int err = 0;
   // issue the bulk copy of weight chunk c of layer l into the next stage (thread 0)
   auto issue = [&](int l, int c) {
     const int K = l == 0 ? a.in_pad : a.hidden;
     const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
-    const int s = gc & 1;
+    const int s = gc % kWStages;
     ++gc;
-    if (stage_busy[s]) {  // wait for the MMAs that read this stage
-      if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
+    if (stage_busy[s]) {  // wait for the MMA that read this stage
+      if (!mbar_wait(&bar_free[s], ph_free[s])) err = 1;
       ph_free[s] ^= 1;
       stage_busy[s] = 0;
     }
     const int kc = min(kWChunkK, K - c * kWChunkK);
     const uint32_t bytes = (uint32_t)N * kc * 2;
-    mbar_expect_tx(&bars[s], bytes);
-    bulk_g2s(sW + s * kSmemStage, a.wpack + a.w_off[l] + (long long)c * N * kWChunkK, bytes, &bars[s]);
+    mbar_expect_tx(&bar_full[s], bytes);
+    bulk_g2s(sW + s * kSmemStage, a.wpack + a.w_off[l] + (long long)c * N * kWChunkK, bytes, &bar_full[s]);
     inflight[s] = 1;
   };
   const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
@@ -269,15 +274,16 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
       if (tid == 0) {
         const uint32_t idesc = umma_idesc(kInferRows, N);
         const uint32_t a_sbo = (uint32_t)K * 16;
-        // chunk c sits in stage (base + c) & 1; chunk c + 1 is in flight while chunk c multiplies
+        // chunk c sits in stage (base + c) % S; after chunk c's MMA is queued the copies of the
+        // chunks up to c + S - 1 are issued, so they load while the tensor core works
         const int base = pre ? pre_base : gc;
-        if (!pre) issue(l, 0);
+        int issued = pre;
         pre = 0;
+        if (issued == 0) issue(l, issued++);
         for (int c = 0; c < nchunk && !err; ++c) {
-          if (c + 1 < nchunk) issue(l, c + 1);
-          const int s = (base + c) & 1;
+          const int s = (base + c) % kWStages;
           const int kc = min(kWChunkK, K - c * kWChunkK);
-          if (!mbar_wait(&bars[s], ph_full[s])) err = 1;
+          if (!mbar_wait(&bar_full[s], ph_full[s])) err = 1;
           ph_full[s] ^= 1;
           inflight[s] = 0;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -289,23 +295,29 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
             const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
             umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
           }
-          umma_commit(&bars[2 + s]);
+          umma_commit(&bar_free[s]);
           stage_busy[s] = 1;
+          while (issued < nchunk && issued < c + kWStages) issue(l, issued++);
         }
-        umma_commit(&bars[4]);
+        umma_commit(bar_done);
       }
-      // epilogue
-      const bool ok = mbar_wait(&bars[4], ph_done);
+      // epilogue: one lane per warp polls the layer barrier, the warp follows
+      bool ok = true;
+      if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      __syncwarp();
       ph_done ^= 1;
       if (!ok) err = 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // the next layer's (or the next tile's first layer's) first weight chunk loads during the epilogue
+      // the next layer's (or the next tile's first layer's) first chunks load during the epilogue
       if (tid == 0 && !err) {
         const bool more = l + 1 < a.nlin || tile + (int)gridDim.x < ntiles;
         if (more) {
+          const int nl = l + 1 < a.nlin ? l + 1 : 0;
+          const int nk = ((nl == 0 ? a.in_pad : a.hidden) + kWChunkK - 1) / kWChunkK;
           pre_base = gc;
-          issue(l + 1 < a.nlin ? l + 1 : 0, 0);
-          pre = 1;
+          pre = min(nk, kWStages - 1);
+          for (int c = 0; c < pre; ++c) issue(nl, c);
         }
       }
       // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
@@ -352,10 +364,10 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   // drain: weight copies still in flight (after an error) and the last commits on the stage
   // barriers must complete before the CTA exits; every wait is bounded
   if (tid == 0) {
-    for (int s = 0; s < 2; ++s) {
-      if (inflight[s] && !mbar_wait(&bars[s], ph_full[s])) err = 1;
+    for (int s = 0; s < kWStages; ++s) {
+      if (inflight[s] && !mbar_wait(&bar_full[s], ph_full[s])) err = 1;
       if (stage_busy[s]) {
-        if (!mbar_wait(&bars[2 + s], ph_free[s])) err = 1;
+        if (!mbar_wait(&bar_free[s], ph_free[s])) err = 1;
         ph_free[s] ^= 1;
       }
     }
