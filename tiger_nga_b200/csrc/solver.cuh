@@ -582,31 +582,4 @@ __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const
   x1 = b1;
 }
 
-// Solve (LU) x = b in place; b in shared memory.
-__device__ __forceinline__ void lu_solve_warp(const double* a, const int n, const int rs, const int* piv, double* b, const int lane) {
-  if (lane == 0)
-    for (int k = 0; k < n; ++k) {
-      const int p = piv[k];
-      if (p != k) {
-        const double tmp = b[k];
-        b[k] = b[p];
-        b[p] = tmp;
-      }
-    }
-  __syncwarp();
-  for (int k = 0; k < n; ++k) {
-    const double bk = b[k];
-    for (int i = k + 1 + lane; i < n; i += 32) b[i] = fma(-a[i * rs + k], bk, b[i]);
-    __syncwarp();
-  }
-  for (int k = n - 1; k >= 0; --k) {
-    const double v = b[k];
-    __syncwarp();
-    const double bk = v / a[k * rs + k];
-    for (int i = lane; i < k; i += 32) b[i] = fma(-a[i * rs + k], bk, b[i]);
-    if (lane == 0) b[k] = bk;
-    __syncwarp();
-  }
-}
-
 }  // namespace tng

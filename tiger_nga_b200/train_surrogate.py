@@ -3,8 +3,9 @@
     python -m tiger_nga_b200.train_surrogate --mech grimech30 --pairs 8388608 \\
         --out tiger_nga_b200/models/grimech30.tngs
 
-Pairs (--dist uneven, the default): seeded states of the uneven-stiffness batch -- 128^3 grids of a smooth Fourier-mode
-mixture-fraction field (CH4 fuel / air at 300 K for GRI-Mech, DME at 400 K for DME39),
+Pairs (--dist uneven, the default): seeded states of the uneven-stiffness batch -- 128^3 grids
+of a smooth Fourier-mode mixture-fraction field (CH4 fuel / air at 300 K for GRI-Mech, DME at
+400 K for DME39),
 progress c ~ Beta(2,2) mapped to T in [300, 2400] K, minor species log-uniform in
 [1e-10, 1e-3], dt log-uniform in [1e-7, 1e-5] s per cell, P = 1 atm -- each advanced by
 tng_substep_batch. With --dist mixing-layer the pairs are taken along 100-substep
@@ -110,7 +111,8 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.
     Returns the timed surrogate-with-fallback substep (stats, speed-up over the plain solve) and,
     from the fallback-free prediction of every cell, the error of the cells each consistency
     tolerance (K) and ensemble-spread tolerances (K, mass fraction) would accept, with the plain
-    solver's share of steps those cells leave to the fallback. Per-cell arrays (errors, indicator, reason, T0, dt, steps) are returned as well.
+    solver's share of steps those cells leave to the fallback. Per-cell arrays (errors,
+    indicators, reason, T0, dt, steps) are returned as well.
     """
     import torch
 
