@@ -84,7 +84,9 @@ WORKLOADS = {
                         "steps": 400, "ref_sample": 131072},
 }
 # kernels of this library launched per step (counted from the host code of each path)
-LAUNCHES = {"rates": 1, "substep": 2, "surrogate": 8, "sweep": 8}
+# surrogate step: judge-sample gather, 2 ensemble inferences, post-processing, fallback gather,
+# list fill, solver graph (counter reset + solver), statistics, fallback scatter, judge compare
+LAUNCHES = {"rates": 1, "substep": 3, "surrogate": 11, "sweep": 11}
 
 
 def dist_env():
