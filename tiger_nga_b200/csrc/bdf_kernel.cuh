@@ -16,6 +16,7 @@ __constant__ BdfCoef c_bdf;
 struct BdfLaunch {
   BdfArgs a;
   const int* n_in_dev;  // when non-null, the number of queued cells is read from device memory
+  int cold_in_smem;     // the Jacobian's term lists staged in shared memory (after the hot tables)
 };
 
 // two-entry-per-lane vector helpers
@@ -425,9 +426,14 @@ __host__ __device__ inline int hot_smem_doubles(const SvLayout& L) { return (hot
 template <int WARPS, int MINB = 1>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_bdf(const BdfLaunch P) {
   extern __shared__ __align__(16) double smem[];
-  const SvDev t = stage_tables(P.a.tab, smem);
+  SvDev t = stage_tables(P.a.tab, smem);
+  size_t off = hot_smem_doubles(t.L);
+  if (P.cold_in_smem) {
+    t = stage_cold_tables(t, smem + off);
+    off += cold_smem_doubles(t.L);
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpMem w = warp_mem(smem + hot_smem_doubles(t.L) + (size_t)warp * P.a.smem_warp, t.L, P.a.rs);
+  const WarpMem w = warp_mem(smem + off + (size_t)warp * P.a.smem_warp, t.L, P.a.rs);
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.a.n_in;
   for (;;) {
     int idx = 0;

@@ -59,7 +59,7 @@ struct SolverState {
   cudaGraphExec_t graph[kGraphs] = {};
   SubstepKey key[kGraphs] = {};
   int next_slot = 0;
-  int warps = 0, occ = 0, blocks = 0;
+  int warps = 0, occ = 0, blocks = 0, cold_in_smem = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -128,13 +128,19 @@ static BdfKernel bdf_kernel(int warps, int occ = 1) {
   }
 }
 
-static size_t block_smem(const SolverState* s, int warps) {
-  return ((size_t)hot_smem_doubles(s->dev.L) + (size_t)warps * s->smem_warp) * sizeof(double);
+static size_t block_smem(const SolverState* s, int warps, int cold) {
+  return ((size_t)hot_smem_doubles(s->dev.L) + (cold ? (size_t)cold_smem_doubles(s->dev.L) : 0) +
+          (size_t)warps * s->smem_warp) *
+         sizeof(double);
 }
 
 static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   SolverState* s = h->solver;
-  const size_t smem = block_smem(s, warps);
+  // the Jacobian's term lists go to shared memory when the block still fits the SM with them
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device);
+  s->cold_in_smem = block_smem(s, warps, 1) * occ <= (size_t)optin ? 1 : 0;
+  const size_t smem = block_smem(s, warps, s->cold_in_smem);
   BdfKernel k = bdf_kernel(warps, occ);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
@@ -308,7 +314,8 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
     a.smem_warp = s->smem_warp;
     a.rs = s->rs;
     int* cnt = (int*)s->counters.ptr;  // [0..1] heads, [2..3] out counts
-    const size_t smem = block_smem(s, warps);
+    const size_t smem = block_smem(s, warps, s->cold_in_smem);
+    L.cold_in_smem = s->cold_in_smem;
     cudaStream_t st = h->stream;
     cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     cudaMemsetAsync(s->resume.ptr, 0, ncells * sizeof(int), st);
@@ -384,7 +391,7 @@ extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncel
   int rc = ensure_tables(h);
   if (rc) return rc;
   SolverState* s = h->solver;
-  const size_t smem = block_smem(s, 4);
+  const size_t smem = block_smem(s, 4, 0);
   cudaError_t e = cudaFuncSetAttribute(k_warp_rhs_jac<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   const int blocks = (int)std::min<int64_t>((ncells + 3) / 4, 148 * 8);

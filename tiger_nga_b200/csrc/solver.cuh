@@ -64,6 +64,18 @@ __device__ __forceinline__ SvDev stage_tables(const SvDev& g, void* smem) {
 }
 
 __host__ __device__ inline int hot_smem_bytes(const SvLayout& L) { return L.nhd * 8 + L.nhi * 4; }
+__host__ __device__ inline int cold_smem_doubles(const SvLayout& L) { return (L.nci * 4 + 15) / 16 * 2; }
+
+// Copy the cold tables (the Jacobian's term lists) into shared memory at `at` (all threads),
+// when the block has room for them; otherwise they are read from global memory through L1,
+// which the shared-memory carve-out leaves small.
+__device__ __forceinline__ SvDev stage_cold_tables(SvDev t, double* at) {
+  int* d = reinterpret_cast<int*>(at);
+  for (int e = threadIdx.x; e < t.L.nci; e += blockDim.x) d[e] = t.ci[e];
+  __syncthreads();
+  t.ci = d;
+  return t;
+}
 
 // status codes per cell
 enum { ST_OK = 0, ST_MAXSTEPS = 1, ST_CONVFAIL = 2, ST_ERRFAIL = 3, ST_NONFINITE = 4, ST_HMIN = 5, ST_PENDING = 9 };
