@@ -422,8 +422,10 @@ finish:
 // Shared memory of one block: the staged hot tables, then one workspace per warp.
 __host__ __device__ inline int hot_smem_doubles(const SvLayout& L) { return (hot_smem_bytes(L) + 15) / 16 * 2; }
 
-// One block per SM of WARPS warps (the staged tables are shared by the block's warps).
-template <int WARPS, int MINB = 1>
+// One block per SM of WARPS warps (the staged tables are shared by the block's warps). TAG keeps
+// the instantiations of different translation units apart: each unit has its own constant bank
+// (c_bdf), so two units must not register the same kernel symbol.
+template <int WARPS, int MINB = 1, int TAG = 0>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_bdf(const BdfLaunch P) {
   extern __shared__ __align__(16) double smem[];
   SvDev t = stage_tables(P.a.tab, smem);

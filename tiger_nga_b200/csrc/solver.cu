@@ -136,10 +136,12 @@ static size_t block_smem(const SolverState* s, int warps, int cold) {
 
 static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   SolverState* s = h->solver;
-  // the Jacobian's term lists go to shared memory when the block still fits the SM with them
+  // the Jacobian's term lists go to shared memory when the blocks still leave the SM about a
+  // quarter of its shared/L1 capacity as L1 (measured: with GRI-Mech, 224 KB of shared memory
+  // per SM left too little L1 for the solver's stack and was slower; H2 gains 9 %)
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device);
-  s->cold_in_smem = block_smem(s, warps, 1) * occ <= (size_t)optin ? 1 : 0;
+  s->cold_in_smem = block_smem(s, warps, 1) * occ <= (size_t)optin * 7 / 8 ? 1 : 0;
   const size_t smem = block_smem(s, warps, s->cold_in_smem);
   BdfKernel k = bdf_kernel(warps, occ);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -317,22 +319,34 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
     const size_t smem = block_smem(s, warps, s->cold_in_smem);
     L.cold_in_smem = s->cold_in_smem;
     cudaStream_t st = h->stream;
-    cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
-    cudaMemsetAsync(s->resume.ptr, 0, ncells * sizeof(int), st);
+    cudaError_t pending = cudaGetLastError();  // an earlier asynchronous error is reported, not captured
+    if (pending != cudaSuccess) return cuda_error(pending, "implicit substep (error pending before the graph capture)");
+    cudaError_t first = cudaSuccess;            // the first error inside the capture, and where
+    const char* where = "";
+    auto note = [&](cudaError_t r, const char* w) {
+      if (first == cudaSuccess && r != cudaSuccess) first = r, where = w;
+    };
+    note(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    note(cudaMemsetAsync(s->resume.ptr, 0, ncells * sizeof(int), st), "resume flags");
     for (int pass = 0; pass < passes; ++pass) {
       const int cur = pass & 1;
       a.head = cnt + cur;
       a.n_out = cnt + 2 + cur;
       k_reset_counters<<<1, 32, 0, st>>>(a.head, a.n_out);
+      note(cudaGetLastError(), "counter reset");
       a.queue_in = pass == 0 ? list : (const int*)s->queue[cur ^ 1].ptr;
       a.queue_out = (int*)s->queue[cur].ptr;
       a.n_in = (int)ncells;
       L.n_in_dev = pass == 0 ? nlist : cnt + 2 + (cur ^ 1);
       a.budget = pass == passes - 1 ? 0x7fffffff : budget;
       bdf_kernel(warps, occ)<<<s->blocks, warps * 32, smem, st>>>(L);
+      note(cudaGetLastError(), "solver kernel");
     }
     cudaGraph_t graph;
     e = cudaStreamEndCapture(st, &graph);
+    if (first != cudaSuccess)
+      return set_error(TNG_ERR_CUDA, "solver graph capture, %s (%d blocks x %d threads, %zu B shared): %s", where,
+                       s->blocks, warps * 32, smem, cudaGetErrorString(first));
     if (e != cudaSuccess) return cuda_error(e, "solver graph capture");
     e = cudaGraphInstantiate(&s->graph[slot], graph, 0);
     cudaGraphDestroy(graph);

@@ -139,7 +139,8 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   a.rs = (nv % 2 == 0) ? nv + 1 : nv;
   a.smem_warp = (warp_mem_doubles(L, a.rs) + 3) & ~3;
   const size_t smem = ((size_t)hot_smem_doubles(L) + (size_t)warps * a.smem_warp) * sizeof(double);
-  void (*kern)(const BdfLaunch) = warps == 2 ? k_bdf<2> : warps == 4 ? k_bdf<4> : k_bdf<8>;
+  // this file's own instantiations (TAG 1): they read this file's constant bank
+  void (*kern)(const BdfLaunch) = warps == 2 ? k_bdf<2, 1, 1> : warps == 4 ? k_bdf<4, 1, 1> : k_bdf<8, 1, 1>;
   if (d->smem_set[warps] < smem) {
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: shared memory");
