@@ -10,7 +10,8 @@ progress c ~ Beta(2,2) mapped to T in [300, 2400] K, minor species log-uniform i
 [1e-10, 1e-3], dt log-uniform in [1e-7, 1e-5] s per cell, P = 1 atm -- each advanced by
 tng_substep_batch. With --dist mixing-layer the pairs are taken along 100-substep
 (dt = 2e-6 s) trajectories of temporal mixing layers (fuel above air, seeded burning fraction)
-instead. The network is trained by the library's own CUDA kernels
+instead; with --onpolicy MODEL part of them come from the states MODEL's own sweep visits
+(targets from the implicit solve), so the network also sees its own drift. The network is trained by the library's own CUDA kernels
 (tng_surrogate_train: FP32 forward/backward, Adam, cosine learning rate), then evaluated
 on fresh cells against the plain solve (accepted fraction, max relative error of T, max
 species error over max Y). Writes the weights file and a JSON log beside it.
@@ -102,6 +103,40 @@ def make_trajectory_pairs(chem, n_pairs: int, seed: int, dt: float = 2e-6, subst
             done += take
     d = torch.full((done,), dt, dtype=torch.float64, device="cuda")
     return s0[:, :done].contiguous(), s1[:, :done].contiguous(), d, solve_s
+
+
+def make_onpolicy_pairs(chem, sur, n_pairs: int, seed: int, dt: float = 2e-6, substeps: int = 100,
+                        shape=(64, 48, 48)):
+    """Pairs from the states a surrogate-with-fallback sweep itself visits (its own errors
+    included): a seeded mixing layer is advanced ``substeps`` times by ``sur``; at every substep a
+    random subset of its cells is also advanced by the implicit solve, which gives the targets."""
+    import torch
+
+    m = load(chem.mechanism)
+    fuel, t_fuel = FUEL[chem.mechanism]
+    nv = chem.nspecies + 1
+    per = -(-n_pairs // substeps)
+    s0 = torch.empty((nv, n_pairs), dtype=torch.float64, device="cuda")
+    s1 = torch.empty_like(s0)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    sol, _ = states.mixing_layer(m, shape=shape, seed=seed, fuel=fuel, T_fuel=t_fuel)
+    x = torch.from_numpy(sol).cuda()
+    done = 0
+    for _ in range(substeps):
+        take = min(per, n_pairs - done, x.shape[1])
+        if take <= 0:
+            break
+        idx = torch.randperm(x.shape[1], device="cuda", generator=gen)[:take]
+        a = x[:, idx].contiguous()
+        b = a.clone()
+        chem.substep(b, dt, P_ATM, stats=False)
+        s0[:, done:done + take] = a
+        s1[:, done:done + take] = b
+        done += take
+        sur.substep(x, dt, P_ATM)
+    d = torch.full((done,), dt, dtype=torch.float64, device="cuda")
+    return s0[:, :done].contiguous(), s1[:, :done].contiguous(), d
 
 
 def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.0, 2.0, 4.0),
@@ -198,11 +233,24 @@ def main(argv=None):
     ap.add_argument("--consist-tol", type=float, default=5.0)
     ap.add_argument("--out", required=True)
     ap.add_argument("--cells-out", default="", help="write the per-cell evaluation arrays (.npz) here")
+    ap.add_argument("--onpolicy", default="", help="a trained surrogate: part of the pairs come from the states "
+                    "its own sweep visits (mixing-layer distribution)")
+    ap.add_argument("--onpolicy-frac", type=float, default=0.5)
     a = ap.parse_args(argv)
     chem = capi.FiniteChem(a.mech, "fp64")
     t0 = time.perf_counter()
     if a.dist == "mixing-layer":
-        s0, s1, d, solve_s = make_trajectory_pairs(chem, a.pairs, a.seed)
+        n_on = int(a.pairs * a.onpolicy_frac) if a.onpolicy else 0
+        s0, s1, d, solve_s = make_trajectory_pairs(chem, a.pairs - n_on, a.seed)
+        if n_on:
+            import torch
+
+            prev = capi.Surrogate(chem, members=a.members)
+            prev.load(a.onpolicy)
+            o0, o1, od = make_onpolicy_pairs(chem, prev, n_on, a.seed + 31337)
+            prev.close()
+            s0, s1, d = torch.cat([s0, o0], 1), torch.cat([s1, o1], 1), torch.cat([d, od])
+            del o0, o1, od
     else:
         s0, s1, d, solve_s = make_pairs(chem, a.pairs, a.seed)
     t_pairs = time.perf_counter() - t0
@@ -216,7 +264,8 @@ def main(argv=None):
     ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991, dist=a.dist)
     if a.cells_out:
         np.savez_compressed(a.cells_out, **cells)
-    log = {"mechanism": a.mech, "dist": a.dist, "pairs": a.pairs, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
+    log = {"mechanism": a.mech, "dist": a.dist, "pairs": a.pairs, "onpolicy": a.onpolicy,
+           "onpolicy_frac": a.onpolicy_frac if a.onpolicy else 0.0, "epochs": a.epochs, "batch": a.batch, "lr": a.lr, "seed": a.seed,
            "target_mode": a.target_mode, "post_mode": a.post_mode, "loss_T_weight": a.loss_T_weight,
            "members": a.members,
            "consist_tol_K": a.consist_tol,
