@@ -19,6 +19,10 @@ Workloads (seeded synthetic states, built like the reference's init_flow tool; t
   gri-rates        production-rate evaluation only (finitechem_compute_rhs + PRODRATES),
                    128^3 cells, FP64.
   gri-rates-mixed  the same in mixed precision (FP32 log-space rates, FP64 reverse exponents).
+  gri-transport    the mixture transport properties around the substep (finitechem_viscosity +
+                   finitechem_diffusivity fused: Wilke viscosity, lambda/Cp per species) of the
+                   128^3 rate-evaluation states (Y, T), FP64.
+  gri-density      the equation of state (finitechem_density + finitechem_W) of the same cells.
   dme-sweep        the DME39 mechanism on a 256x192x192 temporal mixing layer (DME at 400 K above air
                    at 300 K, tanh mixture-fraction profile plus seeded Fourier perturbations of
                    amplitude 0.1, seeded burning fraction), 100 consecutive substeps of dt = 2e-6 s
@@ -82,11 +86,20 @@ WORKLOADS = {
                         "metric": "GRI-3.0 (36-sp stand-in) rate evaluation cells/s",
                         "desc": "GRI-Mech 3.0 stand-in (36 sp, 422 slots) rates, 128^3 cells, mixed FP32/FP64",
                         "steps": 400, "ref_sample": 131072},
+    "gri-transport": {"kind": "props", "what": "transport", "mech": "grimech30", "side": 128, "precision": "fp64",
+                      "metric": "GRI-3.0 (36-sp stand-in) mixture transport properties cells/s",
+                      "desc": "finitechem_viscosity + finitechem_diffusivity in one pass (Wilke viscosity, "
+                              "conductivity, lambda/Cp per species), 128^3 cells, FP64", "steps": 200,
+                      "ref_sample": 2048},
+    "gri-density": {"kind": "props", "what": "density", "mech": "grimech30", "side": 128, "precision": "fp64",
+                    "metric": "GRI-3.0 (36-sp stand-in) density (equation of state) cells/s",
+                    "desc": "finitechem_density + finitechem_W, 128^3 cells, FP64", "steps": 400,
+                    "ref_sample": 262144},
 }
 # kernels of this library launched per step (counted from the host code of each path)
 # surrogate step: judge-sample gather, 2 ensemble inferences, post-processing, fallback gather,
 # list fill, solver graph (counter reset + solver), statistics, fallback scatter, judge compare
-LAUNCHES = {"rates": 1, "substep": 3, "surrogate": 11, "sweep": 11}
+LAUNCHES = {"rates": 1, "substep": 3, "surrogate": 11, "sweep": 11, "props": 1}
 
 
 def dist_env():
@@ -178,6 +191,11 @@ def make_state(wl, rank):
     if wl["kind"] == "rates":
         sol, _ = states.chem_state(mech, n, seed, "CH4", grid=(wl["side"],) * 3)
         return sol, None
+    if wl["kind"] == "props":
+        # the solver's scalars [Y_1..Y_N, T] of the rate-evaluation states
+        sol, _ = states.chem_state(mech, n, seed, "CH4", grid=(wl["side"],) * 3)
+        rho = sol[:mech.ns].sum(0)
+        return np.ascontiguousarray(sol / rho), None
     from tiger_nga_b200.train_surrogate import state_batch
 
     return state_batch(wl["mech"], n, seed, side=wl["side"])
@@ -195,20 +213,26 @@ def cpu_rates_runner(mech):
 
 
 def cpu_step(wl, impl, sol, dts, lo, m, nthreads):
-    """One bounded sample of the workload on the host cores (cells lo .. lo+m, wrapping)."""
+    """One bounded sample of the workload on the host cores (cells lo .. lo+m, wrapping).
+    Returns (cells, seconds of the compute call); gathering the sample is not timed."""
     n = sol.shape[1]
     idx = (lo + np.arange(m)) % n
     sub = np.ascontiguousarray(sol[:, idx])
+    d = None if dts is None or np.ndim(dts) == 0 else np.ascontiguousarray(dts[idx])
+    y, t = (np.ascontiguousarray(sub[:-1]), np.ascontiguousarray(sub[-1])) if wl["kind"] == "props" else (None, None)
+    t0 = time.perf_counter()
     if wl["kind"] == "rates":
         impl.rhs_batch(sub, P_ATM, nthreads)
+    elif wl["kind"] == "props":
+        what = ("visc", "diff") if wl["what"] == "transport" else ("wmix", "rho")
+        impl.props_batch(y, t, p_thermo=P_ATM, what=what, nthreads=nthreads)
     else:
-        d = dts if np.ndim(dts) == 0 else np.ascontiguousarray(dts[idx])
-        impl.substep_batch(sub, d, P_ATM, nthreads=nthreads)
-    return m
+        impl.substep_batch(sub, dts if d is None else d, P_ATM, nthreads=nthreads)
+    return m, time.perf_counter() - t0
 
 
 def cpu_impl(wl):
-    if wl["kind"] == "rates":
+    if wl["kind"] in ("rates", "props"):
         return cpu_rates_runner(wl["mech"])
     from oracle.oracle import Oracle
 
@@ -220,14 +244,21 @@ def time_cpu(wl, sol, dts, seconds: float, nthreads: int):
     m = min(wl["ref_sample"], sol.shape[1])
     stride = max(1, sol.shape[1] // m)
     cpu_step(wl, impl, sol, dts, 0, min(m, 256), nthreads)  # warm-up
-    done, t0, i = 0, time.perf_counter(), 0
-    while True:
-        done += cpu_step(wl, impl, sol, dts, (i * 7919 * stride) % sol.shape[1], m, nthreads)
-        i += 1
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
+    done, el, i = 0, 0.0, 0
+    while el < seconds:
+        c, s = cpu_step(wl, impl, sol, dts, (i * 7919 * stride) % sol.shape[1], m, nthreads)
+        done, el, i = done + c, el + s, i + 1
     return kind, done / el, done, el
+
+
+def cpu_what(wl, kind):
+    src = "transliterated reference Fortran" if kind == "reference" else "oracle port"
+    if wl["kind"] == "rates":
+        return f"rate evaluation ({src})"
+    if wl["kind"] == "props":
+        r = "finitechem_viscosity + finitechem_diffusivity" if wl["what"] == "transport" else "finitechem_density"
+        return f"{r} ({'the reference routines restated over its transliterated getters' if kind == 'reference' else src})"
+    return "implicit BDF/Newton substep (oracle port: the reference's CVODE is not buildable here)"
 
 
 def reference_arm(args, wl, config, metric, unit):
@@ -238,14 +269,9 @@ def reference_arm(args, wl, config, metric, unit):
     m = min(wl["ref_sample"], sol.shape[1])
     for w in range(args.warmup):
         cpu_step(wl, impl, sol, dts, w * m, m, nthreads)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        cpu_step(wl, impl, sol, dts, (k * 7919 * m) % sol.shape[1], m, nthreads)
-    el = time.perf_counter() - t0
+    el = sum(cpu_step(wl, impl, sol, dts, (k * 7919 * m) % sol.shape[1], m, nthreads)[1] for k in range(args.steps))
     val = m * args.steps / el
-    what = ("rate evaluation (transliterated reference Fortran)" if kind == "reference" else
-            "rate evaluation (oracle port)") if wl["kind"] == "rates" else \
-        "implicit BDF/Newton substep (oracle port: the reference's CVODE is not buildable here)"
+    what = cpu_what(wl, kind)
     sample = f"{m} cells of the workload per step, {what}, OpenMP over cells"
     print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
@@ -422,6 +448,141 @@ def run_sweep(args, wl, config, metric, unit, ws, rank, local, dev, pg):
     return 0
 
 
+def props_work(mech, what):
+    """Algorithmic bytes and FP64 flops per cell of one properties launch. Bytes: the N+1 scalars
+    read, and for transport the viscosity plus N+1 diffusivities written (density: rho and W_mix).
+    Flops (transport): Wilke's pair sum as three FMAs per ordered pair j != k, plus per species
+    the collision-integral fit (7 FMAs), the NASA cp polynomial (5 FMAs + 1 multiply), the
+    conductivity and the mixture sums (~8)."""
+    ns = mech.ns
+    if what == "transport":
+        return {"bytes": 8 * (ns + 1) + 8 * (1 + ns + 1), "flops": 6 * ns * (ns - 1) + ns * (14 + 11 + 8)}
+    return {"bytes": 8 * (ns + 1) + 16, "flops": 4 * ns}
+
+
+def run_props(args, wl, config, metric, unit, ws, rank, local, dev, pg):
+    """Mixture properties (tng_chem_transport / tng_chem_density) of a resident batch: K launches
+    back to back between one event pair; e2e through the Fortran-array C-ABI with host arrays."""
+    import ctypes
+
+    import torch
+
+    from tiger_nga_b200 import capi
+
+    mech = load_mech(wl["mech"])
+    sol, _ = make_state(wl, rank)
+    n = sol.shape[1]
+    ns = mech.ns
+    chem = capi.FiniteChem(wl["mech"], wl["precision"], device=local)
+    st = chem.torch_stream()
+    x0 = torch.from_numpy(sol).to(dev)
+    transport = wl["what"] == "transport"
+    outs = {"visc": torch.empty(n, dtype=torch.float64, device=dev),
+            "diff": torch.empty((ns + 1, n), dtype=torch.float64, device=dev)} if transport else \
+        {"rho": torch.empty(n, dtype=torch.float64, device=dev), "wmix": torch.empty(n, dtype=torch.float64, device=dev)}
+    ext = capi.batch_extent(n, ns)
+    lib, h = chem.lib, chem.h
+
+    def launch():
+        if transport:
+            rc = lib.tng_chem_transport(h, outs["visc"].data_ptr(), outs["diff"].data_ptr(), x0.data_ptr(), None,
+                                        ctypes.byref(ext), None, 0, capi.TNG_DEVICE_PTRS)
+        else:
+            rc = lib.tng_chem_density(h, outs["rho"].data_ptr(), outs["wmix"].data_ptr(), x0.data_ptr(), None,
+                                      ctypes.byref(ext), P_ATM, capi.TNG_DEVICE_PTRS)
+        if rc:
+            raise RuntimeError(capi.last_error())
+
+    torch.cuda.synchronize(dev)
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize(dev)
+    if pg:
+        pg.barrier()
+    uuid = str(torch.cuda.get_device_properties(dev).uuid)
+    clocks = ClockSampler(uuid if uuid.startswith("GPU-") else f"GPU-{uuid}")
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        launch()
+    e1.record(st)
+    e1.synchronize()
+    ms_total = e0.elapsed_time(e1)
+    if pg:
+        pg.barrier()
+    clk = clocks.stop()
+    ms_total = max_over_ranks(pg, dev, ms_total)
+    ms_step = ms_total / args.steps
+    value = n * ws / (ms_step * 1e-3)
+    for v in outs.values():
+        if not bool(torch.isfinite(v).all()):
+            raise RuntimeError("non-finite values in the benchmark output")
+
+    hbm_peak, _, peak_src = peaks()
+    wk = props_work(mech, wl["what"])
+    achieved = wk["bytes"] * n / (ms_step * 1e-3) / 1e9
+    fp64_peak = capi.fp64_peak_tflops(local)
+    fp64_ach = wk["flops"] * n / (ms_step * 1e-3) / 1e12
+    tr = read_profile_value(f"k_props_{wl['mech']}_{wl['what']}.txt", "dram_bytes_per_cell")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+            "traffic": tr * n if tr else None, "peak_source": peak_src, "kernel": "k_props",
+            "algorithmic_bytes_per_cell": wk["bytes"],
+            "fp64_pipe": {"achieved_tflops": fp64_ach, "peak_tflops_measured": fp64_peak, "frac": fp64_ach / fp64_peak,
+                          "alg_flops_per_cell": wk["flops"]}}
+
+    # e2e: the Fortran-array drop-in with host arrays (copies in and out inside the call)
+    hin = torch.from_numpy(sol).pin_memory()
+    SC = hin.numpy().T  # Fortran (n, N+1)
+    if transport:
+        hv = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        hd = torch.empty((ns + 1, n), dtype=torch.float64).pin_memory().numpy().T
+        call = lambda: chem.transport(SC, ext_dict(ext), VISC=hv, DIFF=hd)  # noqa: E731
+        d2h = 8 * n * (ns + 2)
+    else:
+        hr = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        hw = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+        call = lambda: chem.density(hr, SC, ext_dict(ext), P_ATM, W=hw)  # noqa: E731
+        d2h = 16 * n
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 5)
+    call()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        call()
+    e2e_s = max_over_ranks(pg, dev, (time.perf_counter() - t0) / e2e_steps)
+    e2e = {"value": n * ws / e2e_s, "unit": unit, "h2d_bytes_per_step": sol.nbytes * ws,
+           "d2h_bytes_per_step": d2h * ws, "steps": e2e_steps}
+    cpu = None
+    if rank == 0 and ws == 1 and args.cpu_seconds > 0:
+        kind, cval, cdone, cel = time_cpu(wl, sol, None, args.cpu_seconds, os.cpu_count() or 1)
+        cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
+               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, {cpu_what(wl, kind)}, OpenMP over cells"}
+    if rank == 0:
+        print(json.dumps({"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded CH4/air states)",
+                          "config": config, "e2e": e2e, "gpu_launches": LAUNCHES["props"] * args.steps,
+                          "roofline": roof, "cpu_baseline": cpu, "clocks": clk}))
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    chem.close()
+    return 0
+
+
+def ext_dict(e):
+    return {f: getattr(e, f) for f, _ in e._fields_}
+
+
+def load_mech(name):
+    from tiger_nga_b200.mechanism import load
+
+    return load(name)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -481,6 +642,8 @@ def main():
 
     if wl["kind"] == "sweep":
         return run_sweep(args, wl, config, metric, unit, ws, rank, local, dev, pg)
+    if wl["kind"] == "props":
+        return run_props(args, wl, config, metric, unit, ws, rank, local, dev, pg)
     sol, dts = make_state(wl, rank)
     chem = capi.FiniteChem(wl["mech"], wl["precision"], device=local)
     st = chem.torch_stream()
@@ -676,7 +839,7 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and args.cpu_seconds > 0:
         kind, cval, cdone, cel = time_cpu(wl, sol, dts, args.cpu_seconds, os.cpu_count() or 1)
-        what = "rate evaluation" if wl["kind"] == "rates" else "implicit BDF/Newton substep (no surrogate)"
+        what = cpu_what(wl, kind) if wl["kind"] in ("rates", "props") else "implicit BDF/Newton substep (no surrogate)"
         cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
                "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, {what}, OpenMP over cells"}
     if rank == 0:

@@ -180,6 +180,28 @@ typedef struct tng_extent {
 int tng_chem_substep(tng_chem* h, const double* rho, double* sc, const int* mask, const tng_extent* ext, double dt,
                      double p_mid, double* hr, double* chemsrc, int flags, tng_substep_stats* stats);
 
+/* ---- Mixture properties around the substep, on the same Fortran arrays. Like the reference,
+ * they visit every cell of the padded block (imino..imaxo, jmino..jmaxo, kmino..kmaxo) whose
+ * mask(i,j) /= 1 and leave masked cells untouched; only ext's padded extents, nscalar, isc_sc
+ * and isc_T are read. flags: TNG_DEVICE_PTRS (asynchronous on the handle's stream) or
+ * TNG_HOST_PTRS (copied through the device; the call returns when the results are back).
+ *
+ * Replaces finitechem_density (combustion/finitechem.f90:324-345) with finitechem_W (:65-74):
+ *   W_mix = sum(Y')/sum(Y'/W), Y' = min(max(Y,0),1);  rho = p_thermo*W_mix/(8314.34*T).
+ * rho and wmix (both shaped like RHO) are each nullable. */
+int tng_chem_density(tng_chem* h, double* rho, double* wmix, const double* sc, const int* mask, const tng_extent* ext,
+                     double p_thermo, int flags);
+
+/* Replaces finitechem_viscosity (finitechem.f90:351-406) and finitechem_diffusivity (:412-461),
+ * with finitechem_omegamu (:467-487): T clipped to [50, 5000] K, species viscosities from the
+ * mechanism's GETMUCOEFF / GETKOVEREPS fits, Wilke's mixture rule into visc (shaped like RHO),
+ * and lambda/Cp_mix into diff (shaped like SC): diff(isc_sc+k-1) = lambda/Cp_mix/lewis[k],
+ * diff(isc_T) = lambda/Cp_mix, and diff(isc_zmix) = lambda/Cp_mix when isc_zmix > 0. visc or
+ * diff may be null (one of the two routines alone); both non-null computes them in one pass.
+ * lewis: N Lewis numbers in HOST memory (the 'Lewis <species>' inputs, :293-301); null = 1. */
+int tng_chem_transport(tng_chem* h, double* visc, double* diff, const double* sc, const int* mask,
+                       const tng_extent* ext, const double* lewis, int isc_zmix, int flags);
+
 /* Parity helper: the solver's own (table-driven, warp-cooperative) right-hand side and, when
  * jac is non-null, its Jacobian (cell-major, (N+1)^2 row-major per cell), device pointers. */
 int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,

@@ -7,7 +7,8 @@ The reference's chemistry rates live in three self-contained generated Fortran f
 (combustion/HYDROGENF.f90, combustion/grimech30F.f90, combustion/DME39F.f90, each with its
 ``*F90.h`` parameter header). No Fortran compiler exists in this image, so this recipe
 transliterates the routines on the path -- ``PRODRATES``, ``GETLINDRATECOEFF``,
-``COMPTHERMODATA`` and ``GETMOLARMASS`` -- statement by statement into C, keeping:
+``COMPTHERMODATA``, ``GETMOLARMASS`` and the transport fits ``GETMUCOEFF`` / ``GETKOVEREPS`` --
+statement by statement into C, keeping:
 
 * the statement order and each expression's operator order (C and Fortran both associate
   ``+ - * /`` left to right; the C file is compiled with ``-ffp-contract=off`` so no FMA is
@@ -37,7 +38,7 @@ MECHS = {
     "grimech30": ("grimech30F.f90", "grimech30F90.h"),
     "dme39": ("DME39F.f90", "DME39F90.h"),
 }
-ROUTINES = ("PRODRATES", "GETLINDRATECOEFF", "COMPTHERMODATA", "GETMOLARMASS")
+ROUTINES = ("PRODRATES", "GETLINDRATECOEFF", "COMPTHERMODATA", "GETMOLARMASS", "GETMUCOEFF", "GETKOVEREPS")
 INTRINSICS = {"EXP": "exp", "DLOG": "log", "DLOG10": "log10", "MAX": "fmax", "DSQRT": "sqrt", "LOG": "log"}
 
 
@@ -345,6 +346,94 @@ void ref_{mech}_rhs_batch(const double *sol, double p, double *rhs, int64_t ncel
       tmp = tmp - h[k] * r;
     }}
     rhs[{nspec} * ld + i] = tmp / cpmix;
+  }}
+}}
+""")
+    # finitechem_W + finitechem_density (finitechem.f90:65-74, :324-345), finitechem_viscosity
+    # (:351-406), finitechem_diffusivity (:412-461) with finitechem_omegamu (:467-487) and
+    # finitechem_Cp (:79-88), per cell in the reference's statement order over the transliterated
+    # getters and COMPTHERMODATA (called inside the species loop, as :428-432 does); Fortran's
+    # x**-0.5 / **0.5 / **0.25 are pow calls and (..)**2 a product.
+    out.append(f"""
+static double ref_{mech}_omegamu(double temp) {{
+  const double m1 = 3.3530622607, m2 = 2.53272006, m3 = 2.9024238575, m4 = 0.11186138893, m5 = 0.8662326188;
+  const double m6 = 1.3913958626, m7 = 3.158490576, m8 = 0.18973411754, m9 = 0.00018682962894;
+  double num = m1 + temp * (m2 + temp * (m3 + temp * m4));
+  double den = m5 + temp * (m6 + temp * (m7 + temp * (m8 + temp * m9)));
+  return num / den;
+}}
+static double ref_{mech}_w(const double *sc, double *W_sp) {{
+  double a = 0.0, b = 0.0;
+  for (int k = 0; k < {nspec}; ++k) {{
+    double t = fmin(fmax(sc[k], 0.0), 1.0);
+    a = a + t;
+  }}
+  for (int k = 0; k < {nspec}; ++k) {{
+    double t = fmin(fmax(sc[k], 0.0), 1.0);
+    b = b + t / W_sp[k];
+  }}
+  return a / b;
+}}
+void ref_{mech}_props_batch(const double *y, const double *Tin, int64_t ncells, int64_t ld, double P_thermo,
+                            const double *lewis, double *wmix, double *rho, double *visc, double *diff, int nthreads) {{
+  const double R_cst = 8314.34, Tmin = 50.0, Tmax = 5000.0;
+  double W_sp[{nspec}], mucoeff[{nspec}], kOverEps[{nspec}];
+  ref_{mech}_getmolarmass(W_sp);
+  ref_{mech}_getmucoeff(mucoeff);
+  ref_{mech}_getkovereps(kOverEps);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+  for (int64_t c = 0; c < ncells; ++c) {{
+    double sc[{nspec}], eta[{nspec}], cond[{nspec}], h_sp[{nspec}], Cp_sp[{nspec}];
+    double phi[{nspec}][{nspec}];
+    for (int k = 0; k < {nspec}; ++k) sc[k] = y[k * ld + c];
+    const double T = Tin[c];
+    const double W_mix = ref_{mech}_w(sc, W_sp);
+    if (wmix) wmix[c] = W_mix;
+    if (rho) rho[c] = P_thermo * W_mix / (R_cst * T);
+    double temp = fmin(fmax(T, Tmin), Tmax);
+    if (visc) {{
+      for (int n = 0; n < {nspec}; ++n) {{
+        double om = ref_{mech}_omegamu(temp * kOverEps[n]);
+        eta[n] = mucoeff[n] * sqrt(temp) / om;
+      }}
+      for (int k = 0; k < {nspec}; ++k)
+        for (int j = 0; j < {nspec}; ++j) {{
+          phi[k][j] = (1.0 / sqrt(8.0)) * pow(1.0 + (W_sp[k] / W_sp[j]), -0.5);
+          double temp1 = pow(eta[k] / eta[j], 0.5) * pow(W_sp[j] / W_sp[k], 0.25);
+          phi[k][j] = phi[k][j] * ((1.0 + temp1) * (1.0 + temp1));
+        }}
+      double sum_2 = 0.0;
+      for (int k = 0; k < {nspec}; ++k) {{
+        double sum_1 = 0.0;
+        for (int j = 0; j < {nspec}; ++j)
+          if (j != k) sum_1 = sum_1 + (sc[j] * W_mix * phi[k][j] / W_sp[j]);
+        sum_1 = sum_1 + sc[k] * W_mix / W_sp[k];
+        if (sc[k] > 0.0) sum_2 = sum_2 + (sc[k] * W_mix * eta[k] / (W_sp[k] * sum_1));
+      }}
+      visc[c] = sum_2;
+    }}
+    if (diff) {{
+      for (int n = 0; n < {nspec}; ++n) {{
+        double om = ref_{mech}_omegamu(temp * kOverEps[n]);
+        eta[n] = mucoeff[n] * sqrt(temp) / om;
+        ref_{mech}_compthermodata(h_sp, Cp_sp, &temp);
+        cond[n] = eta[n] * (Cp_sp[n] + 1.25 * R_cst / W_sp[n]);
+      }}
+      double sum_1 = 0.0, sum_2 = 0.0;
+      for (int n = 0; n < {nspec}; ++n) {{
+        sum_1 = sum_1 + (sc[n] * W_mix / (cond[n] * W_sp[n]));
+        sum_2 = sum_2 + (sc[n] * cond[n] * W_mix / W_sp[n]);
+      }}
+      double lambda = 0.5 * (sum_2 + (1.0 / sum_1));
+      ref_{mech}_compthermodata(h_sp, Cp_sp, &temp);
+      double Cp_mix = 0.0;
+      for (int n = 0; n < {nspec}; ++n) Cp_mix = Cp_mix + sc[n] * Cp_sp[n];
+      for (int n = 0; n < {nspec}; ++n) diff[n * ld + c] = (lambda / Cp_mix) / (lewis ? lewis[n] : 1.0);
+      diff[{nspec} * ld + c] = lambda / Cp_mix;
+    }}
   }}
 }}
 """)

@@ -6,7 +6,9 @@ module, and only as the checker or the timed CPU baseline. The product never imp
 * :class:`Oracle` loads a mechanism table (the JSON under ``tiger_nga_b200/mechanisms``),
   turns every literal into the double the reference binary would use (default-real literals
   rounded to float32, Makefile.in:23-24), and drives ``chem_oracle.c`` -- the table-driven
-  restatement of PRODRATES / GETLINDRATECOEFF / COMPTHERMODATA / finitechem_compute_rhs.
+  restatement of PRODRATES / GETLINDRATECOEFF / COMPTHERMODATA / finitechem_compute_rhs, and
+  ``props_oracle.c`` for the mixture properties (finitechem_W / _density / _viscosity /
+  _diffusivity).
 * :class:`Reference` drives ``oracle/_ref/libref_mech.so``, the reference's own Fortran
   mechanism routines transliterated statement by statement to C by ``oracle/f90_to_c.py``.
   It exists only where that library was built (it needs the reference tree to build).
@@ -33,7 +35,8 @@ REF_LIB = os.path.join(HERE, "_ref", "libref_mech.so")
 
 def build_oracle(force: bool = False) -> str:
     """Compile chem_oracle.c (and solver_oracle.c when present) with gcc + OpenMP."""
-    srcs = [os.path.join(HERE, f) for f in ("chem_oracle.c", "solver_oracle.c") if os.path.exists(os.path.join(HERE, f))]
+    srcs = [os.path.join(HERE, f) for f in ("chem_oracle.c", "solver_oracle.c", "props_oracle.c")
+            if os.path.exists(os.path.join(HERE, f))]
     newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(HERE, "orc_mech.h")])
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
         os.makedirs(os.path.dirname(LIB), exist_ok=True)
@@ -164,6 +167,8 @@ class Oracle:
             return out
 
         self.wmol = D([L(x) for x in tab["molar_mass"]])
+        self.mucoeff = D([L(x) for x in tab["mucoeff"]])
+        self.koveps = D([L(x) for x in tab["koveps"]])
         nu = np.zeros((ns, nslot))
         for k, terms in enumerate(tab["cdot"]):
             for sgn, c, r in terms:
@@ -205,6 +210,9 @@ class Oracle:
                                                  ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
         self.lib.orc_rates_batch.argtypes = [ctypes.POINTER(_Mech), ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
                                              ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int]
+        self.lib.orc_props_batch.argtypes = ([ctypes.POINTER(_Mech)] + [ctypes.c_void_p] * 5 +
+                                             [ctypes.c_int64, ctypes.c_int64, ctypes.c_double] +
+                                             [ctypes.c_void_p] * 4 + [ctypes.c_int])
 
     # ---- single cell --------------------------------------------------------------------
     def prodrates(self, C, T, P):
@@ -252,6 +260,21 @@ class Oracle:
         out = np.empty((self.nslot, sol.shape[1]))
         self.lib.orc_rates_batch(ctypes.byref(self.m), _p(sol), float(p), _p(out), sol.shape[1], sol.shape[1],
                                  sol.shape[1], int(nthreads))
+        return out
+
+    def props_batch(self, Y, T, p_thermo=101325.0, lewis=None, what=("wmix", "rho", "visc", "diff"), nthreads=0):
+        """finitechem_W / _density / _viscosity / _diffusivity (finitechem.f90:65-74, :324-461) over a
+        species-major batch: Y (N, ncells), T (ncells). Returns a dict of the requested outputs;
+        'diff' is (N+1, ncells): lambda/Cp_mix/Lewis_k per species, then lambda/Cp_mix."""
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        n = Y.shape[1]
+        out = {k: np.zeros((self.ns + 1, n) if k == "diff" else n) for k in what}
+        lw = None if lewis is None else np.ascontiguousarray(lewis, dtype=np.float64)
+        g = lambda k: _p(out[k]) if k in out else None  # noqa: E731
+        self.lib.orc_props_batch(ctypes.byref(self.m), _p(self.mucoeff), _p(self.koveps),
+                                 _p(lw) if lw is not None else None, _p(Y), _p(T), n, n, float(p_thermo),
+                                 g("wmix"), g("rho"), g("visc"), g("diff"), int(nthreads))
         return out
 
     def max_threads(self):
@@ -339,11 +362,34 @@ class Reference:
         self._th = getattr(self.lib, f"ref_{name}_compthermodata")
         self._mm = getattr(self.lib, f"ref_{name}_getmolarmass")
         self._rb = getattr(self.lib, f"ref_{name}_rhs_batch")
+        self._pb = getattr(self.lib, f"ref_{name}_props_batch", None)
         for f in (self._pr, self._th, self._mm, self._rb):
             f.restype = None
         mm = np.zeros(self.ns)
         self._mm(_p(mm))
         self.wmol = mm
+        if self._pb is not None:
+            self._pb.restype = None
+            self._pb.argtypes = ([ctypes.c_void_p] * 2 + [ctypes.c_int64, ctypes.c_int64, ctypes.c_double] +
+                                 [ctypes.c_void_p] * 5 + [ctypes.c_int])
+            self.mucoeff, self.koveps = np.zeros(self.ns), np.zeros(self.ns)
+            getattr(self.lib, f"ref_{name}_getmucoeff")(_p(self.mucoeff))
+            getattr(self.lib, f"ref_{name}_getkovereps")(_p(self.koveps))
+
+    def props_batch(self, Y, T, p_thermo=101325.0, lewis=None, what=("wmix", "rho", "visc", "diff"), nthreads=0):
+        """The reference's finitechem_W / _density / _viscosity / _diffusivity over the
+        transliterated getters; same outputs as :meth:`Oracle.props_batch`."""
+        if self._pb is None:
+            raise FileNotFoundError("oracle/_ref predates the property routines; rebuild it")
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        n = Y.shape[1]
+        out = {k: np.zeros((self.ns + 1, n) if k == "diff" else n) for k in what}
+        lw = None if lewis is None else np.ascontiguousarray(lewis, dtype=np.float64)
+        g = lambda k: _p(out[k]) if k in out else None  # noqa: E731
+        self._pb(_p(Y), _p(T), n, n, float(p_thermo), _p(lw) if lw is not None else None,
+                 g("wmix"), g("rho"), g("visc"), g("diff"), int(nthreads))
+        return out
 
     def rhs_batch(self, sol, p, nthreads=0):
         """finitechem_compute_rhs over a species-major batch, OpenMP over cells."""

@@ -119,6 +119,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_rates_autotune": (I, [V, V, L, L, D, ctypes.POINTER(TuneResult)]),
         "tng_substep_autotune": (I, [V, V, L, L, V, D, D, L, ctypes.POINTER(TuneResult)]),
         "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
+        "tng_chem_density": (I, [V, V, V, V, V, ctypes.POINTER(Extent), D, I]),
+        "tng_chem_transport": (I, [V, V, V, V, V, ctypes.POINTER(Extent), V, I, I]),
         "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
         "tng_mlp_destroy": (I, [V]),
         "tng_mlp_param_count": (L, [V]),
@@ -393,6 +395,80 @@ def _source_chemistry(self, RHO, SC, ext: dict, dt: float, p_mid: float, mask=No
     return st.as_dict()
 
 
+def _fortran_f64(*arrays):
+    for a in arrays:
+        if a is not None and not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous):
+            raise ValueError("arrays must be Fortran-ordered float64 NumPy arrays")
+
+
+def _density(self, RHO, SC, ext: dict, p_thermo: float, mask=None, W=None):
+    """finitechem_density (finitechem.f90:324-345) on the solver's own arrays (NumPy, Fortran
+    order): RHO (and W_mix into W when given) for every unmasked cell of the padded block."""
+    _fortran_f64(RHO, SC, W)
+    e = Extent(**ext)
+    mk = None if mask is None else np.asfortranarray(mask, dtype=np.int32)
+    _check(self.lib.tng_chem_density(self.h, RHO.ctypes.data if RHO is not None else None,
+                                     W.ctypes.data if W is not None else None, SC.ctypes.data,
+                                     mk.ctypes.data if mk is not None else None, ctypes.byref(e), float(p_thermo),
+                                     TNG_HOST_PTRS), "tng_chem_density")
+
+
+def _transport(self, SC, ext: dict, VISC=None, DIFF=None, mask=None, lewis=None, isc_zmix: int = 0):
+    """finitechem_viscosity + finitechem_diffusivity (finitechem.f90:351-461) on the solver's own
+    arrays: VISC shaped like RHO, DIFF shaped like SC (species, T and ZMIX columns written)."""
+    _fortran_f64(SC, VISC, DIFF)
+    e = Extent(**ext)
+    mk = None if mask is None else np.asfortranarray(mask, dtype=np.int32)
+    lw = None if lewis is None else np.ascontiguousarray(lewis, dtype=np.float64)
+    _check(self.lib.tng_chem_transport(self.h, VISC.ctypes.data if VISC is not None else None,
+                                       DIFF.ctypes.data if DIFF is not None else None, SC.ctypes.data,
+                                       mk.ctypes.data if mk is not None else None, ctypes.byref(e),
+                                       lw.ctypes.data if lw is not None else None, int(isc_zmix), TNG_HOST_PTRS),
+           "tng_chem_transport")
+
+
+def batch_extent(ncells: int, nspecies: int) -> Extent:
+    """The extent that presents a species-major device batch [Y_1..Y_N, T] (shape (N+1, ncells))
+    as a one-row Fortran block: nscalar N+1, species at 1..N, T at N+1."""
+    return Extent(imino=1, imaxo=ncells, jmino=1, jmaxo=1, kmino=1, kmaxo=1, imin=1, imax=ncells, jmin=1, jmax=1,
+                  kmin=1, kmax=1, nscalar=nspecies + 1, isc_sc=1, isc_T=nspecies + 1, isc_H2O=0, isc_CO=0, isc_CO2=0)
+
+
+def _mixture_props(self, sc, p_thermo: float | None = None, visc: bool = False, diff: bool = False, lewis=None,
+                   out=None):
+    """Mixture properties of a species-major CUDA batch ``sc`` = [Y_1..Y_N, T] (float64, shape
+    (N+1, ncells), unit stride along cells): with p_thermo, 'rho' and 'wmix' (tng_chem_density);
+    with visc / diff, 'visc' (ncells) and 'diff' ((N+1, ncells): lambda/Cp_mix/Lewis_k, then
+    lambda/Cp_mix) from tng_chem_transport. ``out`` may supply the output tensors."""
+    import torch
+
+    ns = self.nspecies
+    if not (sc.is_cuda and sc.dtype == torch.float64 and sc.dim() == 2 and sc.shape[0] == ns + 1 and sc.is_contiguous()):
+        raise ValueError(f"sc must be a contiguous CUDA float64 tensor of shape ({ns + 1}, ncells)")
+    n = sc.shape[1]
+    e = batch_extent(n, ns)
+    out = dict(out or {})
+    sst = self.torch_stream()
+    sst.wait_stream(torch.cuda.current_stream(sc.device))
+    if p_thermo is not None:
+        for k in ("rho", "wmix"):
+            out.setdefault(k, torch.empty(n, dtype=torch.float64, device=sc.device))
+        _check(self.lib.tng_chem_density(self.h, out["rho"].data_ptr(), out["wmix"].data_ptr(), sc.data_ptr(), None,
+                                         ctypes.byref(e), float(p_thermo), TNG_DEVICE_PTRS), "tng_chem_density")
+    if visc or diff:
+        if visc:
+            out.setdefault("visc", torch.empty(n, dtype=torch.float64, device=sc.device))
+        if diff:
+            out.setdefault("diff", torch.empty((ns + 1, n), dtype=torch.float64, device=sc.device))
+        lw = None if lewis is None else np.ascontiguousarray(lewis, dtype=np.float64)
+        _check(self.lib.tng_chem_transport(self.h, out["visc"].data_ptr() if visc else None,
+                                           out["diff"].data_ptr() if diff else None, sc.data_ptr(), None,
+                                           ctypes.byref(e), lw.ctypes.data if lw is not None else None, 0,
+                                           TNG_DEVICE_PTRS), "tng_chem_transport")
+    torch.cuda.current_stream(sc.device).wait_stream(sst)
+    return out
+
+
 def _substep_static(self, state, dt, p: float) -> int:
     """tng_substep_batch_static on a CUDA tensor (allocates nothing on the device during the
     call; at most 262144 cells; calls must not overlap). Returns the number of failed cells."""
@@ -487,6 +563,9 @@ def _autotune(self, state, dt=None, p: float = 101325.0, kind: str = "substep", 
 FiniteChem._tuning_key = _tuning_key
 FiniteChem.autotune = _autotune
 FiniteChem.source_chemistry = _source_chemistry
+FiniteChem.density = _density
+FiniteChem.transport = _transport
+FiniteChem.mixture_props = _mixture_props
 FiniteChem.substep_static = _substep_static
 FiniteChem.substep = _substep
 FiniteChem.solver_rhs_jac = _solver_rhs_jac

@@ -318,6 +318,116 @@ class _Gen:
             o.append(f"      cpm = fma(y, cpk, cpm);")
             o.append(f"      tmp = fma(-hk, rk, tmp); }}")
 
+    # ---------------------------------------------------------------- mixture properties
+    def props(self) -> str:
+        """Per-cell mixture properties around the substep (finitechem.f90:65-74, :324-487).
+
+        ``mix_w``: W_mix of the clipped mass fractions (finitechem_W). ``transport``: the species
+        viscosities eta_k = mucoeff_k sqrt(T) / Omega(T kOverEps_k) (finitechem_omegamu's rational
+        fit), then
+        * the conductivity sums, Cp_mix and lambda/Cp_mix of finitechem_diffusivity;
+        * Wilke's mixture viscosity of finitechem_viscosity. Its pair factor
+          phi_kj = A_kj (1 + sqrt(eta_k/eta_j) B_kj)^2, A_kj = (1 + W_k/W_j)^-1/2 / sqrt(8),
+          B_kj = (W_j/W_k)^1/4, is expanded as A + 2AB s_k r_j + AB^2 s_k^2 r_j^2 (s = sqrt(eta),
+          r = 1/s), so that sum_j x_j phi_kj becomes three dot products of per-cell vectors
+          (u = Y/W, v = u r, w = v r) with constant matrices -- three FMAs per pair with the
+          matrix entries as constant-bank operands, instead of the reference's three pow calls.
+          W_mix cancels between sum_1 and sum_2 and is left out. The per-cell vectors live in
+          shared memory (stride B, one slice per thread); rows are processed in tiles of six so
+          that each vector load feeds eighteen FMAs; ``TNG_SCHED_FENCE`` (an empty asm with a
+          memory clobber) every two columns bounds how many of a tile's loads are hoisted.
+        """
+        m32, m64 = self.m32, self.m64
+        ns = self.ns
+        o: list[str] = []
+        W32, W64 = m32.wmol, m64.wmol
+        rc = 8314.34  # R_cst (finitechem.f90:15), a double literal
+        om = {i + 1: v for i, v in enumerate((3.3530622607, 2.53272006, 2.9024238575, 0.11186138893, 0.8662326188,
+                                              1.3913958626, 3.158490576, 0.18973411754, 0.00018682962894))}
+        o.append("  template <int LM>")
+        o.append("  __device__ static __forceinline__ double mix_w(const double* __restrict__ y) {")
+        o.append("    double st = 0.0, sw = 0.0;")
+        for k in range(ns):
+            o.append(f"    {{ const double t = fmin(fmax(y[{k}], 0.0), 1.0); st = st + t; "
+                     f"sw = fma(t, {_lm(1.0 / W32[k], 1.0 / W64[k])}, sw); }}")
+        o.append("    return st / sw;")
+        o.append("  }")
+
+        # the species loop of transport is a runtime loop over per-species records in constant
+        # memory (props_records): unrolled, the scheduler would keep every species' fit live at once
+        o.append("  template <int LM, bool VISC, bool DIFF, int B>")
+        o.append("  __device__ static __forceinline__ void transport(const double* __restrict__ y, long long ldy, double T,"
+                 " double* __restrict__ sv, double* visc, double* lam_cp) {")
+        o.append("    const double Tc = fmin(fmax(T, 50.0), 5000.0);  // Tmin, Tmax (finitechem.f90:7-8)")
+        o.append("    const double sq = sqrt(Tc);")
+        o.append(f"    const int toff = Tc > {_lm(m32.tmid, m64.tmid)} ? 4 : 10;")
+        o.append("    double s1 = 0.0, s2 = 0.0, cpm = 0.0, st = 0.0, sw = 0.0;")
+        o.append("#pragma unroll 1")
+        o.append(f"    for (int k = 0; k < {ns}; ++k) {{")
+        o.append(f"      const double* q = {self.name}_props_records[LM] + 16 * k;")
+        o.append("      const double yk = __ldg(y + k * ldy);")
+        o.append("      const double x = Tc * q[0];")
+        o.append(f"      const double num = fma(x, fma(x, fma(x, {_d(om[4])}, {_d(om[3])}), {_d(om[2])}), {_d(om[1])});")
+        o.append(f"      const double den = fma(x, fma(x, fma(x, fma(x, {_d(om[9])}, {_d(om[8])}), {_d(om[7])}), "
+                 f"{_d(om[6])}), {_d(om[5])});")
+        o.append("      const double e = q[1] * sq * den / num;  // mucoeff sqrt(T) / Omega(T kOverEps)")
+        o.append("      const double u = yk * q[2];")
+        o.append("      if (VISC) { const double r = rsqrt(e); const double v = u * r; "
+                 "sv[4 * k * B] = u; sv[(4 * k + 1) * B] = v; sv[(4 * k + 2) * B] = v * r; sv[(4 * k + 3) * B] = e * r; }")
+        o.append("      if (DIFF) {")
+        o.append("        const double* a = q + toff;")
+        o.append("        const double cp = a[0] * (a[1] + Tc * (a[2] + Tc * (a[3] + Tc * (a[4] + Tc * a[5]))));")
+        o.append("        const double c = e * (cp + q[3]);")
+        o.append("        s1 = s1 + u / c; s2 = fma(u, c, s2); cpm = fma(yk, cp, cpm);")
+        o.append("        const double t = fmin(fmax(yk, 0.0), 1.0); st = st + t; sw = fma(t, q[2], sw);")
+        o.append("      }")
+        o.append("    }")
+        o.append("    if (DIFF) { const double wmix = st / sw; *lam_cp = (0.5 * (wmix * s2 + 1.0 / (wmix * s1))) / cpm; }")
+        o.append("    if (VISC) {")
+        o.append("      double acc = 0.0;")
+        for k0 in range(0, ns, 6):
+            rows = list(range(k0, min(ns, k0 + 6)))
+            o.append("      {")
+            o.append("        " + " ".join(f"double a{k} = 0.0, b{k} = 0.0, c{k} = 0.0;" for k in rows))
+            for j in range(ns):
+                o.append(f"        {{ const double u = sv[{4 * j} * B], v = sv[{4 * j + 1} * B], w = sv[{4 * j + 2} * B];")
+                for k in rows:
+                    if k == j:
+                        continue
+                    a32 = (1.0 / math.sqrt(8.0)) * (1.0 + W32[k] / W32[j]) ** -0.5
+                    a64 = (1.0 / math.sqrt(8.0)) * (1.0 + W64[k] / W64[j]) ** -0.5
+                    b32 = (W32[j] / W32[k]) ** 0.25
+                    b64 = (W64[j] / W64[k]) ** 0.25
+                    o.append(f"          a{k} = fma({_lm(a32, a64)}, u, a{k}); b{k} = fma({_lm(2.0 * a32 * b32, 2.0 * a64 * b64)}, v, b{k}); "
+                             f"c{k} = fma({_lm(a32 * b32 * b32, a64 * b64 * b64)}, w, c{k});")
+                o.append("        }")
+                if j % 2 == 1:
+                    o.append("        TNG_SCHED_FENCE();")
+            for k in rows:
+                o.append(f"        {{ const double uk = sv[{4 * k} * B], s = sv[{4 * k + 3} * B];")
+                o.append(f"          const double t = uk * (s * s) / (uk + fma(s, fma(s, c{k}, b{k}), a{k}));")
+                o.append("          acc += uk > 0.0 ? t : 0.0; }")
+            o.append("      }")
+        o.append("      *visc = acc;")
+        o.append("    }")
+        o.append("  }")
+        return "\n".join(o)
+
+    def props_records(self) -> str:
+        """Per-species records of ``transport``, [literal mode][species x 16]: kOverEps, mucoeff,
+        1/W, 1.25 R_cst/W (finitechem.f90:431), then the NASA cp coefficients c0, b1..b5 of the
+        high and of the low range."""
+        rc = 8314.34
+
+        def rec(m, k):
+            return ([m.koveps[k], m.mucoeff[k], 1.0 / m.wmol[k], 1.25 * rc / m.wmol[k]]
+                    + [m.th_hi[k][i] for i in (0, 7, 8, 9, 10, 11)] + [m.th_lo[k][i] for i in (0, 7, 8, 9, 10, 11)])
+        rows = []
+        for mm in (self.m32, self.m64):
+            rows.append("{" + ", ".join(_d(v) for k in range(self.ns) for v in rec(mm, k)) + "}")
+        return (f"// per-species records of Mech_{self.name}::transport, [literal mode][species][16]\n"
+                f"static __constant__ double {self.name}_props_records[2][{self.ns * 16}] = {{{', '.join(rows)}}};")
+
     def header(self) -> str:
         m32, m64 = self.m32, self.m64
         cls = f"Mech_{self.name}"
@@ -326,6 +436,7 @@ class _Gen:
                "#pragma once",
                '#include "tng_device.cuh"',
                "namespace tng {",
+               self.props_records(),
                f"struct {cls} {{",
                f"  static constexpr int NS = {self.ns};",
                f"  static constexpr int NSLOT = {self.nslot};",
@@ -333,6 +444,7 @@ class _Gen:
                f'  static constexpr const char* NAME = "{self.name}";']
         out.append(self.rhs("fp64", dump=True))
         out.append(self.rhs("mixed", dump=True))
+        out.append(self.props())
         out.append("};")
         # host-side info
         names = ", ".join(f'"{s}"' for s in m32.species)

@@ -50,6 +50,24 @@ inline unsigned rhs_grid(long long n, int block) {
   return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
+// Per-cell mixture properties (csrc/props_kernels.cuh): which outputs, and where.
+enum { TNG_PROPS_DENSITY = 1, TNG_PROPS_VISC = 2, TNG_PROPS_DIFF = 4 };
+struct PropsArgs {
+  const double* y;         // species k of cell c at y[k*ldy + c]
+  long long ldy;
+  const double* T;         // temperature of cell c
+  const int* mask;         // mask(i,j) of the padded block (nxo x nyo), nullable
+  long long nxo, nyo;
+  long long n;             // cells
+  double p;                // thermodynamic pressure (density)
+  double *rho, *wmix;      // density outputs, nullable
+  double* visc;            // viscosity output
+  double* diff;            // species diffusivities, species k at diff[k*ldd + c]
+  long long ldd;
+  double *diff_T, *diff_Z; // temperature / mixture-fraction diffusivity (diff_Z nullable)
+  const double* inv_lewis; // device, NS reciprocal Lewis numbers
+};
+
 struct MechOps {
   const char* name;
   int ns, nslot, nm, nelem;
@@ -65,6 +83,8 @@ struct MechOps {
   const double* sv_hd[2];  // hot doubles per literal mode
   const int* sv_hi;        // hot ints
   const int* sv_ci;        // cold ints
+  // mixture properties: lm 0/1, what = TNG_PROPS_* bits (density alone, or viscosity and/or diffusivity)
+  cudaError_t (*props)(int lm, int what, const PropsArgs& a, int sm_count, cudaStream_t st);
 };
 
 // Kernel variants of the rate evaluation (the autotuner's choices): 0 = plain, 1 = block

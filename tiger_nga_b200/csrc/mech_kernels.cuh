@@ -1,6 +1,7 @@
 // Builds the operation table of one generated mechanism.
 #pragma once
 #include "kernels.cuh"
+#include "props_kernels.cuh"
 
 namespace tng {
 
@@ -25,6 +26,7 @@ MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int
   o.sv_hd[1] = hd1;
   o.sv_hi = hi;
   o.sv_ci = ci;
+  o.props = &launch_props<Mech>;
   return o;
 }
 

@@ -6,6 +6,9 @@
 // Literal-mode select: LM == 0 keeps the reference build's literal kinds (default-real
 // literals rounded to float32), LM == 1 reads every literal as a double.
 #define TNG_LM(ref, dbl) (LM ? (dbl) : (ref))
+// Scheduling fence for generated straight-line code: memory operations are not moved across it,
+// which bounds how many loads the compiler hoists (and so the registers they hold).
+#define TNG_SCHED_FENCE() asm volatile("" ::: "memory")
 
 namespace tng {
 

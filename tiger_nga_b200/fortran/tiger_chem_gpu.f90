@@ -7,11 +7,15 @@
 ! finitechem_source_chemistry_gpu where combustion_source_scalar_full calls
 ! finitechem_source_chemistry (combustion.f90:1047-1049). The mechanism is chosen by name at
 ! run time instead of by the linked *F.f90 file (combustion/Makefile:3-5).
+! The mixture-property routines around the substep have drop-ins too: finitechem_density_gpu
+! (for finitechem_density, combustion.f90:1098 and :1149), finitechem_viscosity_gpu
+! (:1197) and finitechem_diffusivity_gpu (:1305), or finitechem_transport_gpu for both.
 module tiger_chem_gpu
   use iso_c_binding
   implicit none
   private
   public :: tiger_chem_gpu_init, finitechem_source_chemistry_gpu, tiger_chem_gpu_finalize
+  public :: finitechem_density_gpu, finitechem_viscosity_gpu, finitechem_diffusivity_gpu, finitechem_transport_gpu
   public :: tng_cfg, tng_extent, tng_default_cfg, tng_chem_create, tng_chem_destroy, tng_chem_substep
   public :: tng_prodrates_batch, tng_last_error
 
@@ -65,6 +69,28 @@ module tiger_chem_gpu
       integer(c_int), value :: flags
       type(c_ptr), value :: stats
     end function tng_chem_substep
+
+    integer(c_int) function tng_chem_density(h, rho, wmix, sc, mask, ext, p_thermo, flags) &
+         bind(C, name='tng_chem_density')
+      import :: c_int, c_double, c_ptr, tng_extent
+      type(c_ptr), value :: h, rho, wmix
+      real(c_double), dimension(*), intent(in) :: sc
+      integer(c_int), dimension(*), intent(in) :: mask
+      type(tng_extent), intent(in) :: ext
+      real(c_double), value :: p_thermo
+      integer(c_int), value :: flags
+    end function tng_chem_density
+
+    integer(c_int) function tng_chem_transport(h, visc, diff, sc, mask, ext, lewis, isc_zmix, flags) &
+         bind(C, name='tng_chem_transport')
+      import :: c_int, c_double, c_ptr, tng_extent
+      type(c_ptr), value :: h, visc, diff
+      real(c_double), dimension(*), intent(in) :: sc
+      integer(c_int), dimension(*), intent(in) :: mask
+      type(tng_extent), intent(in) :: ext
+      type(c_ptr), value :: lewis
+      integer(c_int), value :: isc_zmix, flags
+    end function tng_chem_transport
 
     integer(c_int) function tng_prodrates_batch(h, sol, rhs, ncells, ld, p, flags) bind(C, name='tng_prodrates_batch')
       import :: c_int, c_int64_t, c_double, c_ptr
@@ -129,6 +155,60 @@ contains
          0.5_WP * (P_thermo + P_thermo_old), HR_gp, chemsrc_gp, TNG_HOST_PTRS, c_null_ptr)
     if (rc /= TNG_OK) call report('tng_chem_substep')
   end subroutine finitechem_source_chemistry_gpu
+
+  ! The padded block of this rank with the species / temperature columns of SC.
+  function block_extent() result(ext)
+    use finitechem
+    type(tng_extent) :: ext
+    ext = tng_extent(imino_, imaxo_, jmino_, jmaxo_, kmino_, kmaxo_, imin_, imax_, jmin_, jmax_, kmin_, kmax_, &
+         nscalar, isc_sc, isc_T, 0, 0, 0)
+  end function block_extent
+
+  ! Same effect as finitechem_density (finitechem.f90:324-345): RHO of every unmasked cell of
+  ! the padded block from the equation of state.
+  subroutine finitechem_density_gpu
+    use finitechem
+    use masks
+    integer(c_int) :: rc
+    rc = tng_chem_density(handle, c_loc(RHO), c_null_ptr, SC, mask(imino_:imaxo_, jmino_:jmaxo_), block_extent(), &
+         P_thermo, TNG_HOST_PTRS)
+    if (rc /= TNG_OK) call report('tng_chem_density')
+  end subroutine finitechem_density_gpu
+
+  ! Same effect as finitechem_viscosity (finitechem.f90:351-406), border update included.
+  subroutine finitechem_viscosity_gpu
+    use finitechem
+    use masks
+    integer(c_int) :: rc
+    rc = tng_chem_transport(handle, c_loc(VISC), c_null_ptr, SC, mask(imino_:imaxo_, jmino_:jmaxo_), block_extent(), &
+         c_loc(Lewis), 0_c_int, TNG_HOST_PTRS)
+    if (rc /= TNG_OK) call report('tng_chem_transport')
+    call boundary_update_border(VISC, '+', 'ym')
+  end subroutine finitechem_viscosity_gpu
+
+  ! Same effect as finitechem_diffusivity (finitechem.f90:412-461), border update included.
+  subroutine finitechem_diffusivity_gpu
+    use finitechem
+    use masks
+    integer(c_int) :: rc
+    rc = tng_chem_transport(handle, c_null_ptr, c_loc(DIFF), SC, mask(imino_:imaxo_, jmino_:jmaxo_), block_extent(), &
+         c_loc(Lewis), int(isc_ZMIX, c_int), TNG_HOST_PTRS)
+    if (rc /= TNG_OK) call report('tng_chem_transport')
+    call boundary_update_border(DIFF, '+', 'ym')
+  end subroutine finitechem_diffusivity_gpu
+
+  ! Both of the above in one pass over SC (combustion_prestep calls them back to back,
+  ! combustion.f90:686-687).
+  subroutine finitechem_transport_gpu
+    use finitechem
+    use masks
+    integer(c_int) :: rc
+    rc = tng_chem_transport(handle, c_loc(VISC), c_loc(DIFF), SC, mask(imino_:imaxo_, jmino_:jmaxo_), &
+         block_extent(), c_loc(Lewis), int(isc_ZMIX, c_int), TNG_HOST_PTRS)
+    if (rc /= TNG_OK) call report('tng_chem_transport')
+    call boundary_update_border(VISC, '+', 'ym')
+    call boundary_update_border(DIFF, '+', 'ym')
+  end subroutine finitechem_transport_gpu
 
   subroutine report(what)
     character(len=*), intent(in) :: what

@@ -99,6 +99,9 @@ class Mechanism:
         self.nm = tab["n_thirdbody"]
         self.species = list(tab["species"])
         self.wmol = np.array([L(x) for x in tab["molar_mass"]])
+        # transport fits (GETMUCOEFF / GETKOVEREPS, e.g. HYDROGENF.f90:453-497)
+        self.mucoeff = np.array([L(x) for x in tab["mucoeff"]])
+        self.koveps = np.array([L(x) for x in tab["koveps"]])
         self.rgas = L(tab["rgas"])
         self.tmid = L(tab["thermo"]["tmid"])
         self.third_body = [[(s, L(c)) for s, c in terms] for terms in tab["third_body"]]
