@@ -327,34 +327,37 @@ class _Gen:
         fit), then
         * the conductivity sums, Cp_mix and lambda/Cp_mix of finitechem_diffusivity;
         * Wilke's mixture viscosity of finitechem_viscosity. Its pair factor
-          phi_kj = A_kj (1 + sqrt(eta_k/eta_j) B_kj)^2, A_kj = (1 + W_k/W_j)^-1/2 / sqrt(8),
-          B_kj = (W_j/W_k)^1/4, is expanded as A + 2AB s_k r_j + AB^2 s_k^2 r_j^2 (s = sqrt(eta),
-          r = 1/s), so that sum_j x_j phi_kj becomes three dot products of per-cell vectors
-          (u = Y/W, v = u r, w = v r) with constant matrices -- three FMAs per pair with the
-          matrix entries as constant-bank operands, instead of the reference's three pow calls.
-          W_mix cancels between sum_1 and sum_2 and is left out. The per-cell vectors live in
-          shared memory (stride B, one slice per thread); rows are processed in tiles of six so
-          that each vector load feeds eighteen FMAs; ``TNG_SCHED_FENCE`` (an empty asm with a
-          memory clobber) every two columns bounds how many of a tile's loads are hoisted.
+          phi_kj = A_kj (1 + sqrt(eta_k/eta_j) (W_j/W_k)^1/4)^2, A_kj = (1 + W_k/W_j)^-1/2 / sqrt(8),
+          is rewritten with q = W^1/4 as A_kj (1 + sig_k rho_j)^2, rho = q/sqrt(eta), sig = 1/rho,
+          so that sum_j x_j phi_kj = A.u + 2 sig_k A.(u rho) + sig_k^2 A.(u rho^2):
+          three dot products of per-cell vectors with ONE constant matrix A (zero diagonal: the
+          reference's j /= k), three FMAs per pair instead of the reference's three pow calls.
+          W_mix cancels between sum_1 and sum_2 and is left out, and with rho_k = v_k/u_k,
+          rho_k^2 = w_k/u_k row k's term u_k eta_k / sum_1 becomes
+          u_k^2 q_k^2 / (w_k (u_k + A.u) + 2 v_k A.(u rho) + u_k A.(u rho^2)): one division. The
+          per-cell vectors u, v = u rho, w = v rho live in shared memory (stride B, one slice per
+          thread); rows run in tiles of up to 13 (a runtime loop, A read from constant memory at a
+          warp-uniform address), so each vector load feeds up to 39 FMAs and the code stays
+          small enough for the instruction cache.
         """
         m32, m64 = self.m32, self.m64
         ns = self.ns
         o: list[str] = []
         W32, W64 = m32.wmol, m64.wmol
-        rc = 8314.34  # R_cst (finitechem.f90:15), a double literal
         om = {i + 1: v for i, v in enumerate((3.3530622607, 2.53272006, 2.9024238575, 0.11186138893, 0.8662326188,
                                               1.3913958626, 3.158490576, 0.18973411754, 0.00018682962894))}
         o.append("  template <int LM>")
-        o.append("  __device__ static __forceinline__ double mix_w(const double* __restrict__ y) {")
+        o.append("  __device__ static __forceinline__ double mix_w(const double* __restrict__ y, long long ld) {")
         o.append("    double st = 0.0, sw = 0.0;")
-        for k in range(ns):
-            o.append(f"    {{ const double t = fmin(fmax(y[{k}], 0.0), 1.0); st = st + t; "
-                     f"sw = fma(t, {_lm(1.0 / W32[k], 1.0 / W64[k])}, sw); }}")
+        o.append("#pragma unroll 4")
+        o.append(f"    for (int k = 0; k < {ns}; ++k) {{")
+        o.append("      const double t = fmin(fmax(__ldcs(y + k * ld), 0.0), 1.0);")
+        o.append(f"      st = st + t; sw = fma(t, {self.name}_props_records[LM][19 * k + 2], sw);")
+        o.append("    }")
         o.append("    return st / sw;")
         o.append("  }")
-
-        # the species loop of transport is a runtime loop over per-species records in constant
-        # memory (props_records): unrolled, the scheduler would keep every species' fit live at once
+        # the species loop is a runtime loop over per-species records in constant memory
+        # (props_records): unrolled, the scheduler would keep every species' fit live at once
         o.append("  template <int LM, bool VISC, bool DIFF, int B>")
         o.append("  __device__ static __forceinline__ void transport(const double* __restrict__ y, long long ldy, double T,"
                  " double* __restrict__ sv, double* visc, double* lam_cp) {")
@@ -362,18 +365,26 @@ class _Gen:
         o.append("    const double sq = sqrt(Tc);")
         o.append(f"    const int toff = Tc > {_lm(m32.tmid, m64.tmid)} ? 4 : 10;")
         o.append("    double s1 = 0.0, s2 = 0.0, cpm = 0.0, st = 0.0, sw = 0.0;")
-        o.append("#pragma unroll 1")
+        o.append("    // stage the mass fractions in this thread's shared-memory slice first (all loads in")
+        o.append("    // flight at once; the species loop below would otherwise wait on each in turn)")
+        o.append("    constexpr int SV = VISC ? 3 : 1;")
+        o.append("#pragma unroll")
+        o.append(f"    for (int k = 0; k < {ns}; ++k) sv[SV * k * B] = __ldcs(y + k * ldy);")
+        o.append("#pragma unroll 4  // four species' dependent chains (fit, division, rsqrt) interleaved")
         o.append(f"    for (int k = 0; k < {ns}; ++k) {{")
-        o.append(f"      const double* q = {self.name}_props_records[LM] + 16 * k;")
-        o.append("      const double yk = __ldg(y + k * ldy);")
+        o.append(f"      const double* q = {self.name}_props_records[LM] + 19 * k;")
+        o.append("      const double yk = sv[SV * k * B];")
         o.append("      const double x = Tc * q[0];")
         o.append(f"      const double num = fma(x, fma(x, fma(x, {_d(om[4])}, {_d(om[3])}), {_d(om[2])}), {_d(om[1])});")
         o.append(f"      const double den = fma(x, fma(x, fma(x, fma(x, {_d(om[9])}, {_d(om[8])}), {_d(om[7])}), "
                  f"{_d(om[6])}), {_d(om[5])});")
         o.append("      const double e = q[1] * sq * den / num;  // mucoeff sqrt(T) / Omega(T kOverEps)")
         o.append("      const double u = yk * q[2];")
-        o.append("      if (VISC) { const double r = rsqrt(e); const double v = u * r; "
-                 "sv[4 * k * B] = u; sv[(4 * k + 1) * B] = v; sv[(4 * k + 2) * B] = v * r; sv[(4 * k + 3) * B] = e * r; }")
+        o.append("      if (VISC) {  // u, u rho, u rho^2 with rho = q/sqrt(eta)")
+        o.append("        const double r = rsqrt(e) * q[16];")
+        o.append("        const double v = u * r;")
+        o.append("        sv[3 * k * B] = u; sv[(3 * k + 1) * B] = v; sv[(3 * k + 2) * B] = v * r;")
+        o.append("      }")
         o.append("      if (DIFF) {")
         o.append("        const double* a = q + toff;")
         o.append("        const double cp = a[0] * (a[1] + Tc * (a[2] + Tc * (a[3] + Tc * (a[4] + Tc * a[5]))));")
@@ -383,50 +394,83 @@ class _Gen:
         o.append("      }")
         o.append("    }")
         o.append("    if (DIFF) { const double wmix = st / sw; *lam_cp = (0.5 * (wmix * s2 + 1.0 / (wmix * s1))) / cpm; }")
+        R, nrow = self.wilke_tile()
         o.append("    if (VISC) {")
         o.append("      double acc = 0.0;")
-        for k0 in range(0, ns, 6):
-            rows = list(range(k0, min(ns, k0 + 6)))
-            o.append("      {")
-            o.append("        " + " ".join(f"double a{k} = 0.0, b{k} = 0.0, c{k} = 0.0;" for k in rows))
-            for j in range(ns):
-                o.append(f"        {{ const double u = sv[{4 * j} * B], v = sv[{4 * j + 1} * B], w = sv[{4 * j + 2} * B];")
-                for k in rows:
-                    if k == j:
-                        continue
-                    a32 = (1.0 / math.sqrt(8.0)) * (1.0 + W32[k] / W32[j]) ** -0.5
-                    a64 = (1.0 / math.sqrt(8.0)) * (1.0 + W64[k] / W64[j]) ** -0.5
-                    b32 = (W32[j] / W32[k]) ** 0.25
-                    b64 = (W64[j] / W64[k]) ** 0.25
-                    o.append(f"          a{k} = fma({_lm(a32, a64)}, u, a{k}); b{k} = fma({_lm(2.0 * a32 * b32, 2.0 * a64 * b64)}, v, b{k}); "
-                             f"c{k} = fma({_lm(a32 * b32 * b32, a64 * b64 * b64)}, w, c{k});")
-                o.append("        }")
-                if j % 2 == 1:
-                    o.append("        TNG_SCHED_FENCE();")
-            for k in rows:
-                o.append(f"        {{ const double uk = sv[{4 * k} * B], s = sv[{4 * k + 3} * B];")
-                o.append(f"          const double t = uk * (s * s) / (uk + fma(s, fma(s, c{k}, b{k}), a{k}));")
-                o.append("          acc += uk > 0.0 ? t : 0.0; }")
-            o.append("      }")
+        o.append("#pragma unroll 1")
+        o.append(f"      for (int k0 = 0; k0 < {ns}; k0 += {R}) {{")
+        o.append(f"        const double* A = {self.name}_wilke[LM] + k0 * {ns};")
+        o.append("        " + " ".join(f"double a{r} = 0.0, b{r} = 0.0, c{r} = 0.0;" for r in range(R)))
+
+        def loads(jj):
+            o.append(f"        const double u{jj} = sv[{3 * jj} * B], v{jj} = sv[{3 * jj + 1} * B], "
+                     f"w{jj} = sv[{3 * jj + 2} * B];")
+            o.append("        const double " + ", ".join(f"m{jj}_{r} = A[{r * ns + jj}]" for r in range(R)) + ";")
+
+        # software-pipelined columns: column j+1's loads are issued before column j's FMAs, and
+        # a scheduling fence keeps the compiler from hoisting further ahead (registers)
+        loads(0)
+        for jj in range(ns):
+            if jj + 1 < ns:
+                loads(jj + 1)
+            o.append("        TNG_SCHED_FENCE();")
+            for r in range(R):
+                o.append(f"        a{r} = fma(m{jj}_{r}, u{jj}, a{r}); b{r} = fma(m{jj}_{r}, v{jj}, b{r}); "
+                         f"c{r} = fma(m{jj}_{r}, w{jj}, c{r});")
+        for r in range(R):
+            o.append(f"        if (k0 + {r} < {ns}) {{")
+            o.append(f"          const int k = k0 + {r};")
+            o.append("          const double uk = sv[3 * k * B];")
+            o.append("          // u eta / sum_1 with eta = q^2 / rho^2, rho = v/u, rho^2 = w/u (rows with u <= 0 add nothing)")
+            o.append("          if (uk > 0.0) {")
+            o.append("            const double vk = sv[(3 * k + 1) * B], wk = sv[(3 * k + 2) * B];")
+            o.append(f"            acc += uk * uk * {self.name}_props_records[LM][19 * k + 18] / "
+                     f"fma(wk, uk + a{r}, fma(2.0 * b{r}, vk, c{r} * uk));")
+            o.append("          }")
+            o.append("        }")
+        o.append("      }")
         o.append("      *visc = acc;")
         o.append("    }")
         o.append("  }")
         return "\n".join(o)
 
+    def wilke_tile(self):
+        """Rows per tile of the Wilke sum (at most 13, three accumulators each) and the padded
+        row count of the matrix."""
+        ntiles = -(-self.ns // 13)
+        R = -(-self.ns // ntiles)
+        return R, R * ntiles
+
     def props_records(self) -> str:
-        """Per-species records of ``transport``, [literal mode][species x 16]: kOverEps, mucoeff,
-        1/W, 1.25 R_cst/W (finitechem.f90:431), then the NASA cp coefficients c0, b1..b5 of the
-        high and of the low range."""
+        """Per-species records of ``transport``, [literal mode][species x 19]: kOverEps,
+        mucoeff, 1/W, 1.25 R_cst/W (finitechem.f90:431), the NASA cp coefficients c0, b1..b5 of
+        the high and of the low range, then q = W^1/4, 1/q and q^2 (Wilke's rewritten factor).
+        And Wilke's matrix A_kj = (1 + W_k/W_j)^-1/2 / sqrt(8) with a zero diagonal, rows padded to
+        a whole number of tiles with zeros, [literal mode][row x N]."""
         rc = 8314.34
+        ns = self.ns
+        nrow = self.wilke_tile()[1]
 
         def rec(m, k):
+            q = m.wmol[k] ** 0.25
             return ([m.koveps[k], m.mucoeff[k], 1.0 / m.wmol[k], 1.25 * rc / m.wmol[k]]
-                    + [m.th_hi[k][i] for i in (0, 7, 8, 9, 10, 11)] + [m.th_lo[k][i] for i in (0, 7, 8, 9, 10, 11)])
-        rows = []
-        for mm in (self.m32, self.m64):
-            rows.append("{" + ", ".join(_d(v) for k in range(self.ns) for v in rec(mm, k)) + "}")
-        return (f"// per-species records of Mech_{self.name}::transport, [literal mode][species][16]\n"
-                f"static __constant__ double {self.name}_props_records[2][{self.ns * 16}] = {{{', '.join(rows)}}};")
+                    + [m.th_hi[k][i] for i in (0, 7, 8, 9, 10, 11)] + [m.th_lo[k][i] for i in (0, 7, 8, 9, 10, 11)]
+                    + [q, 1.0 / q, q * q])
+
+        def wilke(m):
+            A = np.zeros((nrow, ns))
+            for k in range(ns):
+                for j in range(ns):
+                    if j != k:
+                        A[k, j] = (1.0 / math.sqrt(8.0)) * (1.0 + m.wmol[k] / m.wmol[j]) ** -0.5
+            return A
+
+        recs = ["{" + ", ".join(_d(v) for k in range(ns) for v in rec(mm, k)) + "}" for mm in (self.m32, self.m64)]
+        mats = ["{" + ", ".join(_d(v) for v in wilke(mm).ravel()) + "}" for mm in (self.m32, self.m64)]
+        return (f"// per-species records of Mech_{self.name}::transport, [literal mode][species][19]\n"
+                f"static __constant__ double {self.name}_props_records[2][{ns * 19}] = {{{', '.join(recs)}}};\n"
+                f"// Wilke's matrix of Mech_{self.name}::transport, [literal mode][row][species]\n"
+                f"static __constant__ double {self.name}_wilke[2][{nrow * ns}] = {{{', '.join(mats)}}};")
 
     def header(self) -> str:
         m32, m64 = self.m32, self.m64
