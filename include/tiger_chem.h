@@ -202,6 +202,30 @@ int tng_chem_density(tng_chem* h, double* rho, double* wmix, const double* sc, c
 int tng_chem_transport(tng_chem* h, double* visc, double* diff, const double* sc, const int* mask,
                        const tng_extent* ext, const double* lewis, int isc_zmix, int flags);
 
+/* ---- ARTS data files: the solver states the reference reads and writes (core/data.f90:217-284
+ * data_read, :379-457 data_write_full3D; tools/init_flow/param.f90:113-148 through
+ * library/fileio_c.c). Layout: int32 nx, ny, nz, nvars; float64 dt, time; nvars names of 8
+ * blank-padded characters; each variable's nx*ny*nz doubles in Fortran order.
+ *
+ * Header of a file: dims = (nx, ny, nz, nvars), dt, time (nullable), and when names is non-null
+ * the nvars blank-padded 8-character names into names[0 .. 8*nvars) (names_len bytes available). */
+int tng_data_info(const char* path, int* dims, double* dt, double* time, char* names, int names_len);
+
+/* Replaces data_read for one rank: the sub-block start (0-based i, j, k) / count of the named
+ * variables (trailing blanks ignored) into out, variable v of block cell (i, j, k) at
+ * out[v*ld + i + ci*(j + cj*k)] (the species-major layout of the batch entry points), ld >= the
+ * block's cells. start/count null = the whole grid. flags: TNG_HOST_PTRS (h may be null) or
+ * TNG_DEVICE_PTRS (out on h's device; the file is streamed through pinned buffers on h's
+ * stream). Returns when out holds the data. */
+int tng_data_read(tng_chem* h, const char* path, const char* const* vars, int nvar, const int* start,
+                  const int* count, double* out, int64_t ld, int flags);
+
+/* Replaces data_write_full3D for the whole grid dims = (nx, ny, nz): nvar variables named vars
+ * (at most 8 characters) from fields[v*ld + i + nx*(j + ny*k)], with dt and time in the header.
+ * flags as for tng_data_read (device fields are streamed through pinned buffers). */
+int tng_data_write(tng_chem* h, const char* path, const int* dims, const char* const* vars, int nvar, double dt,
+                   double time, const double* fields, int64_t ld, int flags);
+
 /* Parity helper: the solver's own (table-driven, warp-cooperative) right-hand side and, when
  * jac is non-null, its Jacobian (cell-major, (N+1)^2 row-major per cell), device pointers. */
 int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncells, int64_t ld, double p, double* rhs,

@@ -18,6 +18,10 @@ statement by statement into C, keeping:
   C ``float`` literals that are widened on use, integer literals are exact;
 * the by-reference argument passing (``GETLINDRATECOEFF`` overwrites its ``K0`` argument).
 
+The same recipe compiles the reference's own C file library (library/fileio_c.c, unchanged,
+into ``oracle/_ref/libref_fileio.so``): the writer and reader behind its data files
+(tools/init_flow/param.f90:113-148), used to pin the library's data-file reader and writer.
+
 The transliteration is mechanical and shares no code with the product's table generator, so
 it pins that generator and the table-driven oracle independently. Outputs (C sources and the
 shared library) go to ``oracle/_ref/`` only; they are git-ignored and are rebuilt from the
@@ -441,8 +445,19 @@ void ref_{mech}_props_batch(const double *y, const double *Tin, int64_t ncells, 
     return "\n".join(out) + "\n"
 
 
+def build_fileio(src_dir, out_dir=OUT, cc="gcc"):
+    """The reference's own binary file library (library/fileio_c.c, C, compiled unchanged from
+    where it lies) into oracle/_ref/libref_fileio.so: the writer and reader of its data files."""
+    lib_src = os.path.join(os.path.dirname(os.path.abspath(src_dir)), "library", "fileio_c.c")
+    so = os.path.join(out_dir, "libref_fileio.so")
+    if os.path.exists(lib_src):
+        subprocess.check_call([cc, "-O2", "-fPIC", "-shared", "-o", so, lib_src])
+    return so
+
+
 def build(src_dir, out_dir=OUT, cc="gcc"):
     os.makedirs(out_dir, exist_ok=True)
+    build_fileio(src_dir, out_dir, cc)
     cfiles = []
     for mech in MECHS:
         path = os.path.join(out_dir, f"ref_{mech}.c")

@@ -31,6 +31,7 @@ REPO = os.path.dirname(HERE)
 MECH_DIR = os.path.join(REPO, "tiger_nga_b200", "mechanisms")
 LIB = os.path.join(HERE, "_build", "libchem_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_mech.so")
+REF_FILEIO = os.path.join(HERE, "_ref", "libref_fileio.so")
 
 
 def build_oracle(force: bool = False) -> str:
@@ -435,3 +436,79 @@ class Reference:
             tmp = tmp - h[k] * out[k]
         out[N] = tmp / cpmix
         return out
+
+
+class RefFileIO:
+    """The reference's own binary file library (library/fileio_c.c, built unchanged into
+    oracle/_ref/libref_fileio.so), driven in the statement order of its data-file writer
+    (tools/init_flow/param.f90:113-148, param_write_data) and reader (core/data.f90:217-284)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_FILEIO):
+            raise FileNotFoundError(REF_FILEIO)
+        self.lib = ctypes.CDLL(REF_FILEIO)
+        P = ctypes.POINTER(ctypes.c_int)
+        self.lib.BINARY_FILE_OPEN.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, P, ctypes.c_int, ctypes.c_int]
+        self.lib.BINARY_FILE_WRITE.argtypes = [P, ctypes.c_void_p, P, P, P]
+        self.lib.BINARY_FILE_READ.argtypes = [P, ctypes.c_void_p, P, P, P]
+        self.lib.BINARY_FILE_CLOSE.argtypes = [P, P]
+
+    def _open(self, path, mode):
+        unit, ierr = ctypes.c_int(), ctypes.c_int()
+        p = path.encode()
+        if len(p) >= 64:  # BINARY_FILE_OPEN copies the name into char[64] (library/fileio_c.c)
+            raise ValueError(f"the reference's file library takes paths shorter than 64 bytes: {path}")
+        self.lib.BINARY_FILE_OPEN(ctypes.byref(unit), p, mode.encode(), ctypes.byref(ierr), len(p), len(mode))
+        if ierr.value:
+            raise OSError(f"BINARY_FILE_OPEN failed on {path}")
+        return unit
+
+    def _io(self, f, unit, buf, count, size):
+        c, s, e = ctypes.c_int(count), ctypes.c_int(size), ctypes.c_int()
+        f(ctypes.byref(unit), buf, ctypes.byref(c), ctypes.byref(s), ctypes.byref(e))
+
+    def write_data(self, path, data, names, dt=0.0, time=0.0):
+        """param_write_data: data is (nx, ny, nz, nvar) in Fortran order, names up to 8 chars."""
+        data = np.asfortranarray(data, dtype=np.float64)
+        nx, ny, nz, nvar = data.shape
+        u = self._open(path, "w")
+        W = self.lib.BINARY_FILE_WRITE
+        for v in (nx, ny, nz, nvar):
+            x = ctypes.c_int(v)
+            self._io(W, u, ctypes.byref(x), 1, 4)
+        for v in (dt, time):
+            x = ctypes.c_double(v)
+            self._io(W, u, ctypes.byref(x), 1, 8)
+        for n in names:
+            b = ctypes.create_string_buffer(n.ljust(8).encode(), 8)
+            self._io(W, u, b, 8, 1)
+        for v in range(nvar):
+            col = np.asfortranarray(data[:, :, :, v])
+            self._io(W, u, col.ctypes.data, nx * ny * nz, 8)
+        e = ctypes.c_int()
+        self.lib.BINARY_FILE_CLOSE(ctypes.byref(u), ctypes.byref(e))
+
+    def read_data(self, path):
+        """Header, names and fields in the order data_read reads them: (dims, dt, time, names,
+        data (nx, ny, nz, nvar) Fortran order)."""
+        u = self._open(path, "r")
+        R = self.lib.BINARY_FILE_READ
+        dims = np.zeros(4, dtype=np.int32)
+        self._io(R, u, dims.ctypes.data, 4, 4)
+        dt, time = ctypes.c_double(), ctypes.c_double()
+        self._io(R, u, ctypes.byref(dt), 1, 8)
+        self._io(R, u, ctypes.byref(time), 1, 8)
+        names = []
+        for _ in range(int(dims[3])):
+            b = ctypes.create_string_buffer(8)
+            self._io(R, u, b, 8, 1)
+            names.append(b.raw.decode().rstrip(" \x00"))
+        nx, ny, nz, nvar = (int(x) for x in dims)
+        data = np.zeros((nx, ny, nz, nvar), order="F")
+        for v in range(nvar):
+            col = np.zeros((nx, ny, nz), order="F")
+            self._io(R, u, col.ctypes.data, nx * ny * nz, 8)
+            data[:, :, :, v] = col
+        e = ctypes.c_int()
+        self.lib.BINARY_FILE_CLOSE(ctypes.byref(u), ctypes.byref(e))
+        return (nx, ny, nz, nvar), dt.value, time.value, names, data

@@ -120,6 +120,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_substep_autotune": (I, [V, V, L, L, V, D, D, L, ctypes.POINTER(TuneResult)]),
         "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
         "tng_chem_density": (I, [V, V, V, V, V, ctypes.POINTER(Extent), D, I]),
+        "tng_data_info": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(D), ctypes.POINTER(D),
+                              ctypes.c_char_p, I]),
+        "tng_data_read": (I, [V, ctypes.c_char_p, V, I, V, V, V, L, I]),
+        "tng_data_write": (I, [V, ctypes.c_char_p, V, V, I, D, D, V, L, I]),
         "tng_chem_transport": (I, [V, V, V, V, V, ctypes.POINTER(Extent), V, I, I]),
         "tng_mlp_create": (I, [V, I, I, I, I, ctypes.c_uint64, ctypes.POINTER(V)]),
         "tng_mlp_destroy": (I, [V]),
@@ -467,6 +471,66 @@ def _mixture_props(self, sc, p_thermo: float | None = None, visc: bool = False, 
                                            TNG_DEVICE_PTRS), "tng_chem_transport")
     torch.cuda.current_stream(sc.device).wait_stream(sst)
     return out
+
+
+def _names(vars_):
+    arr = (ctypes.c_char_p * len(vars_))(*[v.encode() for v in vars_])
+    return arr
+
+
+def data_info(path: str) -> dict:
+    """Header of an ARTS data file (tng_data_info): dims, dt, time, variable names."""
+    lib = load_library()
+    dims = (ctypes.c_int * 4)()
+    dt, time = ctypes.c_double(), ctypes.c_double()
+    _check(lib.tng_data_info(path.encode(), dims, ctypes.byref(dt), ctypes.byref(time), None, 0), "tng_data_info")
+    buf = ctypes.create_string_buffer(8 * dims[3] + 1)
+    _check(lib.tng_data_info(path.encode(), dims, None, None, buf, 8 * dims[3] + 1), "tng_data_info")
+    raw = buf.raw[:8 * dims[3]].decode()
+    return {"dims": tuple(dims[:3]), "nvars": dims[3], "dt": dt.value, "time": time.value,
+            "names": [raw[8 * v:8 * v + 8].rstrip() for v in range(dims[3])]}
+
+
+def data_read(path: str, vars_, start=None, count=None, chem: "FiniteChem | None" = None, out=None):
+    """The named variables of a sub-block (0-based start / count along i, j, k; default the whole
+    grid) of an ARTS data file (tng_data_read), species-major (nvar, ncells of the block, i
+    fastest). With ``chem`` the result is a CUDA tensor on its device, else a NumPy array."""
+    lib = load_library()
+    info = data_info(path)
+    s = list(start) if start is not None else [0, 0, 0]
+    c = list(count) if count is not None else [d - o for d, o in zip(info["dims"], s)]
+    n = int(np.prod(c))
+    si, ci = (ctypes.c_int * 3)(*s), (ctypes.c_int * 3)(*c)
+    if chem is None:
+        out = np.empty((len(vars_), n)) if out is None else out
+        _check(lib.tng_data_read(None, path.encode(), _names(vars_), len(vars_), si, ci, out.ctypes.data, n,
+                                 TNG_HOST_PTRS), "tng_data_read")
+        return out
+    import torch
+
+    out = torch.empty((len(vars_), n), dtype=torch.float64, device=f"cuda:{chem.device}") if out is None else out
+    chem.torch_stream().wait_stream(torch.cuda.current_stream(out.device))
+    _check(lib.tng_data_read(chem.h, path.encode(), _names(vars_), len(vars_), si, ci, out.data_ptr(), n,
+                             TNG_DEVICE_PTRS), "tng_data_read")
+    return out
+
+
+def data_write(path: str, dims, vars_, fields, dt: float = 0.0, time: float = 0.0, chem: "FiniteChem | None" = None):
+    """Write an ARTS data file of the whole grid dims = (nx, ny, nz) (tng_data_write); fields is
+    (nvar, nx*ny*nz), i fastest: a NumPy array, or a CUDA tensor with ``chem``."""
+    lib = load_library()
+    d = (ctypes.c_int * 3)(*dims)
+    n = int(np.prod(dims))
+    if chem is None:
+        f = np.ascontiguousarray(fields, dtype=np.float64)
+        _check(lib.tng_data_write(None, path.encode(), d, _names(vars_), len(vars_), float(dt), float(time),
+                                  f.ctypes.data, n, TNG_HOST_PTRS), "tng_data_write")
+        return
+    import torch
+
+    chem.torch_stream().wait_stream(torch.cuda.current_stream(fields.device))
+    _check(lib.tng_data_write(chem.h, path.encode(), d, _names(vars_), len(vars_), float(dt), float(time),
+                              fields.contiguous().data_ptr(), n, TNG_DEVICE_PTRS), "tng_data_write")
 
 
 def _substep_static(self, state, dt, p: float) -> int:
