@@ -28,7 +28,10 @@ def _worker(rank, ws, port, q):
         wl = dict(bench.WORKLOADS["h2-substep"])
         wl["side"] = 4
         sol, dt = bench.make_state(wl, rank)
-        q.put((rank, t, float(sol.sum()), sol.shape, dt))
+        wp = dict(bench.WORKLOADS["gri-transport"])
+        wp["side"] = 4
+        props, _ = bench.make_state(wp, rank)  # [Y_1..Y_N, T] of this rank's cells
+        q.put((rank, t, float(sol.sum()) + float(props[-1].sum()), (sol.shape, props.shape), dt))
     finally:
         dist.destroy_process_group()
 
