@@ -155,6 +155,16 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double v) {
 // prediction -> state with conservation; fallback cells keep their state and are listed
 constexpr int kPostNs = 48;  // species of a cell held by the post-processing thread
 
+// The mass fractions of one cell read from the state in place (Y_k = state[k] / rho): the state is
+// read-only until the cell's result is stored, and a warp's reads of one species are one
+// coalesced, L1-resident segment, whereas a per-thread copy would live in local memory.
+struct CellY {
+  const double* s;  // &state[cell]
+  long long ld;
+  double irho;      // 1 / rho
+  __device__ __forceinline__ double operator[](int k) const { return s[(long long)k * ld] * irho; }
+};
+
 // Column k of the constraint matrix: the nel element rows (atoms per kg, a_ek / W_k), then, when
 // NC > nel, the enthalpy row h_k(Th) * hsc.
 template <int NC>
@@ -180,7 +190,7 @@ __device__ __forceinline__ void constraint_col(const SurPost& a, int k, double T
 // is zero and is then left out; otherwise, or when the active set does not settle, the cell is
 // rejected (returns false).
 template <int NC>
-__device__ bool project_t(const SurPost& a, const double* Y0, double* dY, double* D, double Th, double hsc,
+__device__ bool project_t(const SurPost& a, const CellY& Y0, double* dY, float* D, double Th, double hsc,
                           double hrhs) {
   for (int pass = 0; pass < 8; ++pass) {
     double G[NC][NC], r[NC], sc[NC];
@@ -198,7 +208,7 @@ __device__ bool project_t(const SurPost& a, const double* Y0, double* dY, double
       for (int e = 0; e < NC; ++e) {
         r[e] = fma(c[e], dY[k], r[e]);
         sc[e] += fabs(c[e]) * (Y0[k] + fabs(dY[k]));
-        const double cd = c[e] * D[k];
+        const double cd = c[e] * (double)D[k];
 #pragma unroll
         for (int g = 0; g <= e; ++g) G[e][g] = fma(cd, c[g], G[e][g]);
       }
@@ -245,16 +255,16 @@ __device__ bool project_t(const SurPost& a, const double* Y0, double* dY, double
     }
     bool pinned = false;
     for (int k = 0; k < a.ns; ++k) {
-      if (D[k] == 0.0) continue;
+      if (D[k] == 0.0f) continue;
       double c[NC];
       constraint_col<NC>(a, k, Th, hsc, c);
       double corr = 0.0;
 #pragma unroll
       for (int e = 0; e < NC; ++e) corr = fma(c[e], lam[e], corr);
-      dY[k] -= D[k] * corr;
+      dY[k] -= (double)D[k] * corr;
       if (Y0[k] + dY[k] < 0.0) {
         dY[k] = -Y0[k];
-        D[k] = 0.0;
+        D[k] = 0.0f;
         pinned = true;
       }
     }
@@ -264,7 +274,7 @@ __device__ bool project_t(const SurPost& a, const double* Y0, double* dY, double
 }
 
 // the projection for the run-time constraint count nc = nel (+1 with the enthalpy row)
-__device__ bool project(const SurPost& a, int nc, const double* Y0, double* dY, double* D, double Th, double hsc,
+__device__ bool project(const SurPost& a, int nc, const CellY& Y0, double* dY, float* D, double Th, double hsc,
                         double hrhs) {
   switch (nc) {
     case 1: return project_t<1>(a, Y0, dY, D, Th, hsc, hrhs);
@@ -279,22 +289,37 @@ __device__ bool project(const SurPost& a, int nc, const double* Y0, double* dY, 
 }
 
 // mass fractions after the projection: max(Y0 + dY, 0) renormalised to sum 1
-__device__ __forceinline__ double y_new(const double* Y0, const double* dY, int k, double inv_sum) {
+__device__ __forceinline__ double y_new(const CellY& Y0, const double* dY, int k, double inv_sum) {
   return fmax(Y0[k] + dY[k], 0.0) * inv_sum;
 }
 
-// temperature with sum Y_k h_k(T) = h0 (Newton from T), Y = y_new(...)
-__device__ double enthalpy_T(const SurPost& a, const double* Y0, const double* dY, double inv_sum, double h0,
+// temperature with sum Y_k h_k(T) = h0 (Newton from T), Y = y_new(...). Within one NASA range
+// the mixture enthalpy and heat capacity are polynomials in T whose coefficients are the
+// Y-weighted sums of the species' (c0 a_i, c0 b_i): they are formed once per range visited, so
+// a Newton iteration is two Horner chains instead of a pass over the species.
+__device__ double enthalpy_T(const SurPost& a, const CellY& Y0, const double* dY, double inv_sum, double h0,
                              double T) {
+  double ch[6], cc[5];  // H(T) = T (ch0 + T (ch1 + ... + T ch4)) + ch5, Cp(T) = cc0 + T (cc1 + ... + T cc4)
+  int range = -1;
   for (int it = 0; it < 12; ++it) {
-    double hh = 0.0, cp = 0.0;
-    for (int k = 0; k < a.ns; ++k) {
-      double hk, cpk;
-      nasa(a.th, a.tmid, k, T, &hk, &cpk);
-      const double y = y_new(Y0, dY, k, inv_sum);
-      hh = fma(y, hk, hh);
-      cp = fma(y, cpk, cp);
+    const int r = T > a.tmid ? 0 : 1;
+    if (r != range) {
+      range = r;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) ch[i] = 0.0;
+#pragma unroll
+      for (int i = 0; i < 5; ++i) cc[i] = 0.0;
+      for (int k = 0; k < a.ns; ++k) {
+        const double* t = a.th + 24 * k + 12 * r;
+        const double w = y_new(Y0, dY, k, inv_sum) * t[0];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) ch[i] = fma(w, t[1 + i], ch[i]);
+#pragma unroll
+        for (int i = 0; i < 5; ++i) cc[i] = fma(w, t[7 + i], cc[i]);
+      }
     }
+    const double hh = T * (ch[0] + T * (ch[1] + T * (ch[2] + T * (ch[3] + T * ch[4])))) + ch[5];
+    const double cp = cc[0] + T * (cc[1] + T * (cc[2] + T * (cc[3] + T * cc[4])));
     const double step = (hh - h0) / cp;
     T -= step;
     if (fabs(step) < 1e-9 * T) break;
@@ -315,7 +340,11 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
       const float span = a.fmax[i] - a.fmin[i];
       if (f < a.fmin[i] - a.margin * span || f > a.fmax[i] + a.margin * span) reason = 1;
     }
-    double Y0[kPostNs], dY[kPostNs], D[kPostNs];
+    // dY in double, the projection weights D in float (the constraints hold exactly for any
+    // weights, since the normal equations use the same D); Y0 is read from the state in place
+    double dY[kPostNs];
+    float D[kPostNs];
+    const CellY Y0{a.state + cell, a.ld, 1.0 / rho};
     // the ensemble: mean prediction, and the spread of the members as an error indicator
     const float* o = a.out + (size_t)cell * a.out_pad;
     double rT = 0.0, tlo = 1e300, thi = -1e300, sY = 0.0;
@@ -328,7 +357,6 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
     const double sT = T0 * (thi - tlo);
     double neg = 0.0, h0 = 0.0;  // negative mass fraction the network predicted (clip test)
     for (int k = 0; k < a.ns; ++k) {
-      Y0[k] = a.state[(long long)k * a.ld + cell] / rho;
       double m = 0.0, lo = 1e300, hi = -1e300;
       for (int i = 0; i < a.members; ++i) {
         const double v = (double)o[i * a.member_stride + 1 + k] * a.tstd[1 + k] + a.tmean[1 + k];
@@ -337,7 +365,7 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
       }
       dY[k] = m / a.members;
       sY = fmax(sY, hi - lo);
-      D[k] = fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12;
+      D[k] = (float)(fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12);
       if (Y0[k] + dY[k] < 0.0) neg -= Y0[k] + dY[k];
       double hk, cpk;
       nasa(a.th, a.tmid, k, T0, &hk, &cpk);
