@@ -783,7 +783,8 @@ def main():
             "max_dY_over_maxY": float(errY.max()), "p99_dY_over_maxY": float(torch.quantile(errY.float(), 0.99)),
             "within_1pct_T": bool(float(errT.max()) <= 0.01), "within_1e-3_dY": bool(float(errY.max()) <= 1e-3)}
         extra["surrogate"] = {k: stats_last[k] for k in ("accepted", "fallback_ood", "fallback_consistency",
-                                                         "fallback_clip", "judged", "judge_max_rel_dT",
+                                                         "fallback_clip", "fallback_ensemble", "judged",
+                                                         "judge_max_rel_dT",
                                                          "judge_max_dY", "ms_infer", "ms_post", "ms_fallback",
                                                          "ms_total")}
         extra["surrogate"]["fallback_fraction"] = 1.0 - stats_last["accepted"] / ncells
