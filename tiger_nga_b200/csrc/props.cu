@@ -109,10 +109,20 @@ extern "C" int tng_chem_transport(tng_chem* h, double* visc, double* diff, const
       inv[k] = 1.0 / lewis[k];
     }
   }
+  if (ns > 64) return set_error(TNG_ERR_ARG, "tng_chem_transport: more than 64 species");
   DeviceGuard g(h->cfg.device);
   cudaStream_t st = h->stream;
-  if (!h->bufs[8].reserve(sizeof(double) * ns)) return set_error(TNG_ERR_CUDA, "tng_chem_transport: allocation failed");
-  cudaMemcpyAsync(h->bufs[8].ptr, inv.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+  // the device copy of the reciprocal Lewis numbers is refreshed only when they change (a copy
+  // from pageable memory would wait for the stream, and the values rarely change between calls)
+  if (h->props_lewis_n != ns || std::memcmp(h->props_inv_lewis, inv.data(), sizeof(double) * ns) != 0) {
+    if (!h->bufs[8].reserve(sizeof(double) * ns))
+      return set_error(TNG_ERR_CUDA, "tng_chem_transport: allocation failed");
+    // stream-ordered: an earlier launch that still reads the previous values finishes first
+    cudaError_t ce = cudaMemcpyAsync(h->bufs[8].ptr, inv.data(), sizeof(double) * ns, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return cuda_error(ce, "tng_chem_transport");
+    std::memcpy(h->props_inv_lewis, inv.data(), sizeof(double) * ns);
+    h->props_lewis_n = ns;
+  }
   PropsArgs a{};
   a.ldy = b.vol, a.ldd = b.vol;
   a.nxo = b.nxo, a.nyo = b.nyo, a.n = b.vol;

@@ -72,4 +72,6 @@ struct tng_chem {
   tng::DevBuf bufs[10];  // 0-3 rate staging, 4-5 solver, 6-7 Fortran substep, 8-9 mixture properties
   tng::SolverState* solver = nullptr;
   int dependents = 0;  // live tng_mlp / tng_surrogate objects using this handle's stream
+  double props_inv_lewis[64];  // reciprocal Lewis numbers held in bufs[8] (props_lewis_n of them)
+  int props_lewis_n = 0;
 };
