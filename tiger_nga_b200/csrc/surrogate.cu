@@ -371,6 +371,10 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
       nasa(a.th, a.tmid, k, T0, &hk, &cpk);
       h0 = fma(Y0[k], hk, h0);
     }
+    // species the network drives below zero are pinned at zero before the first pass (the
+    // projection would pin them one pass at a time otherwise)
+    for (int k = 0; k < a.ns; ++k)
+      if (Y0[k] + dY[k] < 0.0) dY[k] = -Y0[k], D[k] = 0.0f;
     // element conservation, then the temperature the conserved Y implies
     bool ok = project(a, a.nel, Y0, dY, D, 0.0, 0.0, 0.0);
     double sum = 0.0;
