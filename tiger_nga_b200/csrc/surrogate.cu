@@ -456,9 +456,14 @@ __global__ void k_scatter_list(double* __restrict__ dst, long long ld, int nv, c
     for (int v = 0; v < nv; ++v) dst[(long long)v * ld + list[j]] = src[(long long)v * src_ld + J + j];
 }
 
-__global__ void k_iota(int* __restrict__ a, long long n) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    a[i] = (int)i;
+// Processing order of the joint batch (judged sample in columns 0..J-1, the *count fallback
+// cells after it): the fallback cells first -- the ones the surrogate could not take, usually the
+// stiffest -- so that the longest integrations start earliest and the tail is shorter.
+__global__ void k_joint_order(int* __restrict__ a, const int* __restrict__ count, int J, long long cap) {
+  const long long n = *count;
+  const long long m = (J + n < cap) ? J + n : cap;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+    a[i] = (int)(i < n ? J + i : i - n);
 }
 
 // surrogate(+fallback) result vs implicit result on the judged cells
@@ -1032,7 +1037,7 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   if (joint) {
     // fallback cells and the judged sample in one implicit solve, then the fallback cells back
     k_gather_list<<<1184, 128, 0, st>>>(dstate, dld, nv, fb_list, fb_count, J, comp, ldc, ddts, dt, comp_dts, comp_n);
-    k_iota<<<(int)std::min<int64_t>(4096, (ldc + 255) / 256), 256, 0, st>>>(comp_iota, ldc);
+    k_joint_order<<<(int)std::min<int64_t>(4096, (ldc + 255) / 256), 256, 0, st>>>(comp_iota, fb_count, J, ldc);
     rc = substep_run(h, comp, ldc, ldc, comp_dts, 0.0, p, TNG_DEVICE_PTRS, comp_iota, comp_n, nullptr, nullptr, nullptr,
                      &fst);
     if (rc) return rc;
