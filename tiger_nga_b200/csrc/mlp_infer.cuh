@@ -60,7 +60,8 @@ __device__ __forceinline__ float sur_raw_input(int i, int ns, int bath, const do
   int k = lin ? i - ns - 2 : i - 2;
   if (k >= bath) ++k;
   const double y = state[(long long)k * ld + cell] / rho;
-  return lin ? (float)y : (float)log10(fmax(y, 1e-30));
+  // the logarithm in FP32: the feature is rounded to FP32 (and to BF16 for the network) anyway
+  return lin ? (float)y : log10f(fmaxf((float)y, 1e-30f));
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
