@@ -51,7 +51,7 @@ struct InferArgs {
 // in mechanism order without the bath gas, once on a log scale (trace radicals) and once linear
 // (heat release is linear in the mass fractions). n_in = 2 ns + 1.
 __device__ __forceinline__ float sur_raw_input(int i, int ns, int bath, const double* __restrict__ state, long long ld,
-                                               int cell, double rho, double T, double logp, double dt) {
+                                               int cell, double irho, double T, double logp, double dt) {
   if (i == 0) return (float)T;
   if (i == 1) return (float)logp;
   if (i == ns + 1) return (float)log10(fmax(dt, 1e-30));
@@ -59,7 +59,7 @@ __device__ __forceinline__ float sur_raw_input(int i, int ns, int bath, const do
   const bool lin = i > ns + 1;
   int k = lin ? i - ns - 2 : i - 2;
   if (k >= bath) ++k;
-  const double y = state[(long long)k * ld + cell] / rho;
+  const double y = state[(long long)k * ld + cell] * irho;  // irho = 1 / rho
   // the logarithm in FP32: the feature is rounded to FP32 (and to BF16 for the network) anyway
   return lin ? (float)y : log10f(fmaxf((float)y, 1e-30f));
 }
@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         s_T[row] = T;
       }
       __syncthreads();
-      const double rho = s_rho[row], T = s_T[row];
+      const double irho = 1.0 / s_rho[row], T = s_T[row];
       const double dt = live ? (a.dts ? a.dts[cell] : a.dt_scalar) : 0.0;
       const int ng = a.in_pad / 8, g0 = part == 0 ? 0 : (ng + 1) / 2, g1 = part == 0 ? (ng + 1) / 2 : ng;
       for (int g = g0; g < g1; ++g) {
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         for (int q = 0; q < 8; ++q) {
           const int i = k8 + q;
           f[q] = (live && i < a.n_in)
-                     ? (sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, rho, T, a.logp, dt) - a.fmean[i]) * a.fistd[i]
+                     ? (sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, irho, T, a.logp, dt) - a.fmean[i]) * a.fistd[i]
                      : 0.f;
         }
         __nv_bfloat162 p0 = __floats2bfloat162_rn(f[0], f[1]);

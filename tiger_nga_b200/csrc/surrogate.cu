@@ -65,7 +65,8 @@ __device__ __forceinline__ int raw_features(const double* state, long long ld, i
   for (int k = 0; k < ns; ++k) rho += state[(long long)k * ld + cell];
   const double T = state[(long long)ns * ld + cell] / rho;
   const int n_in = 2 * ns + 1;
-  for (int i = 0; i < n_in; ++i) f[i] = sur_raw_input(i, ns, bath, state, ld, cell, rho, T, logp, dt);
+  const double irho = 1.0 / rho;
+  for (int i = 0; i < n_in; ++i) f[i] = sur_raw_input(i, ns, bath, state, ld, cell, irho, T, logp, dt);
   *rho_out = rho;
   *T_out = T;
   return n_in;
@@ -334,9 +335,10 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
     double rho = 0.0;
     for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
     const double T0 = a.state[(long long)a.ns * a.ld + cell] / rho;
+    const double irho0 = 1.0 / rho;
     int reason = 0;
     for (int i = 0; i < a.n_in && !reason; ++i) {
-      const float f = sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, rho, T0, a.logp, dt);
+      const float f = sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, irho0, T0, a.logp, dt);
       const float span = a.fmax[i] - a.fmin[i];
       if (f < a.fmin[i] - a.margin * span || f > a.fmax[i] + a.margin * span) reason = 1;
     }
