@@ -82,6 +82,22 @@ int tng_chem_species_name(const tng_chem* h, int k, char* buf, int len);
 /* The handle's CUDA stream (cudaStream_t) for callers that enqueue around it. */
 void* tng_chem_stream(tng_chem* h);
 
+/* ---- Compatibility shims with the mechanism's Fortran signatures, arguments by reference, for a
+ * caller that still evaluates the mechanism one cell at a time (finitechem_compute_rhs,
+ * finitechem.f90:93-175); a Fortran caller writes `call tng_prodrates(CDOT, W, K, C, M, T, P)`.
+ * They run on the GPU of the handle registered here (one launch and two copies per call: the
+ * batch entry points above are the fast path). No status is returned, as for the Fortran
+ * routines: on an error the outputs are NaN and tng_last_error has the message. */
+void tng_set_mechanism_handle(tng_chem* h);
+/* PRODRATES(CDOT, W, K, C, M, TEMP, PRESSURE) (HYDROGENF.f90:4-277; grimech30F.f90:4-2580):
+ * CDOT[N] in kmol/m^3/s from C[N] in kmol/m^3, and the slot rates W[R] (reference literal kinds
+ * only; W may be null). K and M are the reference's work arrays and are not written. */
+void tng_prodrates_(double* cdot, double* w, double* k, const double* c, double* m, const double* temp,
+                    const double* pressure);
+/* COMPTHERMODATA(H, CP, T) (HYDROGENF.f90:514-673): h_k in J/kg and cp_k in J/(kg K) at T (the
+ * NASA range switch T > 1000 K strict). */
+void tng_compthermodata_(double* h, double* cp, const double* t);
+
 /* Batched finitechem_compute_rhs (finitechem.f90:93-175, low-Mach branch) with PRODRATES,
  * GETLINDRATECOEFF and COMPTHERMODATA inside: for each of ncells cells,
  *   sol = (rho*Y_1..rho*Y_N, rho*T)  ->  rhs = (d(rho*Y_k)/dt, d(rho*T)/dt)

@@ -64,7 +64,7 @@ def test_fp64_matches_oracle(mech, oracles):
 @pytest.mark.parametrize("mech", list(FUEL))
 def test_fp64_slot_rates_match_oracle(mech, oracles):
     """Every slot's rate W_r (the PRODRATES work array) agrees with the oracle."""
-    sol = state(mech, 4096, seed=2)
+    sol = state(mech, 4099, seed=2)  # ragged against the 128-thread blocks: idle lanes must not store
     chem = capi.FiniteChem(mech, "fp64")
     x = torch.from_numpy(sol).cuda()
     _, rates = chem.compute_rhs_rates(x, P)

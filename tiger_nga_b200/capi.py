@@ -120,6 +120,9 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_substep_autotune": (I, [V, V, L, L, V, D, D, L, ctypes.POINTER(TuneResult)]),
         "tng_chem_substep": (I, [V, V, V, V, ctypes.POINTER(Extent), D, D, V, V, I, ctypes.POINTER(SubstepStats)]),
         "tng_chem_density": (I, [V, V, V, V, V, ctypes.POINTER(Extent), D, I]),
+        "tng_set_mechanism_handle": (None, [V]),
+        "tng_prodrates_": (None, [V, V, V, V, V, ctypes.POINTER(D), ctypes.POINTER(D)]),
+        "tng_compthermodata_": (None, [V, V, ctypes.POINTER(D)]),
         "tng_data_info": (I, [ctypes.c_char_p, ctypes.POINTER(I), ctypes.POINTER(D), ctypes.POINTER(D),
                               ctypes.c_char_p, I]),
         "tng_data_read": (I, [V, ctypes.c_char_p, V, I, V, V, V, L, I]),
@@ -533,6 +536,30 @@ def data_write(path: str, dims, vars_, fields, dt: float = 0.0, time: float = 0.
                               fields.contiguous().data_ptr(), n, TNG_DEVICE_PTRS), "tng_data_write")
 
 
+def _prodrates_cell(self, C, T: float, P: float):
+    """One cell through the Fortran-signature shim tng_prodrates_ (PRODRATES(CDOT, W, K, C, M, T, P)):
+    returns (CDOT [kmol/m^3/s], W slot rates)."""
+    c = np.ascontiguousarray(C, dtype=np.float64)
+    cdot, w = np.zeros(self.nspecies), np.zeros(self.nreactions)
+    k, m = np.zeros(self.nreactions), np.zeros(max(self.nthirdbody, 1))
+    self.lib.tng_set_mechanism_handle(self.h)
+    self.lib.tng_prodrates_(cdot.ctypes.data, w.ctypes.data, k.ctypes.data, c.ctypes.data, m.ctypes.data,
+                            ctypes.byref(ctypes.c_double(T)), ctypes.byref(ctypes.c_double(P)))
+    if np.isnan(cdot).any():
+        raise ChemError(f"tng_prodrates_ failed: {last_error()}")
+    return cdot, w
+
+
+def _thermo_cell(self, T: float):
+    """COMPTHERMODATA(H, CP, T) through the shim tng_compthermodata_: (h [J/kg], cp [J/(kg K)])."""
+    hk, cp = np.zeros(self.nspecies), np.zeros(self.nspecies)
+    self.lib.tng_set_mechanism_handle(self.h)
+    self.lib.tng_compthermodata_(hk.ctypes.data, cp.ctypes.data, ctypes.byref(ctypes.c_double(T)))
+    if np.isnan(hk).any():
+        raise ChemError(f"tng_compthermodata_ failed: {last_error()}")
+    return hk, cp
+
+
 def _substep_static(self, state, dt, p: float) -> int:
     """tng_substep_batch_static on a CUDA tensor (allocates nothing on the device during the
     call; at most 262144 cells; calls must not overlap). Returns the number of failed cells."""
@@ -627,6 +654,8 @@ def _autotune(self, state, dt=None, p: float = 101325.0, kind: str = "substep", 
 FiniteChem._tuning_key = _tuning_key
 FiniteChem.autotune = _autotune
 FiniteChem.source_chemistry = _source_chemistry
+FiniteChem.prodrates_cell = _prodrates_cell
+FiniteChem.thermo_cell = _thermo_cell
 FiniteChem.density = _density
 FiniteChem.transport = _transport
 FiniteChem.mixture_props = _mixture_props

@@ -232,7 +232,7 @@ class _Gen:
                     sg = "".join(f" * sg{c}" for c in s32.C) + (f" * sm{s32.M}" if s32.M >= 0 else "")
                     o.append(f"    const double w = (double)(tng_ex2f(lk2{tail}){sg});")
                 if dump:
-                    o.append(f"    if (DUMP) dump[{r}LL * dld] = w;")
+                    o.append(f"    if (DUMP && dump) dump[{r}LL * dld] = w;  // null for the lanes past the last cell")
                 self.scatter(r, o, "    ")
                 o.append("  }")
                 continue
@@ -276,7 +276,7 @@ class _Gen:
                 sg = "".join(f" * sg{c}" for c in s32.C) + (f" * sm{s32.M}" if s32.M >= 0 else "")
                 o.append(f"  {{ const double w = (double)(tng_ex2f({head}{tail}){sg});")
             if dump:
-                o.append(f"    if (DUMP) dump[{r}LL * dld] = w;")
+                o.append(f"    if (DUMP && dump) dump[{r}LL * dld] = w;  // null for the lanes past the last cell")
             self.scatter(r, o, "    ")
             o.append("  }")
 

@@ -69,7 +69,7 @@ struct tng_chem {
   int sm_count = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t copy_stream[2] = {nullptr, nullptr};
-  tng::DevBuf bufs[10];  // 0-3 rate staging, 4-5 solver, 6-7 Fortran substep, 8-9 mixture properties
+  tng::DevBuf bufs[11];  // 0-3 rate staging, 4-5 solver, 6-7 Fortran substep, 8-9 mixture properties, 10 shims
   tng::SolverState* solver = nullptr;
   int dependents = 0;  // live tng_mlp / tng_surrogate objects using this handle's stream
   double props_inv_lewis[64];  // reciprocal Lewis numbers held in bufs[8] (props_lewis_n of them)
