@@ -343,7 +343,6 @@ class _Gen:
         m32, m64 = self.m32, self.m64
         ns = self.ns
         o: list[str] = []
-        W32, W64 = m32.wmol, m64.wmol
         om = {i + 1: v for i, v in enumerate((3.3530622607, 2.53272006, 2.9024238575, 0.11186138893, 0.8662326188,
                                               1.3913958626, 3.158490576, 0.18973411754, 0.00018682962894))}
         o.append("  template <int LM>")
