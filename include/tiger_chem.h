@@ -6,6 +6,9 @@
  *   - the substep  finitechem_source_chemistry(RHO_, SC_)    combustion/finitechem.f90:962-1071
  *   - the mechanism plugin  PRODRATES / COMPTHERMODATA / GETMOLARMASS / GETSPECIESNAMES /
  *     GETNSPECIES / GETNREACTIONS                            combustion/mechanism.f90:17-108
+ * and, around the substep, the per-cell mixture properties (finitechem_density / _W /
+ * _viscosity / _diffusivity, finitechem.f90:65-74, :324-487) and the solver-state data files
+ * (core/data.f90:217-457), which have entry points here too.
  * Every entry point here takes plain pointers and sizes, returns an int status (0 = OK,
  * negative = error; tng_last_error() gives the message) and is callable from Fortran through
  * ISO_C_BINDING (see fortran/tiger_chem_gpu.f90).
