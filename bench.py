@@ -591,7 +591,7 @@ def main():
     ap.add_argument("--workload", default="gri-surrogate", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="tiger", choices=["tiger", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (0: min(steps, 3))")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (0: the timed steps of `value`)")
     ap.add_argument("--plain-cells", type=int, default=262144,
                     help="gri-surrogate: cells of the strided subsample solved by the plain GPU path (0 = all)")
     ap.add_argument("--side", type=int, default=0, help="cube side override (small profiling cases)")
@@ -742,17 +742,23 @@ def main():
         fp64_peak = capi.fp64_peak_tflops(local)
         nbytes = 2 * (mech.ns + 1) * 8 * (sst["cells"] or 0)
         if flops and ms_solver > 0:
+            # the solver is bound by the latency of a warp's dependent FP64 chains, not by HBM: its
+            # roofline is the FP64 pipe (counted flops over the measured FP64 FMA peak), with the
+            # profile's issue and occupancy figures beside it
             ach = flops / (ms_solver * 1e-3) / 1e12
-            roof = {"bound": "hbm", "achieved": nbytes / (ms_solver * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": nbytes / (ms_solver * 1e-3) / 1e9 / hbm_peak,
+            prof = f"k_bdf_{wl['mech']}.txt"
+            roof = {"bound": "fp64/latency", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": ach / fp64_peak,
                     "traffic": (lambda v: v * sst["cells"] if v else None)(
-                        read_profile_value(f"k_bdf_{wl['mech']}.txt", "dram_bytes_per_cell")),
-                    "peak_source": peak_src, "kernel": "k_bdf",
-                    "fp64_pipe": {"achieved_tflops": ach, "peak_tflops_measured": fp64_peak, "frac": ach / fp64_peak,
-                                  "counted_flops_per_launch": flops,
-                                  "note": "the implicit solve is latency bound (dependent FP64 chains, warp "
-                                          "shuffles); counted flops are a lower bound (RHS per Newton iteration, "
-                                          "LU per Jacobian, triangular solves)"}}
+                        read_profile_value(prof, "dram_bytes_per_cell")),
+                    "peak_source": "measured (the library's FP64 FMA probe on this GPU; MEASURED_PEAKS has no FP64)",
+                    "kernel": "k_bdf", "counted_flops_per_launch": flops,
+                    "issue_active_frac": read_profile_value(prof, "issue_active_frac"),
+                    "warps_active_frac": read_profile_value(prof, "warps_active_frac"),
+                    "hbm": {"algorithmic_bytes": nbytes, "achieved_gbs": nbytes / (ms_solver * 1e-3) / 1e9,
+                            "peak_gbs": hbm_peak},
+                    "note": "counted flops are a lower bound (one reference-formulation RHS per Newton iteration, "
+                            "2/3 n^3 per LU, two triangular solves per iteration); the kernel is latency bound"}
         extra["solver"] = {k: sst.get(k) for k in ("cells", "cells_failed", "steps", "newton_iters", "jacobians",
                                                    "max_steps_cell", "max_newton_cell", "passes", "ms")}
 
@@ -789,17 +795,21 @@ def main():
                                                          "ms_total")}
         extra["surrogate"]["fallback_fraction"] = 1.0 - stats_last["accepted"] / ncells
         extra["surrogate"]["weights"] = os.path.relpath(args.surrogate, REPO)
-        # tensor roofline of the inference chain (reported beside the dominant solver kernel)
-        nparam_flops = 2.0 * sur.nparam  # one multiply-add per weight per cell
+        # tensor roofline of the inference chain (reported beside the dominant solver kernel):
+        # algorithmic flops = 2 x (weights of the unpadded layers) per cell and ensemble member;
+        # ms_infer covers the inference of every member
+        alg = 2.0 * sur.weights_unpadded * sur.members
         t_inf = stats_last["ms_infer"] * 1e-3
         if t_inf > 0 and bf16_peak:
-            ach = nparam_flops * ncells / t_inf / 1e12
+            ach = alg * ncells / t_inf / 1e12
             extra["inference_roofline"] = {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                                            "frac": ach / bf16_peak, "peak_source": peak_src,
-                                           "kernel": "k_mlp_infer", "flops_per_cell": nparam_flops}
+                                           "kernel": "k_mlp_infer", "members": sur.members,
+                                           "alg_flops_per_cell_per_member": 2.0 * sur.weights_unpadded,
+                                           "executed_flops_per_cell_per_member": 2.0 * sur.weights_padded}
 
     # ---- e2e through the C-ABI with pinned host buffers -----------------------------------------
-    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else min(args.steps, 3)
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else args.steps
     hin = torch.from_numpy(sol).pin_memory()
     hbuf = torch.empty_like(hin).pin_memory()
     hd = torch.from_numpy(np.ascontiguousarray(dts)).pin_memory().numpy() if dts is not None and np.ndim(dts) else dts

@@ -173,9 +173,12 @@ int tng_substep_batch(tng_chem* h, double* state, int64_t ncells, int64_t ld, co
  * not allocate device memory during the call; no counterpart in the reference, which lets
  * CVODE allocate per cell. All scratch (tables, per-cell counters) lives in one static device
  * array: at most 262144 cells per call (TNG_ERR_ARG beyond). The first call on a device does
- * a synchronous set-up and should precede any stream capture. Calls that overlap in time on
- * one device race on the shared scratch: order them (e.g. one stream). n_failed (host,
- * nullable) receives the number of cells with a nonzero status; when given the call waits. */
+ * a synchronous set-up (it writes the solver tables of every built-in mechanism into the
+ * array) and should precede any stream capture; later calls copy nothing and may alternate
+ * mechanisms freely. Calls that overlap in time on one device race on the shared scratch:
+ * order them (e.g. one stream). n_failed (host, nullable) receives the number of cells with a
+ * nonzero status; when given the call waits, so it must be NULL inside a stream capture
+ * (TNG_ERR_ARG otherwise). */
 int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncells, int64_t ld, const double* dts, double dt,
                              double p, int* n_failed);
 
@@ -198,6 +201,14 @@ typedef struct tng_extent {
  * TNG_DEVICE_PTRS or TNG_HOST_PTRS (arrays staged through the device; the call then waits). */
 int tng_chem_substep(tng_chem* h, const double* rho, double* sc, const int* mask, const tng_extent* ext, double dt,
                      double p_mid, double* hr, double* chemsrc, int flags, tng_substep_stats* stats);
+
+/* Host-only (no device, no handle): the checks tng_chem_substep makes on a rank's extent for a
+ * mechanism of nspecies species, and what it derives from it -- the number of interior cells
+ * (imax-imin+1)*(jmax-jmin+1)*(kmax-kmin+1), the padded volume, and the positions of H2O / CO /
+ * CO2 in the species block (-1 = absent), each output nullable. Errors as tng_chem_substep's.
+ * Replaces the extent bookkeeping of finitechem_source_chemistry's loops over the rank's block
+ * (finitechem.f90:993-1065) set up by partition_init (geometry/partition.f90:33-93). */
+int tng_extent_plan(const tng_extent* ext, int nspecies, int64_t* n_interior, int64_t* volume, int* diag_species);
 
 /* ---- Mixture properties around the substep, on the same Fortran arrays. Like the reference,
  * they visit every cell of the padded block (imino..imaxo, jmino..jmaxo, kmino..kmaxo) whose
@@ -343,6 +354,12 @@ int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, in
                           double* indicator);
 /* FP32 reference forward of the network on normalised features (device pointers). */
 int tng_surrogate_forward_f32(tng_surrogate* s, const float* X, int64_t n, float* Y);
+/* Test hook of the inference kernel's bounded waits (no counterpart in the reference): every
+ * later inference of s gives up a wait after wait_limit polls (0: the default limit), and with
+ * fault = 1 each CTA's first layer withholds its completion signal, so that the epilogue's wait
+ * runs out. The kernel then drains its own copies and MMAs, frees its tensor memory and reports
+ * the timeout, which the call returns as TNG_ERR_CUDA. (0, 0) restores normal operation. */
+int tng_surrogate_debug_waits(tng_surrogate* s, int wait_limit, int fault);
 /* Tensor-core inference only: normalised predictions (n x out_pad FP32, device) of a state batch. */
 int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double dt,
                         double p, float* out);

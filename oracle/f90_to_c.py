@@ -470,6 +470,14 @@ def build(src_dir, out_dir=OUT, cc="gcc"):
     return so
 
 
+def reference_combustion_dir() -> str:
+    """The reference's ``combustion/`` directory that this recipe reads: under the project root
+    named by the environment variable TNG_REFERENCE_DIR, else under the read-only mount of the
+    reference project in the build container. The directory may be absent (e.g. on a GPU host);
+    callers check for it."""
+    return os.path.join(os.environ.get("TNG_REFERENCE_DIR", "/root/reference"), "combustion")
+
+
 if __name__ == "__main__":
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/combustion"
+    src = sys.argv[1] if len(sys.argv) > 1 else reference_combustion_dir()
     print(build(src))

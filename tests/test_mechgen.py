@@ -8,7 +8,9 @@ import pytest
 from tiger_nga_b200 import mechgen
 from tiger_nga_b200.mechanism import BUILTIN, composition, load
 
-REF = "/root/reference/combustion"
+from oracle.f90_to_c import reference_combustion_dir  # noqa: E402
+
+REF = reference_combustion_dir()
 
 MINI_H = """
      integer, parameter ::   SN2 = 1, SH = 2 , SO2 = 3, SOH = 4 , SEND = 5

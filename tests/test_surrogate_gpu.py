@@ -58,6 +58,63 @@ def test_tensor_core_chain_matches_fp32_forward(trained):
     assert np.median(np.abs(a - b) / scale) < 0.005
 
 
+def _bf16(t):
+    return t.to(torch.bfloat16).to(torch.float32)
+
+
+def _bf16_chain(sur, X):
+    """FP32 forward of member 0 with the tensor-core chain's roundings: the features, the
+    weights and every hidden activation rounded to BF16, products accumulated in FP32, bias and
+    GELU (tanh form) in FP32."""
+    flat = torch.from_numpy(sur.params()).cuda()
+    off, fi, h = 0, sur.in_pad, _bf16(X)
+    for layer in range(sur.cfg.layers + 1):
+        fo = sur.out_pad if layer == sur.cfg.layers else sur.cfg.hidden
+        W = flat[off:off + fo * fi].view(fo, fi)
+        b = flat[off + fo * fi:off + fo * fi + fo]
+        off += fo * fi + fo
+        z = torch.matmul(h, _bf16(W).T) + b
+        h = z if layer == sur.cfg.layers else _bf16(torch.nn.functional.gelu(z, approximate="tanh"))
+        fi = fo
+    return h
+
+
+def test_tensor_core_chain_matches_bf16_rounded_forward(trained):
+    """The tcgen05 chain against a forward that rounds exactly where the kernel rounds: what is
+    left is FP32 summation order, the kernel's tanh.approx in GELU and the BF16 rounding flips
+    they cause. A wrong operand layout, descriptor or bias would show as O(1) errors."""
+    chem, sur, _ = trained
+    s0, _, d = pairs(chem, 4099, 16)
+    Y_tc = sur.infer(s0, d, P)
+    ref = _bf16_chain(sur, sur.features(s0, d, P))
+    torch.cuda.synchronize()
+    a, b = Y_tc[:, :sur.n_out].double(), ref[:, :sur.n_out].double()
+    scale = torch.clamp(b.abs().amax(0), min=1.0)
+    err = ((a - b).abs() / scale).cpu().numpy()
+    assert np.isfinite(err).all()
+    assert err.max() < 5e-3, err.max()
+    assert np.median(err) < 5e-4, np.median(err)
+
+
+def test_inference_wait_limit_runs_out_and_the_next_call_succeeds(trained):
+    """The inference kernel's bounded waits: with a short poll limit and one withheld completion
+    signal per CTA the wait gives up, the kernel drains its copies and MMAs, frees its tensor
+    memory and reports the timeout (TNG_ERR_CUDA); the next normal call on the same surrogate
+    returns the same predictions as before."""
+    chem, sur, _ = trained
+    s0, _, d = pairs(chem, 4099, 17)
+    good = sur.infer(s0, d, P).clone()
+    sur.debug_waits(wait_limit=2000, fault=1)
+    try:
+        with pytest.raises(capi.ChemError, match="timed out"):
+            sur.infer(s0, d, P)
+    finally:
+        sur.debug_waits(0, 0)
+    again = sur.infer(s0, d, P)
+    torch.cuda.synchronize()
+    assert torch.equal(again, good)
+
+
 def test_surrogate_substep_conserves_and_falls_back(trained):
     chem, sur, _ = trained
     m = load("grimech30")

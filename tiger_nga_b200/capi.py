@@ -115,6 +115,8 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_substep_batch": (I, [V, V, L, L, V, D, D, I, V, V, V, ctypes.POINTER(SubstepStats)]),
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
         "tng_substep_batch_static": (I, [V, V, L, L, V, D, D, ctypes.POINTER(I)]),
+        "tng_surrogate_debug_waits": (I, [V, I, I]),
+        "tng_extent_plan": (I, [ctypes.POINTER(Extent), I, ctypes.POINTER(L), ctypes.POINTER(L), ctypes.POINTER(I)]),
         "tng_chem_set_tuning": (I, [V, I, I, I, I]),
         "tng_rates_autotune": (I, [V, V, L, L, D, ctypes.POINTER(TuneResult)]),
         "tng_substep_autotune": (I, [V, V, L, L, V, D, D, L, ctypes.POINTER(TuneResult)]),
@@ -476,6 +478,18 @@ def _mixture_props(self, sc, p_thermo: float | None = None, visc: bool = False, 
     return out
 
 
+def extent_plan(ext: dict, nspecies: int) -> dict:
+    """tng_extent_plan: host-side checks of a rank's padded block (no device needed). Returns
+    the interior cell count, the padded volume and the H2O / CO / CO2 species positions."""
+    lib = load_library()
+    e = Extent(**ext)
+    n, vol = ctypes.c_int64(), ctypes.c_int64()
+    sp = (ctypes.c_int * 3)()
+    _check(lib.tng_extent_plan(ctypes.byref(e), int(nspecies), ctypes.byref(n), ctypes.byref(vol), sp),
+           "tng_extent_plan")
+    return {"n_interior": n.value, "volume": vol.value, "diag_species": list(sp)}
+
+
 def _names(vars_):
     arr = (ctypes.c_char_p * len(vars_))(*[v.encode() for v in vars_])
     return arr
@@ -787,6 +801,12 @@ class Surrogate:
         _check(self.lib.tng_surrogate_dims(h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ctypes.byref(d),
                                            ctypes.byref(n)), "tng_surrogate_dims")
         self.n_in, self.n_out, self.in_pad, self.out_pad, self.nparam = a.value, b.value, c.value, d.value, n.value
+        self.members = cfg.members
+        H, nh = cfg.hidden, cfg.layers
+        # weights (no biases) of the linear layers n_in -> H -> ... -> H -> n_out, and as executed
+        # with the inputs and outputs padded to the tensor-core tile
+        self.weights_unpadded = self.n_in * H + (nh - 1) * H * H + H * self.n_out
+        self.weights_padded = self.in_pad * H + (nh - 1) * H * H + H * self.out_pad
         chem._children.add(self)
 
     def close(self):
@@ -860,6 +880,11 @@ class Surrogate:
                                               reason.data_ptr(), ind.data_ptr()), "tng_surrogate_predict")
         self._post()
         return out, reason, ind
+
+    def debug_waits(self, wait_limit: int = 0, fault: int = 0):
+        """Test hook: later inferences give up a wait after ``wait_limit`` polls; ``fault=1``
+        withholds one completion signal so the wait runs out (TNG_ERR_CUDA). (0, 0) resets."""
+        _check(self.lib.tng_surrogate_debug_waits(self.h, int(wait_limit), int(fault)), "tng_surrogate_debug_waits")
 
     def forward_f32(self, X):
         import torch

@@ -44,6 +44,11 @@ struct InferArgs {
   int b_off[kMaxLayers];
   float* out;  // [ncells x out_pad] FP32 (normalised predictions)
   int* error;  // non-zero after a timed-out wait
+  // test hook: polls before a wait gives up (0: the default 2^24), and fault = 1 withholds the
+  // first layer's completion signal of each CTA's first tile so that the epilogue's wait runs
+  // out (the MMAs themselves run and are drained as usual)
+  int wait_limit;
+  int fault;
 };
 
 // Raw network input i of a cell (shared by the training features, the inference kernel and the
@@ -95,10 +100,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
-// bounded parity wait; returns false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+constexpr int kWaitPolls = 1 << 24;
+
+// bounded parity wait; returns false after `limit` unsuccessful polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int limit = kWaitPolls) {
   const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < (1 << 24); ++it) {
+  for (int it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -195,6 +202,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
+  const int wlim = a.wait_limit > 0 ? a.wait_limit : kWaitPolls;
   // thread 0 only: parities, pending commits and copies per stage; chunks issued so far (stage =
   // gc % kWStages); chunks of the coming layer already issued (pre) from gc = pre_base
   uint32_t ph_full[kWStages] = {}, ph_free[kWStages] = {}, ph_done = 0;
@@ -208,7 +216,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
     const int s = gc % kWStages;
     ++gc;
     if (stage_busy[s]) {  // wait for the MMA that read this stage
-      if (!mbar_wait(&bar_free[s], ph_free[s])) err = 1;
+      if (!mbar_wait(&bar_free[s], ph_free[s], wlim)) err = 1;
       ph_free[s] ^= 1;
       stage_busy[s] = 0;
     }
@@ -284,7 +292,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         for (int c = 0; c < nchunk && !err; ++c) {
           const int s = (base + c) % kWStages;
           const int kc = min(kWChunkK, K - c * kWChunkK);
-          if (!mbar_wait(&bar_full[s], ph_full[s])) err = 1;
+          if (!mbar_wait(&bar_full[s], ph_full[s], wlim)) err = 1;
           ph_full[s] ^= 1;
           inflight[s] = 0;
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -300,16 +308,21 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
           stage_busy[s] = 1;
           while (issued < nchunk && issued < c + kWStages) issue(l, issued++);
         }
-        umma_commit(bar_done);
+        if (!(a.fault == 1 && l == 0 && tile == (int)blockIdx.x)) umma_commit(bar_done);
       }
       // epilogue: one lane per warp polls the layer barrier, the warp follows
       bool ok = true;
-      if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done);
+      if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done, wlim);
       ok = __shfl_sync(0xffffffffu, ok, 0);
       __syncwarp();
       ph_done ^= 1;
       if (!ok) err = 1;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // after a timed-out wait the layer's MMAs may still read the A operand: no epilogue
+      if (__syncthreads_or(err)) {
+        err = 1;
+        break;
+      }
       // the next layer's (or the next tile's first layer's) first chunks load during the epilogue
       if (tid == 0 && !err) {
         const bool more = l + 1 < a.nlin || tile + (int)gridDim.x < ntiles;

@@ -91,13 +91,11 @@ __global__ void k_fortran_scatter(FortranView v, const double* __restrict__ rho,
 
 }  // namespace tng
 
-using namespace tng;
+namespace tng {
 
-extern "C" int tng_chem_substep(tng_chem* h, const double* rho, double* sc, const int* mask, const tng_extent* ext,
-                                double dt, double p_mid, double* hr, double* chemsrc, int flags,
-                                tng_substep_stats* stats) {
-  if (!h || !rho || !sc || !ext) return set_error(TNG_ERR_ARG, "tng_chem_substep: null argument");
-  if (flags != TNG_DEVICE_PTRS && flags != TNG_HOST_PTRS) return set_error(TNG_ERR_ARG, "tng_chem_substep: bad flags");
+// The host-side checks and index arithmetic of a rank's padded block (no device involved).
+static int extent_view(const tng_extent* ext, int ns, FortranView* out, int* sp3, long long* n_out) {
+  if (!ext) return set_error(TNG_ERR_ARG, "tng_chem_substep: null extent");
   const tng_extent& e = *ext;
   FortranView v;
   v.imino = e.imino, v.jmino = e.jmino, v.kmino = e.kmino;
@@ -107,18 +105,53 @@ extern "C" int tng_chem_substep(tng_chem* h, const double* rho, double* sc, cons
   if (v.nxo <= 0 || v.nyo <= 0 || v.nzo <= 0 || v.nx <= 0 || v.ny <= 0 || v.nz <= 0 || e.imin < e.imino ||
       e.imax > e.imaxo || e.jmin < e.jmino || e.jmax > e.jmaxo || e.kmin < e.kmino || e.kmax > e.kmaxo)
     return set_error(TNG_ERR_ARG, "tng_chem_substep: inconsistent extents");
-  const int ns = h->ops->ns;
   if (e.isc_sc < 1 || e.isc_sc + ns - 1 > e.nscalar || e.isc_T < 1 || e.isc_T > e.nscalar ||
       (e.isc_T >= e.isc_sc && e.isc_T < e.isc_sc + ns))
     return set_error(TNG_ERR_ARG, "tng_chem_substep: scalar indices out of range");
-  if (!(dt > 0.0) || !(p_mid > 0.0)) return set_error(TNG_ERR_ARG, "tng_chem_substep: dt and pressure must be positive");
   auto sp_index = [&](int isc) { return (isc >= e.isc_sc && isc < e.isc_sc + ns) ? isc - e.isc_sc : -1; };
-  const int s_h2o = sp_index(e.isc_H2O), s_co = sp_index(e.isc_CO), s_co2 = sp_index(e.isc_CO2);
+  sp3[0] = sp_index(e.isc_H2O), sp3[1] = sp_index(e.isc_CO), sp3[2] = sp_index(e.isc_CO2);
   v.vol = (long long)v.nxo * v.nyo * v.nzo;
   const long long n = (long long)v.nx * v.ny * v.nz;
   if (n > 0x7fffffffLL) return set_error(TNG_ERR_ARG, "tng_chem_substep: at most 2^31-1 interior cells");
+  *out = v;
+  *n_out = n;
+  return TNG_OK;
+}
+
+}  // namespace tng
+
+using namespace tng;
+
+extern "C" int tng_extent_plan(const tng_extent* ext, int nspecies, int64_t* n_interior, int64_t* volume,
+                               int* diag_species) {
+  if (nspecies < 1) return set_error(TNG_ERR_ARG, "tng_extent_plan: nspecies must be positive");
+  FortranView v;
+  int sp3[3];
+  long long n = 0;
+  const int rc = extent_view(ext, nspecies, &v, sp3, &n);
+  if (rc) return rc;
+  if (n_interior) *n_interior = n;
+  if (volume) *volume = v.vol;
+  if (diag_species) std::memcpy(diag_species, sp3, sizeof(sp3));
+  return TNG_OK;
+}
+
+extern "C" int tng_chem_substep(tng_chem* h, const double* rho, double* sc, const int* mask, const tng_extent* ext,
+                                double dt, double p_mid, double* hr, double* chemsrc, int flags,
+                                tng_substep_stats* stats) {
+  if (!h || !rho || !sc || !ext) return set_error(TNG_ERR_ARG, "tng_chem_substep: null argument");
+  if (flags != TNG_DEVICE_PTRS && flags != TNG_HOST_PTRS) return set_error(TNG_ERR_ARG, "tng_chem_substep: bad flags");
+  const tng_extent& e = *ext;
+  const int ns = h->ops->ns;
+  FortranView v;
+  int sp3[3];
+  long long n = 0;
+  int rc = extent_view(ext, ns, &v, sp3, &n);
+  if (rc) return rc;
+  if (!(dt > 0.0) || !(p_mid > 0.0)) return set_error(TNG_ERR_ARG, "tng_chem_substep: dt and pressure must be positive");
+  const int s_h2o = sp3[0], s_co = sp3[1], s_co2 = sp3[2];
   DeviceGuard g(h->cfg.device);
-  int rc = solver_prepare(h);
+  rc = solver_prepare(h);
   if (rc) return rc;
   cudaStream_t st = h->stream;
   const int nv = ns + 1;

@@ -10,10 +10,14 @@
 //
 // Limits and contract:
 //   * at most kStaticMaxCells cells per call (TNG_ERR_ARG beyond that);
-//   * mechanism tables must fit kStaticTabDoubles / kStaticTabInts (checked, TNG_ERR_ARG);
-//   * the first call on a device does the set-up (symbol address, BDF coefficients into this
-//     file's constant bank, kernel attributes); cudaMemcpyToSymbol there is synchronous, so
-//     that first call should come before any stream capture the caller does;
+//   * the first call on a device does the set-up: the symbol address, the BDF coefficients
+//     into this file's constant bank, and the solver tables of EVERY built-in mechanism (both
+//     literal modes) into their own fixed regions of the array. Those copies are synchronous,
+//     so that first call should come before any stream capture the caller does. A later call
+//     only selects its mechanism's region: it copies no tables, so calls of different
+//     mechanisms can follow each other in any order (and a captured call stays valid);
+//   * with n_failed non-null the call reads the failure count back and waits for the stream,
+//     which a stream capture does not allow: n_failed must then be NULL (TNG_ERR_ARG);
 //   * the scratch is one per device and process: two calls that overlap in time on the same
 //     device (different streams, or different threads without ordering) race on it and give
 //     wrong results. Calls must be ordered, e.g. all on one stream;
@@ -37,25 +41,32 @@ BdfCoef make_coef();  // solver.cu
 namespace {
 
 constexpr int kStaticMaxCells = 1 << 18;
-constexpr int kStaticTabDoubles = 8192;  // GRI-Mech 3.0 needs 4248
-constexpr int kStaticTabInts = 16384;    // GRI-Mech 3.0 needs 9251
+constexpr size_t kStaticTabBytes = (size_t)1 << 20;  // tables of all built-in mechanisms (~0.3 MB used)
+constexpr int kStaticMaxMechs = 16;
 constexpr int kStaticMaxDevices = 64;
 
 // byte offsets inside the scratch array (each region 256-byte aligned)
-constexpr size_t kOffTabD = 0;
-constexpr size_t kOffTabI = kOffTabD + sizeof(double) * kStaticTabDoubles;
-constexpr size_t kOffCtr = kOffTabI + sizeof(int) * kStaticTabInts;               // head, n_out, n_failed
+constexpr size_t kOffTab = 0;
+constexpr size_t kOffCtr = kOffTab + kStaticTabBytes;                               // head, n_out, n_failed
 constexpr size_t kOffCells = kOffCtr + 256;                                         // 6 int arrays of kStaticMaxCells
-constexpr size_t kScratchBytes = kOffCells + sizeof(int) * 6 * (size_t)kStaticMaxCells;  // ~6.2 MB
-static_assert(kOffTabI % 256 == 0 && kOffCtr % 256 == 0 && kOffCells % 256 == 0, "alignment");
+constexpr size_t kScratchBytes = kOffCells + sizeof(int) * 6 * (size_t)kStaticMaxCells;  // ~7.3 MB
+static_assert(kOffCtr % 256 == 0 && kOffCells % 256 == 0, "alignment");
 
 static __device__ __align__(256) unsigned char g_static_scratch[kScratchBytes];
+
+// where one mechanism's tables sit in the table area (byte offsets)
+struct StaticTab {
+  const MechOps* ops = nullptr;
+  size_t hd[2] = {0, 0};  // hot doubles per literal mode
+  size_t ints = 0;        // hot ints, then cold ints
+};
 
 struct StaticDev {
   bool ready = false;
   unsigned char* base = nullptr;
-  const void* tab_key[2] = {nullptr, nullptr};  // host tables last copied in (hot doubles, hot ints)
-  size_t smem_set[9] = {};                      // dynamic shared memory attribute per warp count
+  StaticTab tab[kStaticMaxMechs];
+  int ntab = 0;
+  size_t smem_set[9] = {};  // dynamic shared memory attribute per warp count
 };
 StaticDev g_dev[kStaticMaxDevices];
 std::mutex g_setup_mutex;
@@ -78,8 +89,38 @@ int static_setup(int device, StaticDev** out) {
     const BdfCoef coef = make_coef();
     e = cudaMemcpyToSymbol(c_bdf, &coef, sizeof(coef));
     if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: BDF coefficients");
-    d.base = (unsigned char*)p;
-    d.ready = true;
+    // every built-in mechanism's tables into its own region, packed in registry order
+    unsigned char* base = (unsigned char*)p;
+    size_t off = kOffTab;
+    int nt = 0;
+    auto place = [&](const void* src, size_t bytes, size_t* at) -> int {
+      if (off + bytes > kOffTab + kStaticTabBytes)
+        return set_error(TNG_ERR_ARG, "tng_substep_batch_static: the mechanism tables exceed the static table area");
+      const cudaError_t ce = cudaMemcpy(base + off, src, bytes, cudaMemcpyHostToDevice);
+      if (ce != cudaSuccess) return cuda_error(ce, "tng_substep_batch_static: solver tables");
+      *at = off;
+      off += (bytes + 255) & ~(size_t)255;
+      return TNG_OK;
+    };
+    for (const MechOps* const* m = all_mechanisms(); *m; ++m) {
+      if (nt == kStaticMaxMechs) return set_error(TNG_ERR_ARG, "tng_substep_batch_static: too many mechanisms");
+      const MechOps* o = *m;
+      const SvLayout& L = *o->sv_layout;
+      StaticTab& t = d.tab[nt];
+      t.ops = o;
+      int rc = TNG_OK;
+      for (int lm = 0; lm < 2 && !rc; ++lm) rc = place(o->sv_hd[lm], sizeof(double) * L.nhd, &t.hd[lm]);
+      if (!rc) rc = place(o->sv_hi, sizeof(int) * L.nhi, &t.ints);
+      size_t cold = 0;
+      if (!rc) rc = place(o->sv_ci, sizeof(int) * L.nci, &cold);
+      if (rc) return rc;
+      if (cold != t.ints + ((sizeof(int) * L.nhi + 255) & ~(size_t)255))
+        return set_error(TNG_ERR_STATE, "tng_substep_batch_static: table placement");
+      ++nt;
+    }
+    d.ntab = nt;
+    d.base = base;
+    d.ready = true;  // only once every copy has succeeded
   }
   *out = &d;
   return TNG_OK;
@@ -102,37 +143,36 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   if (!(p > 0.0)) return set_error(TNG_ERR_ARG, "tng_substep_batch_static: pressure must be positive");
   const MechOps* o = h->ops;
   const SvLayout& L = *o->sv_layout;
-  if (L.nhd > kStaticTabDoubles || L.nhi + L.nci > kStaticTabInts)
-    return set_error(TNG_ERR_ARG, "tng_substep_batch_static: tables of %s exceed the static limit", o->name);
   if (n_failed) *n_failed = 0;
   if (ncells == 0) return TNG_OK;
   DeviceGuard g(h->cfg.device);
+  cudaStream_t st = h->stream;
+  cudaError_t e;
+  if (n_failed) {  // the count is read back synchronously, which a stream capture forbids
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return cuda_error(e, "tng_substep_batch_static");
+    if (cs != cudaStreamCaptureStatusNone)
+      return set_error(TNG_ERR_ARG, "tng_substep_batch_static: n_failed must be NULL while the stream is captured");
+  }
   StaticDev* d = nullptr;
   int rc = static_setup(h->cfg.device, &d);
   if (rc) return rc;
-  cudaStream_t st = h->stream;
-  cudaError_t e;
-  double* tab_d = (double*)(d->base + kOffTabD);
-  int* tab_i = (int*)(d->base + kOffTabI);
+  const StaticTab* tab = nullptr;
+  for (int i = 0; i < d->ntab; ++i)
+    if (d->tab[i].ops == o) tab = &d->tab[i];
+  if (!tab) return set_error(TNG_ERR_ARG, "tng_substep_batch_static: %s is not a built-in mechanism", o->name);
+  const double* tab_d = (const double*)(d->base + tab->hd[h->cfg.literal_mode == 1 ? 1 : 0]);
+  const int* tab_i = (const int*)(d->base + tab->ints);
+  const int* tab_c = (const int*)(d->base + tab->ints + ((sizeof(int) * L.nhi + 255) & ~(size_t)255));
   int* ctr = (int*)(d->base + kOffCtr);
   int* cells = (int*)(d->base + kOffCells);
-  const double* hd = o->sv_hd[h->cfg.literal_mode];
-  // tables: copied in when this device last held another mechanism or literal mode
-  if (d->tab_key[0] != hd || d->tab_key[1] != o->sv_hi) {
-    cudaMemcpyAsync(tab_d, hd, sizeof(double) * L.nhd, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(tab_i, o->sv_hi, sizeof(int) * L.nhi, cudaMemcpyHostToDevice, st);
-    e = cudaMemcpyAsync(tab_i + L.nhi, o->sv_ci, sizeof(int) * L.nci, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: tables");
-    d->tab_key[0] = hd;
-    d->tab_key[1] = o->sv_hi;
-  }
   const int warps = (h->cfg.solver_warps == 2 || h->cfg.solver_warps == 4) ? h->cfg.solver_warps : 8;
   BdfLaunch Lh;
   std::memset(&Lh, 0, sizeof(Lh));
   BdfArgs& a = Lh.a;
   a.tab.hd = tab_d;
   a.tab.hi = tab_i;
-  a.tab.ci = tab_i + L.nhi;
+  a.tab.ci = tab_c;
   a.tab.L = L;
   a.tab.mixed = h->cfg.precision == TNG_MIXED;
   const int nv = L.size[SZ_NV];

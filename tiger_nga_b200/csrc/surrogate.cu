@@ -514,6 +514,7 @@ struct tng_surrogate {
   DevBuf out, fb, cnt, judge_state, judge_dts, judge_idx, work, joint;
   cudaEvent_t ev[5] = {};
   int calls = 0;
+  int dbg_wait_limit = 0, dbg_fault = 0;  // test hook of the inference kernel's bounded waits
 };
 
 static int sur_upload_norm(tng_surrogate* s) {
@@ -576,6 +577,8 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double*
   ia.bias = s->member(member).params;
   ia.out = out;
   ia.error = err;
+  ia.wait_limit = s->dbg_wait_limit;
+  ia.fault = s->dbg_fault;
   if ((s->m.nlin - 1) * s->m.hidden + s->m.out_pad > kInferMaxBias)
     return set_error(TNG_ERR_ARG, "inference: the biases do not fit the kernel's shared-memory stage");
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
@@ -867,6 +870,14 @@ int tng_surrogate_load(tng_surrogate* s, const char* path) {
   cudaError_t e = cudaStreamSynchronize(s->m.stream);
   if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_load");
   s->trained = true;
+  return TNG_OK;
+}
+
+int tng_surrogate_debug_waits(tng_surrogate* s, int wait_limit, int fault) {
+  if (!s || wait_limit < 0 || fault < 0 || fault > 1)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_debug_waits: bad argument");
+  s->dbg_wait_limit = wait_limit;
+  s->dbg_fault = fault;
   return TNG_OK;
 }
 

@@ -62,10 +62,13 @@ module tiger_chem_gpu
       type(c_ptr), value :: h
       real(c_double), dimension(*), intent(in) :: rho
       real(c_double), dimension(*), intent(inout) :: sc
-      integer(c_int), dimension(*), intent(in) :: mask
+      ! mask, hr and chemsrc may be left out: an absent optional argument of a bind(C)
+      ! interface is passed as a null pointer (Fortran 2018), which the C side reads as
+      ! "no mask" / "no diagnostics"
+      integer(c_int), dimension(*), intent(in), optional :: mask
       type(tng_extent), intent(in) :: ext
       real(c_double), value :: dt, p_mid
-      real(c_double), dimension(*), intent(inout) :: hr, chemsrc
+      real(c_double), dimension(*), intent(inout), optional :: hr, chemsrc
       integer(c_int), value :: flags
       type(c_ptr), value :: stats
     end function tng_chem_substep
@@ -75,7 +78,7 @@ module tiger_chem_gpu
       import :: c_int, c_double, c_ptr, tng_extent
       type(c_ptr), value :: h, rho, wmix
       real(c_double), dimension(*), intent(in) :: sc
-      integer(c_int), dimension(*), intent(in) :: mask
+      integer(c_int), dimension(*), intent(in), optional :: mask  ! absent: no mask (null)
       type(tng_extent), intent(in) :: ext
       real(c_double), value :: p_thermo
       integer(c_int), value :: flags
@@ -86,7 +89,7 @@ module tiger_chem_gpu
       import :: c_int, c_double, c_ptr, tng_extent
       type(c_ptr), value :: h, visc, diff
       real(c_double), dimension(*), intent(in) :: sc
-      integer(c_int), dimension(*), intent(in) :: mask
+      integer(c_int), dimension(*), intent(in), optional :: mask  ! absent: no mask (null)
       type(tng_extent), intent(in) :: ext
       type(c_ptr), value :: lewis
       integer(c_int), value :: isc_zmix, flags
