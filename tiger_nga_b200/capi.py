@@ -52,7 +52,8 @@ class SurrogateStats(ctypes.Structure):
                 ("fallback_consistency", ctypes.c_int64), ("fallback_clip", ctypes.c_int64),
                 ("judged", ctypes.c_int64), ("judge_max_rel_dT", ctypes.c_double), ("judge_max_dY", ctypes.c_double),
                 ("ms_infer", ctypes.c_double), ("ms_post", ctypes.c_double), ("ms_fallback", ctypes.c_double),
-                ("ms_total", ctypes.c_double), ("fallback", SubstepStats), ("fallback_ensemble", ctypes.c_int64)]
+                ("ms_total", ctypes.c_double), ("fallback", SubstepStats), ("fallback_ensemble", ctypes.c_int64),
+                ("fallback_gate", ctypes.c_int64)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "fallback"}
@@ -65,7 +66,7 @@ class SurrogateCfg(ctypes.Structure):
                 ("ood_margin", ctypes.c_double), ("consist_tol_K", ctypes.c_double), ("clip_tol", ctypes.c_double),
                 ("judge_cells", ctypes.c_int), ("post_mode", ctypes.c_int), ("target_mode", ctypes.c_int),
                 ("loss_T_weight", ctypes.c_float), ("members", ctypes.c_int), ("ens_tol_K", ctypes.c_float),
-                ("ens_tol_Y", ctypes.c_float), ("reserved", ctypes.c_int * 2)]
+                ("ens_tol_Y", ctypes.c_float), ("gate_tol", ctypes.c_float), ("reserved", ctypes.c_int)]
 
 
 class TuneResult(ctypes.Structure):
@@ -116,6 +117,10 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_solver_rhs_jac": (I, [V, V, L, L, D, V, V]),
         "tng_substep_batch_static": (I, [V, V, L, L, V, D, D, ctypes.POINTER(I)]),
         "tng_surrogate_debug_waits": (I, [V, I, I]),
+        "tng_surrogate_refine": (I, [V, V, V, V, L, L, D, I, I, D, D, V, ctypes.POINTER(L)]),
+        "tng_surrogate_train_gate": (I, [V, V, V, V, L, L, D, I, I, D, D, V]),
+        "tng_surrogate_set_gate_tol": (I, [V, D]),
+        "tng_surrogate_gate_info": (I, [V, ctypes.POINTER(I), ctypes.POINTER(D)]),
         "tng_extent_plan": (I, [ctypes.POINTER(Extent), I, ctypes.POINTER(L), ctypes.POINTER(L), ctypes.POINTER(I)]),
         "tng_chem_set_tuning": (I, [V, I, I, I, I]),
         "tng_rates_autotune": (I, [V, V, L, L, D, ctypes.POINTER(TuneResult)]),
@@ -138,6 +143,7 @@ def load_library(path: str | None = None) -> ctypes.CDLL:
         "tng_mlp_forward": (I, [V, V, L, V]),
         "tng_mlp_grad": (I, [V, V, V, V, L, ctypes.POINTER(ctypes.c_float)]),
         "tng_mlp_adam_step": (I, [V, ctypes.c_float]),
+        "tng_mlp_set_under_weight": (I, [V, ctypes.c_float]),
         "tng_mlp_train": (I, [V, V, V, V, L, I, I, D, ctypes.c_uint64, V]),
         "tng_surrogate_default_cfg": (None, [ctypes.POINTER(SurrogateCfg)]),
         "tng_surrogate_create": (I, [V, ctypes.POINTER(SurrogateCfg), ctypes.POINTER(V)]),
@@ -762,6 +768,10 @@ class Mlp:
     def adam_step(self, lr):
         _check(self.lib.tng_mlp_adam_step(self.h, float(lr)), "tng_mlp_adam_step")
 
+    def set_under_weight(self, under: float):
+        """Weight of squared errors of outputs below their target (1: plain weighted MSE)."""
+        _check(self.lib.tng_mlp_set_under_weight(self.h, float(under)), "tng_mlp_set_under_weight")
+
     def train(self, X, T, w_out, epochs, batch, lr, seed=0):
         Xd, Td = self._dev(X, self.in_pad), self._dev(T, self.out_pad)
         wd = self._dev(np.asarray(w_out, dtype=np.float32)[None, :], self.out_pad)
@@ -842,6 +852,39 @@ class Surrogate:
         self._post()
         return losses
 
+    def refine(self, state0, state1, dts, p: float, epochs: int = 10, batch: int = 4096, lr: float = 3e-4,
+               boost: float = 4.0):
+        """Hard-example refinement: more epochs on a population where each pair repeats by its error."""
+        losses = np.zeros(epochs, dtype=np.float32)
+        pop = ctypes.c_int64()
+        self._pre()
+        _check(self.lib.tng_surrogate_refine(self.h, state0.data_ptr(), state1.data_ptr(), dts.data_ptr(),
+                                             state0.shape[1], state0.stride(0), float(p), epochs, batch, float(lr),
+                                             float(boost), losses.ctypes.data, ctypes.byref(pop)),
+               "tng_surrogate_refine")
+        self._post()
+        return losses, pop.value
+
+    def train_gate(self, state0, state1, dts, p: float, epochs: int = 10, batch: int = 4096, lr: float = 2e-3,
+                   under: float = 4.0):
+        """Train the error gate on implicit-solver pairs (the ensemble's own errors as targets)."""
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._pre()
+        _check(self.lib.tng_surrogate_train_gate(self.h, state0.data_ptr(), state1.data_ptr(), dts.data_ptr(),
+                                                 state0.shape[1], state0.stride(0), float(p), epochs, batch,
+                                                 float(lr), float(under), losses.ctypes.data),
+               "tng_surrogate_train_gate")
+        self._post()
+        return losses
+
+    def set_gate_tol(self, tol: float):
+        _check(self.lib.tng_surrogate_set_gate_tol(self.h, float(tol)), "tng_surrogate_set_gate_tol")
+
+    def gate_info(self):
+        g, t = ctypes.c_int(), ctypes.c_double()
+        _check(self.lib.tng_surrogate_gate_info(self.h, ctypes.byref(g), ctypes.byref(t)), "tng_surrogate_gate_info")
+        return bool(g.value), t.value
+
     def save(self, path: str):
         _check(self.lib.tng_surrogate_save(self.h, path.encode()), "tng_surrogate_save")
 
@@ -872,7 +915,7 @@ class Surrogate:
                                                                         device=state.device).contiguous()
         out = torch.empty((state.shape[0], n), dtype=torch.float64, device=state.device)
         reason = torch.empty(n, dtype=torch.int32, device=state.device)
-        ind = torch.empty((n, 3), dtype=torch.float64, device=state.device)
+        ind = torch.empty((n, 5), dtype=torch.float64, device=state.device)
         self._pre()
         _check(self.lib.tng_surrogate_predict(self.chem.h, self.h, state.data_ptr(), n, max(state.stride(0), n),
                                               dts.data_ptr() if dts is not None else None,

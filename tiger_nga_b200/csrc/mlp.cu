@@ -129,7 +129,7 @@ int mlp_backward(Mlp* m, const float* X, const float* T, const float* w_out, int
   float* dA = dY + (size_t)rows * std::max(H, m->out_pad);
   float* dZ = dA + (size_t)rows * std::max(H, m->out_pad);
   const int nb = std::min(1024, (rows * m->out_pad + 255) / 256);
-  k_mse<<<nb, 256, 0, st>>>(Y, T, w_out, rows, m->n_out, m->out_pad, dY, (float*)m->lossp.ptr);
+  k_mse<<<nb, 256, 0, st>>>(Y, T, w_out, rows, m->n_out, m->out_pad, m->under_weight, dY, (float*)m->lossp.ptr);
   float* gcur = dY;  // gradient w.r.t. the output of the current layer (pre-activation for the last)
   for (int l = m->nlin - 1; l >= 0; --l) {
     const int fi = m->fan_in[l], fo = m->fan_out[l];
@@ -181,22 +181,24 @@ int mlp_adam(Mlp* m, float lr) {
 }
 
 int mlp_train(Mlp* m, const float* X, const float* T, const float* w_out, int64_t n, int epochs, int batch,
-              float lr0, uint64_t seed, float* losses) {
-  if (n < batch) batch = (int)n;
-  if (!m->gather.reserve((size_t)batch * (m->in_pad + m->out_pad) * sizeof(float) + sizeof(int) * (size_t)n))
+              float lr0, uint64_t seed, float* losses, const int* pop, int64_t npop) {
+  const int64_t np = pop ? npop : n;
+  if (np < batch) batch = (int)np;
+  if (batch < 1) return set_error(TNG_ERR_ARG, "mlp train: empty population");
+  if (!m->gather.reserve((size_t)batch * (m->in_pad + m->out_pad) * sizeof(float) + sizeof(int) * (size_t)np))
     return set_error(TNG_ERR_CUDA, "mlp gather buffers");
   float* Xb = (float*)m->gather.ptr;
   float* Tb = Xb + (size_t)batch * m->in_pad;
   int* perm_d = (int*)(Tb + (size_t)batch * m->out_pad);
-  std::vector<int> perm(n);
-  for (int64_t i = 0; i < n; ++i) perm[i] = (int)i;
+  std::vector<int> perm(np);
+  for (int64_t i = 0; i < np; ++i) perm[i] = pop ? pop[i] : (int)i;
   std::mt19937_64 rng(seed);
-  const int64_t steps_per_epoch = n / batch;
+  const int64_t steps_per_epoch = np / batch;
   const int64_t total = steps_per_epoch * epochs;
   int64_t s = 0;
   for (int ep = 0; ep < epochs; ++ep) {
     std::shuffle(perm.begin(), perm.end(), rng);
-    cudaMemcpyAsync(perm_d, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, m->stream);
+    cudaMemcpyAsync(perm_d, perm.data(), sizeof(int) * np, cudaMemcpyHostToDevice, m->stream);
     double lsum = 0.0;
     int nrep = 0;
     for (int64_t b = 0; b < steps_per_epoch; ++b, ++s) {
@@ -292,6 +294,12 @@ int tng_mlp_grad(tng_mlp* p, const float* X, const float* T, const float* w_out,
   if (!p || !X || !T || !w_out || rows <= 0 || rows > (1 << 24)) return set_error(TNG_ERR_ARG, "tng_mlp_grad: bad argument");
   DeviceGuard g(p->m.device);
   return mlp_backward(&p->m, X, T, w_out, (int)rows, loss);
+}
+
+int tng_mlp_set_under_weight(tng_mlp* p, float under) {
+  if (!p || !(under > 0.f)) return set_error(TNG_ERR_ARG, "tng_mlp_set_under_weight: bad argument");
+  p->m.under_weight = under;
+  return TNG_OK;
 }
 
 int tng_mlp_adam_step(tng_mlp* p, float lr) {

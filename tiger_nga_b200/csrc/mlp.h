@@ -21,6 +21,9 @@ struct Mlp {
   float* adam_m = nullptr;
   float* adam_v = nullptr;
   int64_t step = 0;
+  // loss weight of outputs predicted below their target (1: plain weighted MSE); the error gate
+  // is trained with a larger one, so that it errs on the side of over-predicting errors
+  float under_weight = 1.f;
   DevBuf act, pre, work, part, lossp, gather;
 };
 
@@ -29,7 +32,10 @@ void mlp_free(Mlp* m);
 int mlp_forward_f32(Mlp* m, const float* X, int rows, float** Y);
 int mlp_backward(Mlp* m, const float* X, const float* T, const float* w_out, int rows, float* loss);
 int mlp_adam(Mlp* m, float lr);
+// Minibatch Adam with a cosine learning rate over `epochs` passes. An epoch visits the row
+// indices of `pop` (host, npop entries, repeats allowed: a resampled population) in a fresh
+// random order, or every row 0..n-1 when pop is null.
 int mlp_train(Mlp* m, const float* X, const float* T, const float* w_out, int64_t n, int epochs, int batch, float lr0,
-              uint64_t seed, float* losses);
+              uint64_t seed, float* losses, const int* pop = nullptr, int64_t npop = 0);
 
 }  // namespace tng

@@ -113,9 +113,10 @@ __global__ void k_gelu_back(const float* __restrict__ dH, const float* __restric
     dZ[i] = dH[i] * gelu_grad_f(P[i]);
 }
 
-// Loss sum_o w_o (y - t)^2 / (rows * nout) and its gradient; per-block partial sums of the loss.
+// Loss sum_o w_o a(r) (y - t)^2 / (rows * nout), a(r) = under for r = y - t < 0 and 1 otherwise,
+// and its gradient; per-block partial sums of the loss.
 __global__ void k_mse(const float* __restrict__ Y, const float* __restrict__ T, const float* __restrict__ w, int rows,
-                      int nout, int ld, float* __restrict__ dY, float* __restrict__ partial) {
+                      int nout, int ld, float under, float* __restrict__ dY, float* __restrict__ partial) {
   __shared__ float red[256];
   float s = 0.f;
   const float scale = 1.0f / ((float)rows * (float)nout);
@@ -123,7 +124,7 @@ __global__ void k_mse(const float* __restrict__ Y, const float* __restrict__ T, 
        e += (int64_t)gridDim.x * blockDim.x) {
     const int o = (int)(e % ld);
     const float r = Y[e] - T[e];
-    const float wo = o < nout ? w[o] : 0.f;
+    const float wo = o < nout ? (r < 0.f ? under * w[o] : w[o]) : 0.f;
     s += wo * r * r;
     dY[e] = 2.f * wo * r * scale;
   }

@@ -43,14 +43,24 @@ struct SurPost {
   int members;       // ensemble members; outputs of member i at out + i * member_stride
   long long member_stride;
   double ens_tol_K, ens_tol_Y;
+  // the error gate: a network that predicts log10 of this prediction's error relative to the
+  // bars (|dT|/T over 1e-2, max |dY| / max Y over 1e-3); cells above log10(gate_tol) fall back
+  const float* gate_out;  // normalised gate outputs [cell][gate_pad], null: no gate
+  int gate_pad;
+  double gate_mean[2], gate_std[2];
+  double gate_log_tol;
   int* fb_list;      // fallback cells
   int* fb_count;
-  unsigned long long* cnt;  // [accepted, ood, consistency, clip, ensemble]
+  unsigned long long* cnt;  // [accepted, ood, consistency, clip, ensemble, gate]
   double* out_state;  // predict mode: every cell's post-processed state here (state untouched, no list)
   long long ld_out;
   int* reason_out;    // per cell, nullable
-  double* ind_out;    // per cell 3 values, nullable
+  double* ind_out;    // per cell kIndicators values, nullable
 };
+
+// per-cell indicators of tng_surrogate_predict: consistency (K), ensemble T spread (K), ensemble
+// Y spread, gate log10(predicted T error / bar), gate log10(predicted Y error / bar)
+constexpr int kIndicators = 5;
 
 __device__ __forceinline__ void nasa(const double* th, double tmid, int k, double T, double* h, double* cp) {
   const double* a = th + 24 * k + (T > tmid ? 0 : 12);
@@ -405,11 +415,21 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
     if (!reason && !(neg <= a.clip_tol)) reason = 3;
     if (!reason && !(isfinite(T1) && ok)) reason = 2;
     if (!reason && !(sT <= a.ens_tol_K && sY <= a.ens_tol_Y)) reason = 4;
+    double gT = -INFINITY, gY = -INFINITY;
+    if (a.gate_out) {
+      const float* go = a.gate_out + (size_t)cell * a.gate_pad;
+      gT = (double)go[0] * a.gate_std[0] + a.gate_mean[0];
+      gY = (double)go[1] * a.gate_std[1] + a.gate_mean[1];
+      if (!reason && !(gT <= a.gate_log_tol && gY <= a.gate_log_tol)) reason = 5;
+    }
     if (a.reason_out) a.reason_out[cell] = reason;
     if (a.ind_out) {
-      a.ind_out[3 * (size_t)cell] = ok ? ind : INFINITY;
-      a.ind_out[3 * (size_t)cell + 1] = sT;
-      a.ind_out[3 * (size_t)cell + 2] = sY;
+      double* io = a.ind_out + kIndicators * (size_t)cell;
+      io[0] = ok ? ind : INFINITY;
+      io[1] = sT;
+      io[2] = sY;
+      io[3] = gT;
+      io[4] = gY;
     }
     if (a.out_state) {
       for (int k = 0; k < a.ns; ++k) a.out_state[(long long)k * a.ld_out + cell] = rho * y_new(Y0, dY, k, inv_sum);
@@ -488,6 +508,38 @@ __global__ void k_judge(const double* __restrict__ state, long long ld, int ns, 
   }
 }
 
+// Per-cell error of a post-processed prediction against the implicit result, relative to the
+// accuracy bars: r[0] = (|T_s - T_p| / T_p) / 1e-2, r[1] = (max_k |Y_s,k - Y_p,k| / max_k Y_p,k) / 1e-3.
+__global__ void k_sur_errors(const double* __restrict__ pred, long long ldp, const double* __restrict__ ref,
+                             long long ldr, int n, int ns, float* __restrict__ r) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    double rs = 0.0, rr = 0.0, ymax = 0.0, dy = 0.0;
+    for (int k = 0; k < ns; ++k) {
+      rs += pred[(long long)k * ldp + c];
+      rr += ref[(long long)k * ldr + c];
+    }
+    const double irs = 1.0 / rs, irr = 1.0 / rr;
+    for (int k = 0; k < ns; ++k) {
+      const double yr = ref[(long long)k * ldr + c] * irr;
+      ymax = fmax(ymax, yr);
+      dy = fmax(dy, fabs(pred[(long long)k * ldp + c] * irs - yr));
+    }
+    const double Ts = pred[(long long)ns * ldp + c] * irs, Tp = ref[(long long)ns * ldr + c] * irr;
+    r[2 * (size_t)c] = (float)(fabs(Ts - Tp) / Tp / 1e-2);
+    r[2 * (size_t)c + 1] = (float)(dy / ymax / 1e-3);
+  }
+}
+
+// gate targets: log10 of the errors relative to the bars, floored at 1e-4 (normalised later)
+__global__ void k_gate_targets(const float* __restrict__ r, int n, int out_pad, float* __restrict__ T) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    float* t = T + (size_t)c * out_pad;
+    t[0] = log10f(fmaxf(r[2 * (size_t)c], 1e-4f));
+    t[1] = log10f(fmaxf(r[2 * (size_t)c + 1], 1e-4f));
+    for (int i = 2; i < out_pad; ++i) t[i] = 0.f;
+  }
+}
+
 }  // namespace tng
 
 using namespace tng;
@@ -515,6 +567,14 @@ struct tng_surrogate {
   cudaEvent_t ev[5] = {};
   int calls = 0;
   int dbg_wait_limit = 0, dbg_fault = 0;  // test hook of the inference kernel's bounded waits
+  // the error gate (a network of the same hidden shape, 2 outputs); absent until trained or loaded
+  bool has_gate = false;
+  Mlp gate;
+  double gate_mean[2] = {0.0, 0.0}, gate_std[2] = {1.0, 1.0};
+  double gate_tol = 0.25;  // fallback above this fraction of the bars (calibrated, saved with the model)
+  __nv_bfloat16* d_gpack = nullptr;
+  long long g_off[kMaxLayers] = {};
+  DevBuf gout;
 };
 
 static int sur_upload_norm(tng_surrogate* s) {
@@ -536,23 +596,44 @@ static int sur_upload_norm(tng_surrogate* s) {
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate normalisation");
 }
 
-static int sur_pack(tng_surrogate* s) {
-  for (int i = 0; i < s->members; ++i) {
-    long long off = 0;
-    Mlp& mi = s->member(i);
-    for (int l = 0; l < mi.nlin; ++l) {
-      s->w_off[l] = off;
-      const int fo = mi.fan_out[l], fi = mi.fan_in[l];
-      k_pack_weights<<<256, 256, 0, s->m.stream>>>(mi.params + mi.w_off[l], fo, fi, s->d_wpack[i] + off);
-      off += (long long)fo * fi;
-    }
+static void pack_net(tng_surrogate* s, const Mlp& mi, __nv_bfloat16* dst, long long* w_off) {
+  long long off = 0;
+  for (int l = 0; l < mi.nlin; ++l) {
+    w_off[l] = off;
+    const int fo = mi.fan_out[l], fi = mi.fan_in[l];
+    k_pack_weights<<<256, 256, 0, s->m.stream>>>(mi.params + mi.w_off[l], fo, fi, dst + off);
+    off += (long long)fo * fi;
   }
+}
+
+static int sur_pack(tng_surrogate* s) {
+  for (int i = 0; i < s->members; ++i) pack_net(s, s->member(i), s->d_wpack[i], s->w_off);
+  if (s->has_gate) pack_net(s, s->gate, s->d_gpack, s->g_off);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate weight packing");
 }
 
+static int launch_net(tng_chem* h, tng_surrogate* s, const Mlp& net, const __nv_bfloat16* wpack,
+                      const long long* w_off, const double* dstate, int64_t ncells, int64_t dld, const double* ddts,
+                      double dt, double p, float* out, int* err);
+
 static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double* dstate, int64_t ncells, int64_t dld,
                         const double* ddts, double dt, double p, float* out, int* err) {
+  return launch_net(h, s, s->member(member), s->d_wpack[member], s->w_off, dstate, ncells, dld, ddts, dt, p, out, err);
+}
+
+// the gate's outputs for every cell into s->gout (no-op without a gate)
+static int launch_gate(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
+                       const double* ddts, double dt, double p, int* err) {
+  if (!s->has_gate) return TNG_OK;
+  if (!s->gout.reserve((size_t)ncells * s->gate.out_pad * sizeof(float)))
+    return set_error(TNG_ERR_CUDA, "surrogate gate output allocation failed");
+  return launch_net(h, s, s->gate, s->d_gpack, s->g_off, dstate, ncells, dld, ddts, dt, p, (float*)s->gout.ptr, err);
+}
+
+static int launch_net(tng_chem* h, tng_surrogate* s, const Mlp& net, const __nv_bfloat16* wpack,
+                      const long long* w_off, const double* dstate, int64_t ncells, int64_t dld, const double* ddts,
+                      double dt, double p, float* out, int* err) {
   InferArgs ia{};
   ia.state = dstate;
   ia.ld = dld;
@@ -563,23 +644,23 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double*
   ia.ns = s->ns;
   ia.bath = s->bath;
   ia.n_in = s->n_in;
-  ia.in_pad = s->m.in_pad;
-  ia.hidden = s->m.hidden;
-  ia.out_pad = s->m.out_pad;
-  ia.nlin = s->m.nlin;
+  ia.in_pad = net.in_pad;
+  ia.hidden = net.hidden;
+  ia.out_pad = net.out_pad;
+  ia.nlin = net.nlin;
   ia.fmean = s->d_fnorm;
   ia.fistd = s->d_fnorm + s->m.in_pad;
-  ia.wpack = s->d_wpack[member];
-  for (int l = 0; l < s->m.nlin; ++l) {
-    ia.w_off[l] = s->w_off[l];
-    ia.b_off[l] = (int)s->m.b_off[l];
+  ia.wpack = wpack;
+  for (int l = 0; l < net.nlin; ++l) {
+    ia.w_off[l] = w_off[l];
+    ia.b_off[l] = (int)net.b_off[l];
   }
-  ia.bias = s->member(member).params;
+  ia.bias = net.params;
   ia.out = out;
   ia.error = err;
   ia.wait_limit = s->dbg_wait_limit;
   ia.fault = s->dbg_fault;
-  if ((s->m.nlin - 1) * s->m.hidden + s->m.out_pad > kInferMaxBias)
+  if ((net.nlin - 1) * net.hidden + net.out_pad > kInferMaxBias)
     return set_error(TNG_ERR_ARG, "inference: the biases do not fit the kernel's shared-memory stage");
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
   if (e != cudaSuccess) return cuda_error(e, "inference shared memory");
@@ -621,6 +702,13 @@ static SurPost post_args(tng_chem* h, tng_surrogate* s, double* state, int64_t l
   pa.ens_tol_Y = s->cfg.ens_tol_Y;
   pa.E = s->d_E;
   solver_thermo(h, &pa.th, &pa.tmid);
+  if (s->has_gate) {
+    pa.gate_out = (const float*)s->gout.ptr;
+    pa.gate_pad = s->gate.out_pad;
+    for (int i = 0; i < 2; ++i) pa.gate_mean[i] = s->gate_mean[i], pa.gate_std[i] = s->gate_std[i];
+    const double tol = s->cfg.gate_tol > 0.f ? (double)s->cfg.gate_tol : s->gate_tol;
+    pa.gate_log_tol = std::log10(tol);
+  }
   return pa;
 }
 }  // namespace tng
@@ -719,6 +807,9 @@ int tng_surrogate_destroy(tng_surrogate* s) {
   DeviceGuard g(s->m.device);
   cudaStreamSynchronize(s->m.stream);
   for (int i = 0; i < s->members; ++i) mlp_free(&s->member(i));
+  if (s->has_gate) mlp_free(&s->gate);
+  if (s->d_gpack) cudaFree(s->d_gpack);
+  s->gout.release();
   if (s->d_fnorm) cudaFree(s->d_fnorm);
   if (s->d_tnorm) cudaFree(s->d_tnorm);
   if (s->d_E) cudaFree(s->d_E);
@@ -733,48 +824,54 @@ int tng_surrogate_destroy(tng_surrogate* s) {
   return TNG_OK;
 }
 
-int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
-                        int64_t ld, double p, int epochs, int batch, double lr, float* losses) {
-  if (!s || !state0 || !state1 || !dts || n < 16 || ld < n || !(p > 0.0) || n > (1LL << 31) - 1)
-    return set_error(TNG_ERR_ARG, "tng_surrogate_train: bad argument");
-  DeviceGuard g(s->m.device);
+}  // extern "C"
+
+namespace {
+
+// Features and normalised targets of n pairs into s->work: X (n x in_pad), T (n x out_pad). With
+// set_norm the normalisation (feature mean/std/range, target mean/std) is computed from these
+// pairs and uploaded; otherwise the surrogate's stored normalisation is applied.
+int sur_prepare_pairs(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                      int64_t ld, double p, bool set_norm, float** Xo, float** To) {
   const int ip = s->m.in_pad, op = s->m.out_pad;
   cudaStream_t st = s->m.stream;
   if (!s->work.reserve((size_t)n * (ip + op) * sizeof(float) + sizeof(double) * 4 * (ip + op) + 256 * sizeof(float)))
-    return set_error(TNG_ERR_CUDA, "tng_surrogate_train: %lld pairs do not fit", (long long)n);
+    return set_error(TNG_ERR_CUDA, "surrogate training: %lld pairs do not fit", (long long)n);
   float* X = (float*)s->work.ptr;
   float* T = X + (size_t)n * ip;
   double* stats = (double*)(T + (size_t)n * op);
   float* nrm = (float*)(stats + 4 * (ip + op));
   k_sur_features<<<1184, 128, 0, st>>>(state0, ld, (int)n, dts, std::log(p), s->ns, s->bath, ip, X);
   k_sur_targets<<<1184, 128, 0, st>>>(state0, state1, ld, (int)n, s->ns, op, T);
-  k_colstats<<<ip, 256, 0, st>>>(X, (int)n, ip, stats);
-  k_colstats<<<op, 256, 0, st>>>(T, (int)n, op, stats + 4 * ip);
-  std::vector<double> hs(4 * (ip + op));
-  cudaMemcpyAsync(hs.data(), stats, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return cuda_error(e, "surrogate statistics");
-  for (int i = 0; i < s->n_in; ++i) {
-    const double mu = hs[4 * i] / n, var = std::max(hs[4 * i + 1] / n - mu * mu, 0.0);
-    s->fmean[i] = mu;
-    s->fstd[i] = std::max(std::sqrt(var), 1e-3 * std::max(1.0, std::fabs(mu)));
-    s->fmin[i] = hs[4 * i + 2];
-    s->fmax[i] = hs[4 * i + 3];
+  if (set_norm) {
+    k_colstats<<<ip, 256, 0, st>>>(X, (int)n, ip, stats);
+    k_colstats<<<op, 256, 0, st>>>(T, (int)n, op, stats + 4 * ip);
+    std::vector<double> hs(4 * (ip + op));
+    cudaMemcpyAsync(hs.data(), stats, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(e, "surrogate statistics");
+    for (int i = 0; i < s->n_in; ++i) {
+      const double mu = hs[4 * i] / n, var = std::max(hs[4 * i + 1] / n - mu * mu, 0.0);
+      s->fmean[i] = mu;
+      s->fstd[i] = std::max(std::sqrt(var), 1e-3 * std::max(1.0, std::fabs(mu)));
+      s->fmin[i] = hs[4 * i + 2];
+      s->fmax[i] = hs[4 * i + 3];
+    }
+    double shared = 0.0;  // target_mode 1: the RMS spread over the species outputs, one scale for all
+    for (int i = 0; i < s->n_out; ++i) {
+      const double* q = &hs[4 * (ip + i)];
+      const double mu = q[0] / n, var = std::max(q[1] / n - mu * mu, 0.0);
+      s->tmean[i] = mu;
+      s->tstd[i] = std::max(std::sqrt(var), 1e-14);
+      if (i > 0) shared += var;
+    }
+    if (s->cfg.target_mode == 1) {
+      shared = std::max(std::sqrt(shared / std::max(1, s->n_out - 1)), 1e-14);
+      for (int i = 1; i < s->n_out; ++i) s->tstd[i] = shared;
+    }
+    const int rc = sur_upload_norm(s);
+    if (rc) return rc;
   }
-  double shared = 0.0;  // target_mode 1: the RMS spread over the species outputs, one scale for all
-  for (int i = 0; i < s->n_out; ++i) {
-    const double* q = &hs[4 * (ip + i)];
-    const double mu = q[0] / n, var = std::max(q[1] / n - mu * mu, 0.0);
-    s->tmean[i] = mu;
-    s->tstd[i] = std::max(std::sqrt(var), 1e-14);
-    if (i > 0) shared += var;
-  }
-  if (s->cfg.target_mode == 1) {
-    shared = std::max(std::sqrt(shared / std::max(1, s->n_out - 1)), 1e-14);
-    for (int i = 1; i < s->n_out; ++i) s->tstd[i] = shared;
-  }
-  int rc = sur_upload_norm(s);
-  if (rc) return rc;
   std::vector<float> hn(2 * (ip + op), 0.f);
   for (int i = 0; i < s->n_in; ++i) hn[i] = (float)s->fmean[i], hn[ip + i] = (float)(1.0 / s->fstd[i]);
   for (int i = 0; i < s->n_out; ++i)
@@ -782,11 +879,56 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
   cudaMemcpyAsync(nrm, hn.data(), sizeof(float) * hn.size(), cudaMemcpyHostToDevice, st);
   k_normalise<<<2048, 256, 0, st>>>(X, (int)n, ip, s->n_in, nrm, nrm + ip);
   k_normalise<<<2048, 256, 0, st>>>(T, (int)n, op, s->n_out, nrm + 2 * ip, nrm + 2 * ip + op);
+  // the staged normalisation is read by the kernels above before the host vector goes away
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_error(e, "surrogate pairs");
+  *Xo = X;
+  *To = T;
+  return TNG_OK;
+}
+
+// Errors of the current ensemble's post-processed prediction on n pairs, relative to the bars
+// (k_sur_errors), into r (device, 2 floats per pair); predictions run in chunks.
+int sur_pair_errors(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                    int64_t ld, double p, float* r) {
+  const int nv = s->ns + 1;
+  const int64_t chunk = std::min<int64_t>(n, 1 << 20);
+  DevBuf tmp;
+  if (!tmp.reserve((size_t)chunk * nv * sizeof(double))) return set_error(TNG_ERR_CUDA, "surrogate errors: scratch");
+  int rc = TNG_OK;
+  for (int64_t c0 = 0; c0 < n && !rc; c0 += chunk) {
+    const int64_t m = std::min(chunk, n - c0);
+    rc = tng_surrogate_predict(s->h, s, state0 + c0, m, ld, dts + c0, 0.0, p, (double*)tmp.ptr, m, nullptr, nullptr);
+    if (rc) break;
+    k_sur_errors<<<(int)std::min<int64_t>(4096, (m + 127) / 128), 128, 0, s->h->stream>>>(
+        (const double*)tmp.ptr, m, state1 + c0, ld, (int)m, s->ns, r + 2 * c0);
+    cudaError_t e = cudaStreamSynchronize(s->h->stream);
+    if (e != cudaSuccess) rc = cuda_error(e, "surrogate errors");
+  }
+  tmp.release();
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                        int64_t ld, double p, int epochs, int batch, double lr, float* losses) {
+  if (!s || !state0 || !state1 || !dts || n < 16 || ld < n || !(p > 0.0) || n > (1LL << 31) - 1)
+    return set_error(TNG_ERR_ARG, "tng_surrogate_train: bad argument");
+  DeviceGuard g(s->m.device);
+  const int op = s->m.out_pad;
+  cudaStream_t st = s->m.stream;
+  float *X, *T;
+  int rc = sur_prepare_pairs(s, state0, state1, dts, n, ld, p, true, &X, &T);
+  if (rc) return rc;
   // loss weights: every species output equally (outputs are normalised), temperature wT
   std::vector<float> w(op, 0.f);
   const float wT = s->cfg.loss_T_weight > 0.f ? s->cfg.loss_T_weight : 2.f;
   for (int i = 0; i < s->n_out; ++i) w[i] = i == 0 ? wT : 1.f;
   float* dw;
+  cudaError_t e;
   if ((e = cudaMalloc(&dw, sizeof(float) * op)) != cudaSuccess) return cuda_error(e, "loss weights");
   cudaMemcpyAsync(dw, w.data(), sizeof(float) * op, cudaMemcpyHostToDevice, st);
   // every member on the same normalised pairs, from its own initialisation and shuffling order;
@@ -806,27 +948,170 @@ int tng_surrogate_train(tng_surrogate* s, const double* state0, const double* st
   return TNG_OK;
 }
 
+int tng_surrogate_refine(tng_surrogate* s, const double* state0, const double* state1, const double* dts, int64_t n,
+                         int64_t ld, double p, int epochs, int batch, double lr, double boost, float* losses,
+                         int64_t* population) {
+  if (!s || !state0 || !state1 || !dts || n < 16 || ld < n || !(p > 0.0) || n > (1LL << 31) - 1 || epochs < 1 ||
+      !(boost >= 0.0))
+    return set_error(TNG_ERR_ARG, "tng_surrogate_refine: bad argument");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_refine: surrogate not trained or loaded");
+  DeviceGuard g(s->m.device);
+  cudaStream_t st = s->m.stream;
+  float* r;
+  cudaError_t e = cudaMalloc(&r, sizeof(float) * 2 * n);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_refine: errors");
+  int rc = sur_pair_errors(s, state0, state1, dts, n, ld, p, r);
+  std::vector<float> hr(2 * (size_t)n);
+  if (!rc) {
+    e = cudaMemcpy(hr.data(), r, sizeof(float) * hr.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_error(e, "tng_surrogate_refine: errors");
+  }
+  cudaFree(r);
+  if (rc) return rc;
+  // the resampled population: pair i appears 1 + min(round(boost * e_i), 16) times, e_i its
+  // larger error relative to the bars
+  std::vector<int> pop;
+  pop.reserve((size_t)n + n / 4);
+  for (int64_t i = 0; i < n; ++i) {
+    const float ei = std::max(hr[2 * i], hr[2 * i + 1]);
+    const int reps = 1 + (std::isfinite(ei) ? (int)std::min(16.0, std::nearbyint(boost * ei)) : 16);
+    for (int k = 0; k < reps; ++k) pop.push_back((int)i);
+  }
+  if (population) *population = (int64_t)pop.size();
+  float *X, *T;
+  if ((rc = sur_prepare_pairs(s, state0, state1, dts, n, ld, p, false, &X, &T))) return rc;
+  const int op = s->m.out_pad;
+  std::vector<float> w(op, 0.f);
+  const float wT = s->cfg.loss_T_weight > 0.f ? s->cfg.loss_T_weight : 2.f;
+  for (int i = 0; i < s->n_out; ++i) w[i] = i == 0 ? wT : 1.f;
+  float* dw;
+  if ((e = cudaMalloc(&dw, sizeof(float) * op)) != cudaSuccess) return cuda_error(e, "loss weights");
+  cudaMemcpyAsync(dw, w.data(), sizeof(float) * op, cudaMemcpyHostToDevice, st);
+  std::vector<float> lm(epochs);
+  if (losses) std::fill(losses, losses + epochs, 0.f);
+  for (int i = 0; i < s->members && !rc; ++i) {
+    rc = mlp_train(&s->member(i), X, T, dw, n, epochs, batch, (float)lr, s->cfg.seed + 77 + 104729ULL * i, lm.data(),
+                   pop.data(), (int64_t)pop.size());
+    if (losses)
+      for (int ep = 0; ep < epochs; ++ep) losses[ep] += lm[ep] / s->members;
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(dw);
+  if (rc) return rc;
+  return sur_pack(s);
+}
+
+int tng_surrogate_train_gate(tng_surrogate* s, const double* state0, const double* state1, const double* dts,
+                             int64_t n, int64_t ld, double p, int epochs, int batch, double lr, double under,
+                             float* losses) {
+  if (!s || !state0 || !state1 || !dts || n < 16 || ld < n || !(p > 0.0) || n > (1LL << 31) - 1 || epochs < 1 ||
+      !(under > 0.0))
+    return set_error(TNG_ERR_ARG, "tng_surrogate_train_gate: bad argument");
+  if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_train_gate: surrogate not trained or loaded");
+  DeviceGuard g(s->m.device);
+  cudaStream_t st = s->m.stream;
+  int rc;
+  if (!s->has_gate) {
+    if ((rc = mlp_init(&s->gate, s->m.device, st, s->n_in, 2, s->cfg.hidden, s->cfg.layers, s->cfg.seed + 424242ULL)))
+      return rc;
+    cudaError_t e = cudaMalloc(&s->d_gpack, sizeof(__nv_bfloat16) * s->gate.nparam);
+    if (e != cudaSuccess) {
+      mlp_free(&s->gate);
+      return cuda_error(e, "tng_surrogate_train_gate: packed weights");
+    }
+    s->has_gate = true;
+  }
+  const int gp = s->gate.out_pad;
+  // errors of the members (the gate's own verdict plays no part in them)
+  float* r;
+  float* Tg;
+  cudaError_t e = cudaMalloc(&r, sizeof(float) * 2 * n);
+  if (e != cudaSuccess) return cuda_error(e, "tng_surrogate_train_gate: errors");
+  if ((e = cudaMalloc(&Tg, sizeof(float) * (size_t)n * gp + sizeof(double) * 4 * gp + 64)) != cudaSuccess) {
+    cudaFree(r);
+    return cuda_error(e, "tng_surrogate_train_gate: targets");
+  }
+  rc = sur_pair_errors(s, state0, state1, dts, n, ld, p, r);
+  float *X = nullptr, *T = nullptr;
+  if (!rc) rc = sur_prepare_pairs(s, state0, state1, dts, n, ld, p, false, &X, &T);
+  if (!rc) {
+    double* gst = (double*)(Tg + (size_t)n * gp);
+    k_gate_targets<<<1184, 128, 0, st>>>(r, (int)n, gp, Tg);
+    k_colstats<<<2, 256, 0, st>>>(Tg, (int)n, gp, gst);
+    double hs[8];
+    cudaMemcpyAsync(hs, gst, sizeof(hs), cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) rc = cuda_error(e, "gate statistics");
+    if (!rc) {
+      std::vector<float> hn(2 * gp, 0.f);
+      for (int i = 0; i < 2; ++i) {
+        const double mu = hs[4 * i] / n, var = std::max(hs[4 * i + 1] / n - mu * mu, 0.0);
+        s->gate_mean[i] = mu;
+        s->gate_std[i] = std::max(std::sqrt(var), 1e-3);
+        hn[i] = (float)mu;
+        hn[gp + i] = (float)(1.0 / s->gate_std[i]);
+      }
+      float* dn = (float*)(gst + 2 * 4);
+      cudaMemcpyAsync(dn, hn.data(), sizeof(float) * hn.size(), cudaMemcpyHostToDevice, st);
+      k_normalise<<<2048, 256, 0, st>>>(Tg, (int)n, gp, 2, dn, dn + gp);
+      std::vector<float> w(gp, 0.f);
+      w[0] = w[1] = 1.f;
+      float* dw = dn + 2 * gp;
+      cudaMemcpyAsync(dw, w.data(), sizeof(float) * gp, cudaMemcpyHostToDevice, st);
+      s->gate.under_weight = (float)under;
+      rc = mlp_train(&s->gate, X, Tg, dw, n, epochs, batch, (float)lr, s->cfg.seed + 99991ULL, losses);
+      cudaStreamSynchronize(st);
+    }
+  }
+  cudaFree(r);
+  cudaFree(Tg);
+  if (rc) return rc;
+  return sur_pack(s);
+}
+
+int tng_surrogate_set_gate_tol(tng_surrogate* s, double tol) {
+  if (!s || !(tol > 0.0)) return set_error(TNG_ERR_ARG, "tng_surrogate_set_gate_tol: bad argument");
+  if (!s->has_gate) return set_error(TNG_ERR_STATE, "tng_surrogate_set_gate_tol: the surrogate has no error gate");
+  s->gate_tol = tol;
+  return TNG_OK;
+}
+
+int tng_surrogate_gate_info(const tng_surrogate* s, int* has_gate, double* tol) {
+  if (!s) return set_error(TNG_ERR_ARG, "tng_surrogate_gate_info: null handle");
+  if (has_gate) *has_gate = s->has_gate ? 1 : 0;
+  if (tol) *tol = s->cfg.gate_tol > 0.f ? (double)s->cfg.gate_tol : s->gate_tol;
+  return TNG_OK;
+}
+
 int tng_surrogate_save(const tng_surrogate* s, const char* path) {
   if (!s || !path) return set_error(TNG_ERR_ARG, "tng_surrogate_save: null argument");
   if (!s->trained) return set_error(TNG_ERR_STATE, "tng_surrogate_save: surrogate not trained");
   std::vector<float> params(s->m.nparam * s->members);
+  std::vector<float> gparams(s->has_gate ? s->gate.nparam : 0);
   DeviceGuard g(s->m.device);
   cudaStreamSynchronize(s->m.stream);
   for (int i = 0; i < s->members; ++i)
     cudaMemcpy(params.data() + i * s->m.nparam, s->member(i).params, sizeof(float) * s->m.nparam,
                cudaMemcpyDeviceToHost);
+  if (s->has_gate) cudaMemcpy(gparams.data(), s->gate.params, sizeof(float) * s->gate.nparam, cudaMemcpyDeviceToHost);
   FILE* f = std::fopen(path, "wb");
   if (!f) return set_error(TNG_ERR_ARG, "tng_surrogate_save: cannot open %s", path);
-  char magic[8] = {'T', 'N', 'G', 'S', 'U', 'R', '2', 0};
+  char magic[8] = {'T', 'N', 'G', 'S', 'U', 'R', '3', 0};
   char mech[32] = {};
   std::snprintf(mech, sizeof(mech), "%s", s->h->ops->name);
-  int hdr[8] = {s->ns, s->n_in, s->n_out, s->cfg.hidden, s->cfg.layers, s->bath, s->h->cfg.literal_mode, s->members};
+  int hdr[10] = {s->ns, s->n_in, s->n_out, s->cfg.hidden, s->cfg.layers, s->bath, s->h->cfg.literal_mode, s->members,
+                 s->has_gate ? 1 : 0, 0};
   int64_t np = s->m.nparam;
-  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(mech, 1, 32, f) == 32 && std::fwrite(hdr, 4, 8, f) == 8 &&
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(mech, 1, 32, f) == 32 && std::fwrite(hdr, 4, 10, f) == 10 &&
             std::fwrite(&np, 8, 1, f) == 1;
   for (const std::vector<double>* v : {&s->fmean, &s->fstd, &s->fmin, &s->fmax, &s->tmean, &s->tstd})
     ok = ok && std::fwrite(v->data(), 8, v->size(), f) == v->size();
   ok = ok && std::fwrite(params.data(), 4, params.size(), f) == params.size();
+  if (s->has_gate) {
+    const int64_t gnp = s->gate.nparam;
+    const double gd[5] = {s->gate_mean[0], s->gate_mean[1], s->gate_std[0], s->gate_std[1], s->gate_tol};
+    ok = ok && std::fwrite(&gnp, 8, 1, f) == 1 && std::fwrite(gd, 8, 5, f) == 5 &&
+         std::fwrite(gparams.data(), 4, gparams.size(), f) == gparams.size();
+  }
   std::fclose(f);
   return ok ? TNG_OK : set_error(TNG_ERR_ARG, "tng_surrogate_save: write failed");
 }
@@ -836,16 +1121,19 @@ int tng_surrogate_load(tng_surrogate* s, const char* path) {
   FILE* f = std::fopen(path, "rb");
   if (!f) return set_error(TNG_ERR_ARG, "tng_surrogate_load: cannot open %s", path);
   char magic[8], mech[32];
-  int hdr[8];
+  int hdr[10] = {};
   int64_t np = 0;
-  bool ok = std::fread(magic, 1, 8, f) == 8 && std::fread(mech, 1, 32, f) == 32 && std::fread(hdr, 4, 8, f) == 8 &&
-            std::fread(&np, 8, 1, f) == 1;
-  if (!ok || std::memcmp(magic, "TNGSUR2", 8) != 0) {
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::fread(mech, 1, 32, f) == 32;
+  // TNGSUR2: 8 header ints, no gate; TNGSUR3: 10 header ints, hdr[8] = gate present
+  const bool v3 = ok && std::memcmp(magic, "TNGSUR3", 8) == 0;
+  if (!ok || (!v3 && std::memcmp(magic, "TNGSUR2", 8) != 0)) {
     std::fclose(f);
     return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is not a surrogate file", path);
   }
+  const int nh = v3 ? 10 : 8;
+  ok = std::fread(hdr, 4, nh, f) == (size_t)nh && std::fread(&np, 8, 1, f) == 1;
   mech[31] = 0;
-  if (std::strcmp(mech, s->h->ops->name) != 0 || hdr[0] != s->ns || hdr[1] != s->n_in || hdr[2] != s->n_out ||
+  if (!ok || std::strcmp(mech, s->h->ops->name) != 0 || hdr[0] != s->ns || hdr[1] != s->n_in || hdr[2] != s->n_out ||
       hdr[3] != s->cfg.hidden || hdr[4] != s->cfg.layers || np != s->m.nparam) {
     std::fclose(f);
     return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s was trained for %s with other sizes", path, mech);
@@ -859,11 +1147,38 @@ int tng_surrogate_load(tng_surrogate* s, const char* path) {
     ok = ok && std::fread(v->data(), 8, v->size(), f) == v->size();
   std::vector<float> params(np * s->members);
   ok = ok && std::fread(params.data(), 4, params.size(), f) == params.size();
+  const bool gate = v3 && hdr[8] == 1;
+  std::vector<float> gparams;
+  double gd[5] = {0.0, 0.0, 1.0, 1.0, 0.25};
+  int64_t gnp = 0;
+  if (ok && gate) {
+    ok = std::fread(&gnp, 8, 1, f) == 1 && std::fread(gd, 8, 5, f) == 5 && gnp > 0 && gnp < (1LL << 30);
+    if (ok) {
+      gparams.resize(gnp);
+      ok = std::fread(gparams.data(), 4, gparams.size(), f) == gparams.size();
+    }
+  }
   std::fclose(f);
   if (!ok) return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s is truncated", path);
   DeviceGuard g(s->m.device);
   for (int i = 0; i < s->members; ++i)
     cudaMemcpy(s->member(i).params, params.data() + i * np, sizeof(float) * np, cudaMemcpyHostToDevice);
+  if (gate) {
+    if (!s->has_gate) {
+      int rc = mlp_init(&s->gate, s->m.device, s->m.stream, s->n_in, 2, s->cfg.hidden, s->cfg.layers, 0);
+      if (rc) return rc;
+      cudaError_t e = cudaMalloc(&s->d_gpack, sizeof(__nv_bfloat16) * s->gate.nparam);
+      if (e != cudaSuccess) {
+        mlp_free(&s->gate);
+        return cuda_error(e, "tng_surrogate_load: gate weights");
+      }
+      s->has_gate = true;
+    }
+    if (gnp != s->gate.nparam) return set_error(TNG_ERR_ARG, "tng_surrogate_load: %s: gate of another size", path);
+    cudaMemcpy(s->gate.params, gparams.data(), sizeof(float) * gnp, cudaMemcpyHostToDevice);
+    s->gate_mean[0] = gd[0], s->gate_mean[1] = gd[1], s->gate_std[0] = gd[2], s->gate_std[1] = gd[3];
+    s->gate_tol = gd[4];
+  }
   int rc = sur_upload_norm(s);
   if (rc) return rc;
   if ((rc = sur_pack(s))) return rc;
@@ -1036,6 +1351,7 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   for (int i = 0; i < s->members && !rc; ++i)
     rc = launch_infer(h, s, i, dstate, ncells, dld, ddts, dt, p,
                       (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad, (int*)(cnt + 8));
+  if (!rc) rc = launch_gate(h, s, dstate, ncells, dld, ddts, dt, p, (int*)(cnt + 8));
   if (rc) return rc;
   cudaEventRecord(s->ev[1], st);
   // post-processing and fallback list
@@ -1093,8 +1409,9 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
       cudaEventElapsedTime(&d, s->ev[0], s->ev[3]);
       stats->ms_infer = a, stats->ms_post = b, stats->ms_fallback = c, stats->ms_total = d;
       stats->fallback = fst;
-      stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3] + hc[4]);
+      stats->fallback.cells = (int64_t)(hc[1] + hc[2] + hc[3] + hc[4] + hc[5]);
       stats->fallback_ensemble = (int64_t)hc[4];
+      stats->fallback_gate = (int64_t)hc[5];
     }
   }
   return TNG_OK;
@@ -1121,6 +1438,7 @@ int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, in
   for (int i = 0; i < s->members && !rc; ++i)
     rc = launch_infer(h, s, i, state, ncells, ld, dts, dt, p, (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad,
                       (int*)(cnt + 8));
+  if (!rc) rc = launch_gate(h, s, state, ncells, ld, dts, dt, p, (int*)(cnt + 8));
   if (rc) return rc;
   SurPost pa = post_args(h, s, const_cast<double*>(state), ld, ncells, dts, dt, p);
   pa.out_state = out;

@@ -139,6 +139,32 @@ def make_onpolicy_pairs(chem, sur, n_pairs: int, seed: int, dt: float = 2e-6, su
     return s0[:, :done].contiguous(), s1[:, :done].contiguous(), d
 
 
+def errors_vs(chem, y, ref):
+    """Per-cell errors of states y against ref relative to the bars: (|dT|/T) / 1e-2 and
+    (max |dY| / max Y) / 1e-3, as numpy arrays."""
+    ns = chem.nspecies
+    ry, rr = y[:ns].sum(0), ref[:ns].sum(0)
+    eT = ((y[ns] / ry - ref[ns] / rr).abs() / (ref[ns] / rr)) / 1e-2
+    eY = ((y[:ns] / ry - ref[:ns] / rr).abs().amax(0) / (ref[:ns] / rr).amax(0)) / 1e-3
+    return eT.cpu().numpy(), eY.cpu().numpy()
+
+
+def calibrate_gate(chem, sur, s0, d, ref, margin: float = 0.7):
+    """The gate threshold on held-out cells: the largest tolerance (fraction of the bars) at which
+    every cell the surrogate accepts has both errors within ``margin`` of the bars. Returns
+    (tol, accepted fraction at tol, max error ratio of the accepted cells)."""
+    pred, reason, ind = sur.predict(s0, d, P_ATM)
+    eT, eY = errors_vs(chem, pred, ref)
+    r = np.maximum(eT, eY)
+    reason = reason.cpu().numpy()
+    g = np.maximum(ind[:, 3].cpu().numpy(), ind[:, 4].cpu().numpy())
+    other = (reason == 0) | (reason == 5)  # accepted apart from the gate
+    viol = other & ~(r <= margin)
+    t = float(g[viol].min()) - 1e-6 if viol.any() else float(g[other].max())
+    acc = other & (g <= t)
+    return 10.0 ** t, float(acc.mean()), float(r[acc].max()) if acc.any() else 0.0
+
+
 def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.0, 2.0, 4.0),
              ens_Y=(1e-4, 2e-4, 5e-4, 1e-3), dist: str = "uneven"):
     """The surrogate against the plain solve on n fresh cells.
@@ -200,7 +226,7 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.
         "cells": n, "plain_s": t_plain, "surrogate_s": t_sur, "speedup": t_plain / t_sur,
         "accepted": st["accepted"], "fallback": st["fallback"]["cells"], "fallback_ood": st["fallback_ood"],
         "fallback_consistency": st["fallback_consistency"], "fallback_clip": st["fallback_clip"],
-        "fallback_ensemble": st["fallback_ensemble"],
+        "fallback_ensemble": st["fallback_ensemble"], "fallback_gate": st["fallback_gate"],
         "max_rel_T": float(errT_run.max()), "p99_rel_T": float(np.quantile(errT_run, 0.99)),
         "max_dY_over_maxY": float(errY_run.max()), "p99_dY_over_maxY": float(np.quantile(errY_run, 0.99)),
         "judge_max_rel_dT": st["judge_max_rel_dT"], "judge_max_dY": st["judge_max_dY"],
@@ -225,7 +251,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--eval-cells", type=int, default=1 << 18)
+    ap.add_argument("--eval-cells", type=int, default=1 << 21)
     ap.add_argument("--target-mode", type=int, default=1)
     ap.add_argument("--post-mode", type=int, default=1)
     ap.add_argument("--members", type=int, default=2)
@@ -236,6 +262,16 @@ def main(argv=None):
     ap.add_argument("--onpolicy", default="", help="a trained surrogate: part of the pairs come from the states "
                     "its own sweep visits (mixing-layer distribution)")
     ap.add_argument("--onpolicy-frac", type=float, default=0.5)
+    ap.add_argument("--refine-epochs", type=int, default=20, help="hard-example refinement epochs (0: none)")
+    ap.add_argument("--refine-lr", type=float, default=5e-4)
+    ap.add_argument("--boost", type=float, default=4.0, help="refinement: extra copies per unit of error/bar")
+    ap.add_argument("--gate-pairs", type=int, default=1 << 22, help="held-out pairs the error gate is trained on "
+                    "(0: no gate)")
+    ap.add_argument("--gate-epochs", type=int, default=30)
+    ap.add_argument("--gate-under", type=float, default=4.0)
+    ap.add_argument("--calib-cells", type=int, default=1 << 21, help="held-out cells that calibrate the gate")
+    ap.add_argument("--calib-margin", type=float, default=0.7, help="accepted cells stay within this fraction of "
+                    "the bars on the calibration cells")
     a = ap.parse_args(argv)
     chem = capi.FiniteChem(a.mech, "fp64")
     t0 = time.perf_counter()
@@ -259,7 +295,31 @@ def main(argv=None):
     t0 = time.perf_counter()
     losses = sur.train(s0, s1, d, P_ATM, epochs=a.epochs, batch=a.batch, lr=a.lr)
     t_train = time.perf_counter() - t0
+    refine = {}
+    if a.refine_epochs > 0:
+        t0 = time.perf_counter()
+        rl, pop = sur.refine(s0, s1, d, P_ATM, epochs=a.refine_epochs, batch=a.batch, lr=a.refine_lr, boost=a.boost)
+        refine = {"epochs": a.refine_epochs, "lr": a.refine_lr, "boost": a.boost, "population": pop,
+                  "losses": [float(v) for v in rl], "s": time.perf_counter() - t0}
     del s0, s1, d
+    gate = {}
+    if a.gate_pairs > 0 and a.dist == "uneven":
+        # the gate learns the ensemble's errors on pairs it was not trained on, and its threshold
+        # is calibrated on further held-out cells against the plain solve
+        import torch
+
+        t0 = time.perf_counter()
+        g0, g1, gd, _ = make_pairs(chem, a.gate_pairs, a.seed + 50021)
+        gl = sur.train_gate(g0, g1, gd, P_ATM, epochs=a.gate_epochs, batch=a.batch, lr=a.lr, under=a.gate_under)
+        del g0, g1, gd
+        c0, c1, cd, _ = make_pairs(chem, a.calib_cells, a.seed + 70001)
+        tol, acc, rmax = calibrate_gate(chem, sur, c0, cd, c1, margin=a.calib_margin)
+        sur.set_gate_tol(tol)
+        del c0, c1, cd
+        torch.cuda.empty_cache()
+        gate = {"pairs": a.gate_pairs, "epochs": a.gate_epochs, "under": a.gate_under, "losses": [float(v) for v in gl],
+                "calib_cells": a.calib_cells, "calib_margin": a.calib_margin, "tol": tol,
+                "calib_accepted": acc, "calib_max_err_ratio": rmax, "s": time.perf_counter() - t0}
     sur.save(a.out)
     ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991, dist=a.dist)
     if a.cells_out:
@@ -270,7 +330,7 @@ def main(argv=None):
            "members": a.members,
            "consist_tol_K": a.consist_tol,
            "pairs_s": t_pairs, "plain_solve_s": solve_s, "train_s": t_train,
-           "losses": [float(v) for v in losses], "eval": ev}
+           "losses": [float(v) for v in losses], "refine": refine, "gate": gate, "eval": ev}
     with open(a.out + ".json", "w") as f:
         json.dump(log, f, indent=1)
     print(json.dumps(log))
