@@ -774,6 +774,18 @@ def solver_header(name: str) -> str:
     out.append(f"static const SvLayout {name}_sv_layout = {{{{{sz}}}, {{{', '.join(map(str, hdo))}}}, "
                f"{{{', '.join(map(str, hio))}}}, {{{', '.join(map(str, cio))}}}, {len(hdf[0])}, {len(hif)}, "
                f"{len(cif)}}};")
+    # the same layout as compile-time constants: the solver kernels are specialised on it
+    def cfun(fname, vals):
+        cases = " ".join(f"case {i}: return {v};" for i, v in enumerate(vals))
+        return (f"  __host__ __device__ static constexpr int {fname}(int k) {{ switch (k) {{ {cases} default: return 0; }} }}")
+
+    out.append(f"struct SvL_{name} {{")
+    out.append(cfun("size", [t["sizes"][k] for k in SV_SIZE_KEYS]))
+    out.append(cfun("hd", hdo))
+    out.append(cfun("hi", hio))
+    out.append(cfun("ci", cio))
+    out.append(f"  static constexpr int nhd = {len(hdf[0])}, nhi = {len(hif)}, nci = {len(cif)};")
+    out.append("};")
     out.append("}  // namespace tng")
     return "\n".join(out) + "\n"
 

@@ -10,11 +10,9 @@ struct BdfCoef {
   double errc[kQmax + 2], dnc[kQmax + 2], upc[kQmax + 2];
 };
 
-// BDF coefficients in constant memory (indexed by the run-time order q).
-__constant__ BdfCoef c_bdf;
-
 struct BdfLaunch {
   BdfArgs a;
+  const BdfCoef* coef;  // device copy of the BDF coefficients (staged into shared memory per block)
   const int* n_in_dev;  // when non-null, the number of queued cells is read from device memory
   int cold_in_smem;     // the Jacobian's term lists staged in shared memory (after the hot tables)
 };
@@ -90,11 +88,11 @@ __device__ __forceinline__ void zset(double (&z)[kQmax + 2][2], const int j, con
 
 // Integrate one cell (warp-cooperative). Returns true when the cell is finished (any status),
 // false when it used up the pass budget and was saved for the next pass.
-__device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, const WarpMem& w, const int cell,
-                                         const int lane) {
+template <class LY>
+__device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, const SvT<LY>& t, const WarpMem& w,
+                                         const int cell, const int lane) {
   const BdfArgs& a = P.a;
-  const BdfCoef& C = c_bdf;
-  const int ns = t.L.size[SZ_NS], nv = ns + 1, rs = a.rs;
+  constexpr int ns = SvT<LY>::NS, nv = ns + 1, rs = SvT<LY>::RS;
   const double dt = a.dts ? a.dts[cell] : a.dt_scalar;
   const double p = a.p, rtol = a.rtol, atol = a.atol;
   const bool h0 = lane < nv, h1 = lane + 32 < nv;
@@ -131,7 +129,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
     ewt[0] = h0 ? 1.0 / (rtol * fabs(u0) + atol) : 0.0;
     ewt[1] = h1 ? 1.0 / (rtol * fabs(u1) + atol) : 0.0;
     {
-      const double2 r = rhs_call(t, w, u0, u1, p, lane);
+      const double2 r = rhs_call(t, w.mat, u0, u1, p, lane);
       f[0] = r.x, f[1] = r.y;
     }
     if (!warp_all_finite(f[0], f[1], nv, lane)) {
@@ -153,7 +151,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
         hnew = hlb;
       } else {
         for (int it = 0; it < 4; ++it) {
-          const double2 gg = rhs_call(t, w, u0 + hg * f[0], u1 + hg * f[1], p, lane);
+          const double2 gg = rhs_call(t, w.mat, u0 + hg * f[0], u1 + hg * f[1], p, lane);
           const double g0 = gg.x, g1 = gg.y;
           const double ydd = wrms2((g0 - f[0]) / hg, (g1 - f[1]) / hg, ewt[0], ewt[1], nv, lane);
           hnew = (ydd * hub * hub > 2.0) ? sqrt(2.0 / ydd) : sqrt(hg * hub);
@@ -225,16 +223,16 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
         bool jcur = false;
         if (need_j || nst >= nst_lu + msbp || fabs(gamma / gamma_lu - 1.0) > dgmax) {
           {
-            const double2 r = rhs_call(t, w, z[0][0], z[0][1], p, lane);
+            const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane);
             f[0] = r.x, f[1] = r.y;
           }
-          jac_call(t, w, rs, z[0][0], z[0][1], f[0], f[1], p, lane);
+          jac_call(t, w.mat, z[0][0], z[0][1], f[0], f[1], p, lane);
           ++nje;
           for (int e = lane; e < nv * rs; e += 32) w.mat[e] = -gamma * w.mat[e];
           __syncwarp();
           for (int i = lane; i < nv; i += 32) w.mat[i * rs + i] += 1.0;
           __syncwarp();
-          const int sing = lu_call(w.mat, nv, rs, w.piv, w.perm, w.cb, lane);
+          const int sing = lu_call<LY>(w.mat, lane);
           gamma_lu = gamma;
           nst_lu = nst;
           jcur = true;
@@ -250,7 +248,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
           conv_fail = true;
           for (int it = 0; it < maxcor; ++it) {
             {
-              const double2 r = rhs_call(t, w, y[0], y[1], p, lane);
+              const double2 r = rhs_call(t, w.mat, y[0], y[1], p, lane);
               f[0] = r.x, f[1] = r.y;
             }
             ++nni;
@@ -310,7 +308,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const SvDev& t, con
             h *= 0.1;
             q = 1;
             {
-              const double2 r = rhs_call(t, w, z[0][0], z[0][1], p, lane);
+              const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane);
               f[0] = r.x, f[1] = r.y;
             }
             z[1][0] = h * f[0];
@@ -422,20 +420,28 @@ finish:
 // Shared memory of one block: the staged hot tables, then one workspace per warp.
 __host__ __device__ inline int hot_smem_doubles(const SvLayout& L) { return (hot_smem_bytes(L) + 15) / 16 * 2; }
 
-// One block per SM of WARPS warps (the staged tables are shared by the block's warps). TAG keeps
-// the instantiations of different translation units apart: each unit has its own constant bank
-// (c_bdf), so two units must not register the same kernel symbol.
-template <int WARPS, int MINB = 1, int TAG = 0>
+// BDF coefficients (l-vectors per order, error constants) as the host computes them.
+BdfCoef make_coef();
+
+// One block per SM of WARPS warps (the staged tables are shared by the block's warps),
+// specialised on the mechanism's layout LY; instantiated once per mechanism (generated unit).
+template <class LY, int WARPS, int MINB = 1>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_bdf(const BdfLaunch P) {
   extern __shared__ __align__(16) double smem[];
-  SvDev t = stage_tables(P.a.tab, smem);
-  size_t off = hot_smem_doubles(t.L);
+  __shared__ BdfCoef s_coef;
+  {
+    const double* src = reinterpret_cast<const double*>(P.coef);
+    double* dst = reinterpret_cast<double*>(&s_coef);
+    for (int e = threadIdx.x; e < (int)(sizeof(BdfCoef) / sizeof(double)); e += blockDim.x) dst[e] = src[e];
+  }
+  SvT<LY> t = stage_tables<LY>(P.a.tab, smem);  // synchronises the block
+  size_t off = hot_smem_doubles(P.a.tab.L);
   if (P.cold_in_smem) {
-    t = stage_cold_tables(t, smem + off);
-    off += cold_smem_doubles(t.L);
+    t = stage_cold_tables<LY>(t, smem + off);
+    off += cold_smem_doubles(P.a.tab.L);
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpMem w = warp_mem(smem + off + (size_t)warp * P.a.smem_warp, t.L, P.a.rs);
+  const WarpMem w = warp_mem<LY>(smem + off + (size_t)warp * P.a.smem_warp);
   const int n_in = P.n_in_dev ? *P.n_in_dev : P.a.n_in;
   for (;;) {
     int idx = 0;
@@ -443,33 +449,48 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_bdf(const BdfLaunch P) {
     idx = __shfl_sync(kFull, idx, 0);
     if (idx >= n_in) break;
     const int cell = P.a.queue_in ? P.a.queue_in[idx] : idx;
-    bdf_cell(P, t, w, cell, lane);
+    bdf_cell<LY>(P, s_coef, t, w, cell, lane);
   }
 }
 
 // Standalone right-hand side / Jacobian of the table-driven warp path (parity checks).
-template <int WARPS>
+template <class LY, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
     k_warp_rhs_jac(SvDev g, const double* __restrict__ state, long long ld, int n, double p, double* __restrict__ rhs,
-                   double* __restrict__ jac, int rs, int smem_warp) {
+                   double* __restrict__ jac, int smem_warp) {
   extern __shared__ __align__(16) double smem[];
-  const SvDev t = stage_tables(g, smem);
+  const SvT<LY> t = stage_tables<LY>(g, smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const WarpMem w = warp_mem(smem + hot_smem_doubles(t.L) + (size_t)warp * smem_warp, t.L, rs);
-  const int nv = t.L.size[SZ_NV];
+  const WarpMem w = warp_mem<LY>(smem + hot_smem_doubles(g.L) + (size_t)warp * smem_warp);
+  constexpr int nv = SvT<LY>::NV, rs = SvT<LY>::RS;
   for (int cell = blockIdx.x * WARPS + warp; cell < n; cell += gridDim.x * WARPS) {
     const double y0 = lane < nv ? state[(long long)lane * ld + cell] : 0.0;
     const double y1 = lane + 32 < nv ? state[(long long)(lane + 32) * ld + cell] : 0.0;
-    const double2 r = rhs_call(t, w, y0, y1, p, lane);
+    const double2 r = rhs_call(t, w.mat, y0, y1, p, lane);
     const double f0 = r.x, f1 = r.y;
     if (lane < nv) rhs[(long long)lane * ld + cell] = f0;
     if (lane + 32 < nv) rhs[(long long)(lane + 32) * ld + cell] = f1;
     if (jac) {
-      jac_call(t, w, rs, y0, y1, f0, f1, p, lane);
+      jac_call(t, w.mat, y0, y1, f0, f1, p, lane);
       for (int e = lane; e < nv * nv; e += 32) jac[(long long)cell * nv * nv + e] = w.mat[(e / nv) * rs + e % nv];
       __syncwarp();
     }
   }
+}
+
+// The solver kernels of one mechanism (instantiated in the mechanism's generated unit and
+// reached through its operation table).
+typedef void (*BdfKernelFn)(const BdfLaunch);
+typedef void (*RhsJacFn)(SvDev, const double*, long long, int, double, double*, double*, int);
+struct SolverKernels {
+  BdfKernelFn bdf2, bdf4, bdf8, bdf8_occ2;  // warps per block; bdf8_occ2: two blocks per SM (128 registers)
+  RhsJacFn rhs_jac4;
+};
+
+template <class LY>
+const SolverKernels* solver_kernels() {
+  static const SolverKernels k = {k_bdf<LY, 2>, k_bdf<LY, 4>, k_bdf<LY, 8>, k_bdf<LY, 8, 2>, k_warp_rhs_jac<LY, 4>};
+  return &k;
 }
 
 static __global__ void k_reset_counters(int* a, int* b) {

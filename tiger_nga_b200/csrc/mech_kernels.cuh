@@ -8,7 +8,7 @@ namespace tng {
 template <class Mech>
 MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int nelem, const char* const* elements,
                  const double* elem, const SvLayout* svl, const double* hd0, const double* hd1, const int* hi,
-                 const int* ci) {
+                 const int* ci, const SolverKernels* sk) {
   MechOps o{};
   o.name = Mech::NAME;
   o.ns = Mech::NS;
@@ -26,6 +26,7 @@ MechOps make_ops(const char* const* species, const double (*wmol)[Mech::NS], int
   o.sv_hd[1] = hd1;
   o.sv_hi = hi;
   o.sv_ci = ci;
+  o.sk = sk;
   o.props = &launch_props<Mech>;
   return o;
 }

@@ -1,16 +1,20 @@
 // K4: surrogate inference on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// One persistent CTA per SM walks tiles of 128 cells. For each tile:
-//   1. the 128 threads compute the cell features from the FP64 state (one cell per thread,
-//      species-major loads) and store them as BF16 into shared memory in the UMMA canonical
-//      K-major layout (8-row x 16-byte core matrices);
-//   2. every layer is D[128 x N] = H[128 x K] * W^T on tcgen05.mma (kind::f16, BF16 operands,
-//      FP32 accumulator in tensor memory); one elected thread issues the MMAs, weights stream
-//      from global memory (L2-resident, shared by all CTAs) into a two-stage shared-memory ring
-//      with cp.async.bulk + mbarrier transaction counts; tcgen05.commit releases ring stages;
-//   3. the epilogue (all 128 threads, each owning one accumulator row = one TMEM lane) reads D
-//      with tcgen05.ld, adds the bias, applies GELU and writes the next layer's BF16 operand back
-//      into shared memory; the last layer's FP32 outputs go to global memory.
+// One launch evaluates every network of the surrogate (the ensemble members and the error gate)
+// on the same cells. Persistent CTAs (two per SM) walk tiles of 128 cells. For each tile:
+//   1. features: the 256 threads split each cell's species between two threads, issue all their
+//      FP64 state loads at once (one memory latency per tile, not one per species), form the
+//      density, temperature and the normalised inputs, and keep them packed as BF16 in registers;
+//   2. for each network, the features are written into shared memory (UMMA canonical K-major
+//      layout, 8-row x 16-byte core matrices) and every layer is D[128 x N] = H[128 x K] * W^T on
+//      tcgen05.mma (kind::f16, BF16 operands, FP32 accumulator in tensor memory); one elected
+//      thread issues the MMAs, weights stream from global memory (L2-resident, shared by all
+//      CTAs) into a two-stage shared-memory ring with cp.async.bulk + mbarrier transaction
+//      counts, and the next layer's (next network's, next tile's) first chunk is fetched while the
+//      epilogue runs; tcgen05.commit releases ring stages;
+//   3. the epilogue (8 warps, two per tensor-memory lane quarter) reads D with tcgen05.ld, adds
+//      the bias, applies GELU and writes the next layer's BF16 operand back into shared memory;
+//      the last layer's FP32 outputs go to the network's output array.
 // Every wait is bounded: on expiry the CTA records an error code and stops issuing work.
 #pragma once
 #include <cuda_bf16.h>
@@ -21,10 +25,21 @@ namespace tng {
 
 constexpr int kInferRows = 128;
 constexpr int kInferThreads = 256;  // 8 warps: two per TMEM lane quarter
-constexpr int kInferMaxBias = 8 * 256 + 256;  // biases of every layer staged in shared memory
 constexpr int kWChunkK = 32;   // K width of one streamed weight chunk (two MMAs)
 constexpr int kWStages = 2;    // weight stages: one chunk in flight ahead of the MMA
 constexpr int kMaxLayers = 9;
+constexpr int kMaxNets = 5;    // ensemble members and the error gate
+constexpr int kFeatSpecies = 24;  // species per feature thread (two threads per cell): ns <= 48
+
+// One network of the launch: hidden layers of the launch's shared shape, its own last layer.
+struct InferNet {
+  const __nv_bfloat16* wpack;   // all layers, chunked canonical layout
+  long long w_off[kMaxLayers];  // element offset of layer l in wpack
+  const float* bias;            // all layers, fan_out entries each
+  int b_off[kMaxLayers];        // offset of layer l's bias in `bias`
+  int out_pad;                  // width of the last layer (multiple of 16)
+  float* out;                   // [ncells x out_pad] FP32 (normalised predictions)
+};
 
 struct InferArgs {
   const double* state;  // species-major [v*ld + cell]
@@ -35,14 +50,11 @@ struct InferArgs {
   double logp;        // log(pressure)
   int ns;             // species count
   int bath;           // species index left out of the inputs (the bath gas)
-  int n_in, in_pad, hidden, out_pad, nlin;
+  int n_in, in_pad, hidden, nlin;
   const float* fmean;  // feature normalisation, n_in entries
   const float* fistd;  // 1/std
-  const __nv_bfloat16* wpack;  // all layers, chunked canonical layout
-  long long w_off[kMaxLayers];  // element offset of layer l in wpack
-  const float* bias;            // all layers, fan_out entries each
-  int b_off[kMaxLayers];
-  float* out;  // [ncells x out_pad] FP32 (normalised predictions)
+  int nnets;
+  InferNet net[kMaxNets];
   int* error;  // non-zero after a timed-out wait
   // test hook: polls before a wait gives up (0: the default 2^24), and fault = 1 withholds the
   // first layer's completion signal of each CTA's first tile so that the epilogue's wait runs
@@ -165,11 +177,14 @@ __device__ __forceinline__ float gelu_fast(float x) {
 
 // shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), two weight stages of
 // 256 x 32 bf16 (16 KB each), barriers and the TMEM address: 96 KB, two CTAs per SM (their
-// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns. (Four stages of 16-wide
-// chunks measured slower: the per-chunk issue and wait overhead outweighs the deeper prefetch.)
+// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns.
 constexpr int kSmemA = kInferRows * 256 * 2;
 constexpr int kSmemStage = 256 * kWChunkK * 2;
 constexpr int kInferSmem = kSmemA + kWStages * kSmemStage + 128;
+
+__device__ __forceinline__ void st_bf16(uint8_t* sA, int row, int col, int K, __nv_bfloat16 v) {
+  *reinterpret_cast<__nv_bfloat16*>(sA + canon_off(row, col, K)) = v;
+}
 
 __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs a) {
   extern __shared__ __align__(1024) uint8_t sm[];
@@ -182,14 +197,7 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   uint64_t* bar_done = bars + 2 * kWStages;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kWStages + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
-  __shared__ float s_bias[kInferMaxBias];
-  __shared__ double s_rho[kInferRows], s_T[kInferRows];
-  // biases, compact: layer l at s_bias[l * hidden] (hidden entries; out_pad for the last layer);
-  // b_off[l] is the offset of layer l's bias inside the parameter array
-  for (int l = 0; l < a.nlin; ++l) {
-    const int nl = l == a.nlin - 1 ? a.out_pad : a.hidden;
-    for (int i = tid; i < nl; i += kInferThreads) s_bias[l * a.hidden + i] = a.bias[a.b_off[l] + i];
-  }
+  __shared__ double s_part[2][kInferRows];  // the two halves of each cell's density
   if (tid == 0) {
     for (int i = 0; i < 2 * kWStages + 1; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -209,10 +217,10 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   int stage_busy[kWStages] = {}, inflight[kWStages] = {};
   int gc = 0, pre = 0, pre_base = 0;
   int err = 0;
-  // issue the bulk copy of weight chunk c of layer l into the next stage (thread 0)
-  auto issue = [&](int l, int c) {
+  // issue the bulk copy of weight chunk c of layer l of network ni into the next stage (thread 0)
+  auto issue = [&](int ni, int l, int c) {
     const int K = l == 0 ? a.in_pad : a.hidden;
-    const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
+    const int N = l == a.nlin - 1 ? a.net[ni].out_pad : a.hidden;
     const int s = gc % kWStages;
     ++gc;
     if (stage_busy[s]) {  // wait for the MMA that read this stage
@@ -223,156 +231,190 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
     const int kc = min(kWChunkK, K - c * kWChunkK);
     const uint32_t bytes = (uint32_t)N * kc * 2;
     mbar_expect_tx(&bar_full[s], bytes);
-    bulk_g2s(sW + s * kSmemStage, a.wpack + a.w_off[l] + (long long)c * N * kWChunkK, bytes, &bar_full[s]);
+    bulk_g2s(sW + s * kSmemStage, a.net[ni].wpack + a.net[ni].w_off[l] + (long long)c * N * kWChunkK, bytes,
+             &bar_full[s]);
     inflight[s] = 1;
+  };
+  // this thread's share of a cell's inputs, normalised, kept as BF16 for every network: species
+  // k0 + j (j < kn) as (log10 Y, Y) pairs; thread part 0 also holds T, log P and log10 dt
+  const int row = tid & (kInferRows - 1), part = tid >> 7;
+  const int half = (a.ns + 1) >> 1, k0 = part * half, kn = min(half, a.ns - k0);
+  __nv_bfloat162 fsp[kFeatSpecies];
+  __nv_bfloat162 fx0 = __floats2bfloat162_rn(0.f, 0.f), fx1 = fx0;
+  // column of species k's log feature (k != bath); its linear feature is ns columns further
+  auto log_col = [&](int k) { return 2 + (k < a.bath ? k : k - 1); };
+  // the packed inputs into A (layer 0's operand, K = in_pad), zero padding included
+  auto write_inputs = [&]() {
+    const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int j = 0; j < kFeatSpecies; ++j) {
+      const int k = k0 + j;
+      if (j < kn && k != a.bath) {
+        st_bf16(sA, row, log_col(k), a.in_pad, __low2bfloat16(fsp[j]));
+        st_bf16(sA, row, log_col(k) + a.ns, a.in_pad, __high2bfloat16(fsp[j]));
+      }
+    }
+    if (part == 0) {
+      st_bf16(sA, row, 0, a.in_pad, __low2bfloat16(fx0));
+      st_bf16(sA, row, 1, a.in_pad, __high2bfloat16(fx0));
+      st_bf16(sA, row, a.ns + 1, a.in_pad, __low2bfloat16(fx1));
+    } else {
+      for (int i = a.n_in; i < a.in_pad; ++i) st_bf16(sA, row, i, a.in_pad, z);
+    }
   };
   const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
   for (int tile = blockIdx.x; tile < ntiles && !err; tile += gridDim.x) {
-    // ---- 1. features of the tile's cells into A (K = in_pad): thread t serves row t % 128 and
-    // one half of the 8-wide input groups; density and temperature are formed once per row
+    // ---- 1. features of the tile's cells (once for all networks)
     {
-      const int row = tid & (kInferRows - 1), part = tid >> 7;
       const int cell = tile * kInferRows + row;
       const bool live = cell < a.ncells;
-      if (part == 0) {
-        double rho = 1.0, T = 0.0;
-        if (live) {
-          rho = 0.0;
-#pragma unroll 4
-          for (int k = 0; k < a.ns; ++k) rho += a.state[(long long)k * a.ld + cell];
-          T = a.state[(long long)a.ns * a.ld + cell] / rho;
-        }
-        s_rho[row] = rho;
-        s_T[row] = T;
-      }
-      __syncthreads();
-      const double irho = 1.0 / s_rho[row], T = s_T[row];
-      const double dt = live ? (a.dts ? a.dts[cell] : a.dt_scalar) : 0.0;
-      const int ng = a.in_pad / 8, g0 = part == 0 ? 0 : (ng + 1) / 2, g1 = part == 0 ? (ng + 1) / 2 : ng;
-      for (int g = g0; g < g1; ++g) {
-        const int k8 = 8 * g;
-        float f[8];
+      double x[kFeatSpecies];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int i = k8 + q;
-          f[q] = (live && i < a.n_in)
-                     ? (sur_raw_input(i, a.ns, a.bath, a.state, a.ld, cell, irho, T, a.logp, dt) - a.fmean[i]) * a.fistd[i]
-                     : 0.f;
+      for (int j = 0; j < kFeatSpecies; ++j) x[j] = (live && j < kn) ? a.state[(long long)(k0 + j) * a.ld + cell] : 0.0;
+      const double xT = (live && part == 0) ? a.state[(long long)a.ns * a.ld + cell] : 0.0;
+      const double dt = (live && part == 0) ? (a.dts ? a.dts[cell] : a.dt_scalar) : 1.0;
+      double ps = 0.0;
+#pragma unroll
+      for (int j = 0; j < kFeatSpecies; ++j) ps += x[j];
+      s_part[part][row] = ps;
+      __syncthreads();
+      const double rho = live ? s_part[0][row] + s_part[1][row] : 1.0;
+      const double irho = 1.0 / rho;
+#pragma unroll
+      for (int j = 0; j < kFeatSpecies; ++j) {
+        const int k = k0 + j;
+        float fl = 0.f, fn = 0.f;
+        if (live && j < kn && k != a.bath) {
+          const int i = log_col(k);
+          const double y = x[j] * irho;
+          // the logarithm in FP32: the feature is rounded to FP32 (and to BF16 for the network) anyway
+          fl = (log10f(fmaxf((float)y, 1e-30f)) - a.fmean[i]) * a.fistd[i];
+          fn = ((float)y - a.fmean[i + a.ns]) * a.fistd[i + a.ns];
         }
-        __nv_bfloat162 p0 = __floats2bfloat162_rn(f[0], f[1]);
-        __nv_bfloat162 p1 = __floats2bfloat162_rn(f[2], f[3]);
-        __nv_bfloat162 p2 = __floats2bfloat162_rn(f[4], f[5]);
-        __nv_bfloat162 p3 = __floats2bfloat162_rn(f[6], f[7]);
-        uint4 v;
-        v.x = *reinterpret_cast<uint32_t*>(&p0);
-        v.y = *reinterpret_cast<uint32_t*>(&p1);
-        v.z = *reinterpret_cast<uint32_t*>(&p2);
-        v.w = *reinterpret_cast<uint32_t*>(&p3);
-        *reinterpret_cast<uint4*>(sA + canon_off(row, k8, a.in_pad)) = v;
+        fsp[j] = __floats2bfloat162_rn(fl, fn);
+      }
+      if (part == 0) {
+        float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+        if (live) {
+          f0 = ((float)(xT / rho) - a.fmean[0]) * a.fistd[0];
+          f1 = ((float)a.logp - a.fmean[1]) * a.fistd[1];
+          f2 = ((float)log10(fmax(dt, 1e-30)) - a.fmean[a.ns + 1]) * a.fistd[a.ns + 1];
+        }
+        fx0 = __floats2bfloat162_rn(f0, f1);
+        fx1 = __floats2bfloat162_rn(f2, 0.f);
       }
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // ---- 2./3. layers
-    for (int l = 0; l < a.nlin && !err; ++l) {
-      const int K = l == 0 ? a.in_pad : a.hidden;
-      const int N = l == a.nlin - 1 ? a.out_pad : a.hidden;
-      const int nchunk = (K + kWChunkK - 1) / kWChunkK;
-      if (tid == 0) {
-        const uint32_t idesc = umma_idesc(kInferRows, N);
-        const uint32_t a_sbo = (uint32_t)K * 16;
-        // chunk c sits in stage (base + c) % S; after chunk c's MMA is queued the copies of the
-        // chunks up to c + S - 1 are issued, so they load while the tensor core works
-        const int base = pre ? pre_base : gc;
-        int issued = pre;
-        pre = 0;
-        if (issued == 0) issue(l, issued++);
-        for (int c = 0; c < nchunk && !err; ++c) {
-          const int s = (base + c) % kWStages;
-          const int kc = min(kWChunkK, K - c * kWChunkK);
-          if (!mbar_wait(&bar_full[s], ph_full[s], wlim)) err = 1;
-          ph_full[s] ^= 1;
-          inflight[s] = 0;
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t wbase = smem_u32(sW + s * kSmemStage);
-          const uint32_t abase = smem_u32(sA);
-          for (int kk = 0; kk < kc; kk += 16) {
-            const int kg = c * kWChunkK + kk;
-            const uint64_t ad = umma_desc(abase + (uint32_t)(kg >> 3) * 128, 128, a_sbo);
-            const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
-            umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
-          }
-          umma_commit(&bar_free[s]);
-          stage_busy[s] = 1;
-          while (issued < nchunk && issued < c + kWStages) issue(l, issued++);
-        }
-        if (!(a.fault == 1 && l == 0 && tile == (int)blockIdx.x)) umma_commit(bar_done);
-      }
-      // epilogue: one lane per warp polls the layer barrier, the warp follows
-      bool ok = true;
-      if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done, wlim);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      __syncwarp();
-      ph_done ^= 1;
-      if (!ok) err = 1;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      // after a timed-out wait the layer's MMAs may still read the A operand: no epilogue
-      if (__syncthreads_or(err)) {
-        err = 1;
-        break;
-      }
-      // the next layer's (or the next tile's first layer's) first chunks load during the epilogue
-      if (tid == 0 && !err) {
-        const bool more = l + 1 < a.nlin || tile + (int)gridDim.x < ntiles;
-        if (more) {
-          const int nl = l + 1 < a.nlin ? l + 1 : 0;
-          const int nk = ((nl == 0 ? a.in_pad : a.hidden) + kWChunkK - 1) / kWChunkK;
-          pre_base = gc;
-          pre = min(nk, kWStages - 1);
-          for (int c = 0; c < pre; ++c) issue(nl, c);
-        }
-      }
-      // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
-      const float* bl = s_bias + l * a.hidden;
-      const int row = (warp & 3) * 32 + (tid & 31);
-      const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-      const bool last = l == a.nlin - 1;
-      const int cell = tile * kInferRows + row;
-      for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 64) {
-        float v[32];
-        tmem_ld32(trow + (uint32_t)c0, v);
-        if (last) {
-          if (cell < a.ncells) {
-            float* o = a.out + (long long)cell * a.out_pad + c0;
-            const int nc = min(32, N - c0);
-            for (int i = 0; i < nc; ++i) o[i] = v[i] + bl[c0 + i];
-          }
-        } else {
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            float x[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) x[i] = gelu_fast(v[q * 8 + i] + bl[c0 + q * 8 + i]);
-            __nv_bfloat162 p0 = __floats2bfloat162_rn(x[0], x[1]);
-            __nv_bfloat162 p1 = __floats2bfloat162_rn(x[2], x[3]);
-            __nv_bfloat162 p2 = __floats2bfloat162_rn(x[4], x[5]);
-            __nv_bfloat162 p3 = __floats2bfloat162_rn(x[6], x[7]);
-            uint4 u;
-            u.x = *reinterpret_cast<uint32_t*>(&p0);
-            u.y = *reinterpret_cast<uint32_t*>(&p1);
-            u.z = *reinterpret_cast<uint32_t*>(&p2);
-            u.w = *reinterpret_cast<uint32_t*>(&p3);
-            *reinterpret_cast<uint4*>(sA + canon_off(row, c0 + q * 8, a.hidden)) = u;
-          }
-        }
-      }
+    // ---- 2./3. networks and their layers
+    for (int ni = 0; ni < a.nnets && !err; ++ni) {
+      const InferNet& net = a.net[ni];
+      write_inputs();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      err = __syncthreads_or(err);
+      for (int l = 0; l < a.nlin && !err; ++l) {
+        const int K = l == 0 ? a.in_pad : a.hidden;
+        const int N = l == a.nlin - 1 ? net.out_pad : a.hidden;
+        const int nchunk = (K + kWChunkK - 1) / kWChunkK;
+        if (tid == 0) {
+          const uint32_t idesc = umma_idesc(kInferRows, N);
+          const uint32_t a_sbo = (uint32_t)K * 16;
+          // chunk c sits in stage (base + c) % S; after chunk c's MMA is queued the copies of the
+          // chunks up to c + S - 1 are issued, so they load while the tensor core works
+          const int base = pre ? pre_base : gc;
+          int issued = pre;
+          pre = 0;
+          if (issued == 0) issue(ni, l, issued++);
+          for (int c = 0; c < nchunk && !err; ++c) {
+            const int s = (base + c) % kWStages;
+            const int kc = min(kWChunkK, K - c * kWChunkK);
+            if (!mbar_wait(&bar_full[s], ph_full[s], wlim)) err = 1;
+            ph_full[s] ^= 1;
+            inflight[s] = 0;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t wbase = smem_u32(sW + s * kSmemStage);
+            const uint32_t abase = smem_u32(sA);
+            for (int kk = 0; kk < kc; kk += 16) {
+              const int kg = c * kWChunkK + kk;
+              const uint64_t ad = umma_desc(abase + (uint32_t)(kg >> 3) * 128, 128, a_sbo);
+              const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
+              umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+            }
+            umma_commit(&bar_free[s]);
+            stage_busy[s] = 1;
+            while (issued < nchunk && issued < c + kWStages) issue(ni, l, issued++);
+          }
+          if (!(a.fault == 1 && ni == 0 && l == 0 && tile == (int)blockIdx.x)) umma_commit(bar_done);
+        }
+        // epilogue: one lane per warp polls the layer barrier, the warp follows
+        bool ok = true;
+        if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done, wlim);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        ph_done ^= 1;
+        if (!ok) err = 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // after a timed-out wait the layer's MMAs may still read the A operand: no epilogue
+        if (__syncthreads_or(err)) {
+          err = 1;
+          break;
+        }
+        // the next layer's (next network's, next tile's) first chunks load during the epilogue
+        if (tid == 0) {
+          int nn = ni, nl = l + 1;
+          if (nl == a.nlin) nl = 0, nn = ni + 1;
+          if (nn == a.nnets) nn = 0;
+          const bool more = l + 1 < a.nlin || ni + 1 < a.nnets || tile + (int)gridDim.x < ntiles;
+          if (more) {
+            const int nk = ((nl == 0 ? a.in_pad : a.hidden) + kWChunkK - 1) / kWChunkK;
+            pre_base = gc;
+            pre = min(nk, kWStages - 1);
+            for (int c = 0; c < pre; ++c) issue(nn, nl, c);
+          }
+        }
+        // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
+        const float* bl = net.bias + net.b_off[l];
+        const int erow = (warp & 3) * 32 + (tid & 31);
+        const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+        const bool last = l == a.nlin - 1;
+        const int cell = tile * kInferRows + erow;
+        for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 64) {
+          float v[32];
+          tmem_ld32(trow + (uint32_t)c0, v);
+          const int nc = min(32, N - c0);
+          if (last) {
+            if (cell < a.ncells) {
+              float* o = net.out + (long long)cell * net.out_pad + c0;
+              for (int i = 0; i < nc; ++i) o[i] = v[i] + __ldg(bl + c0 + i);
+            }
+          } else {
+            const float4* b4 = reinterpret_cast<const float4*>(bl + c0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float4 ba = __ldg(b4 + 2 * q), bb = __ldg(b4 + 2 * q + 1);
+              const float bq[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+              float xq[8];
+#pragma unroll
+              for (int i = 0; i < 8; ++i) xq[i] = gelu_fast(v[q * 8 + i] + bq[i]);
+              __nv_bfloat162 p0 = __floats2bfloat162_rn(xq[0], xq[1]);
+              __nv_bfloat162 p1 = __floats2bfloat162_rn(xq[2], xq[3]);
+              __nv_bfloat162 p2 = __floats2bfloat162_rn(xq[4], xq[5]);
+              __nv_bfloat162 p3 = __floats2bfloat162_rn(xq[6], xq[7]);
+              uint4 u;
+              u.x = *reinterpret_cast<uint32_t*>(&p0);
+              u.y = *reinterpret_cast<uint32_t*>(&p1);
+              u.z = *reinterpret_cast<uint32_t*>(&p2);
+              u.w = *reinterpret_cast<uint32_t*>(&p3);
+              *reinterpret_cast<uint4*>(sA + canon_off(erow, c0 + q * 8, a.hidden)) = u;
+            }
+          }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        err = __syncthreads_or(err);
+      }
     }
   }
   // drain: weight copies still in flight (after an error) and the last commits on the stage

@@ -50,6 +50,7 @@ struct SubstepKey {
 struct SolverState {
   bool tables_ready = false;
   SvDev dev{};
+  BdfCoef* d_coef = nullptr;  // BDF coefficients on the device (staged into shared memory by the kernel)
   int* d_int = nullptr;  // hot ints then cold ints
   double* d_dbl = nullptr;
   int rs = 0, smem_warp = 0;
@@ -70,6 +71,7 @@ void solver_release(tng_chem* h) {
     if (g) cudaGraphExecDestroy(g);
   if (s->d_int) cudaFree(s->d_int);
   if (s->d_dbl) cudaFree(s->d_dbl);
+  if (s->d_coef) cudaFree(s->d_coef);
   for (DevBuf* b : {&s->queue[0], &s->queue[1], &s->counters, &s->save, &s->resume, &s->nst, &s->nni, &s->nje,
                     &s->status, &s->stats})
     b->release();
@@ -85,7 +87,8 @@ static int ensure_tables(tng_chem* h) {
   if (s->tables_ready) return TNG_OK;
   {
     const BdfCoef coef = make_coef();
-    cudaError_t ce = cudaMemcpyToSymbol(c_bdf, &coef, sizeof(coef));
+    cudaError_t ce = cudaMalloc(&s->d_coef, sizeof(BdfCoef));
+    if (ce == cudaSuccess) ce = cudaMemcpy(s->d_coef, &coef, sizeof(coef), cudaMemcpyHostToDevice);
     if (ce != cudaSuccess) return cuda_error(ce, "BDF coefficients");
   }
   const MechOps* o = h->ops;
@@ -113,18 +116,17 @@ static int ensure_tables(tng_chem* h) {
   return TNG_OK;
 }
 
-typedef void (*BdfKernel)(const BdfLaunch);
-
 // occ 2 (with 8 warps): launch bounds for two blocks per SM (registers capped at 128)
-static BdfKernel bdf_kernel(int warps, int occ = 1) {
-  if (warps == 8 && occ == 2) return k_bdf<8, 2>;
+static BdfKernelFn bdf_kernel(const tng_chem* h, int warps, int occ = 1) {
+  const SolverKernels* k = h->ops->sk;
+  if (warps == 8 && occ == 2) return k->bdf8_occ2;
   switch (warps) {
     case 2:
-      return k_bdf<2>;
+      return k->bdf2;
     case 8:
-      return k_bdf<8>;
+      return k->bdf8;
     default:
-      return k_bdf<4>;
+      return k->bdf4;
   }
 }
 
@@ -143,7 +145,7 @@ static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device);
   s->cold_in_smem = block_smem(s, warps, 1) * occ <= (size_t)optin * 7 / 8 ? 1 : 0;
   const size_t smem = block_smem(s, warps, s->cold_in_smem);
-  BdfKernel k = bdf_kernel(warps, occ);
+  BdfKernelFn k = bdf_kernel(h, warps, occ);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   int per_sm = 0;
@@ -293,6 +295,7 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
     }
     BdfLaunch L;
     std::memset(&L, 0, sizeof(L));
+    L.coef = s->d_coef;
     BdfArgs& a = L.a;
     a.tab = s->dev;
     a.state = dstate;
@@ -339,7 +342,7 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
       a.n_in = (int)ncells;
       L.n_in_dev = pass == 0 ? nlist : cnt + 2 + (cur ^ 1);
       a.budget = pass == passes - 1 ? 0x7fffffff : budget;
-      bdf_kernel(warps, occ)<<<s->blocks, warps * 32, smem, st>>>(L);
+      bdf_kernel(h, warps, occ)<<<s->blocks, warps * 32, smem, st>>>(L);
       note(cudaGetLastError(), "solver kernel");
     }
     cudaGraph_t graph;
@@ -406,11 +409,11 @@ extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncel
   if (rc) return rc;
   SolverState* s = h->solver;
   const size_t smem = block_smem(s, 4, 0);
-  cudaError_t e = cudaFuncSetAttribute(k_warp_rhs_jac<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const RhsJacFn kern = h->ops->sk->rhs_jac4;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   const int blocks = (int)std::min<int64_t>((ncells + 3) / 4, 148 * 8);
-  k_warp_rhs_jac<4><<<blocks, 128, smem, h->stream>>>(s->dev, state, ld, (int)ncells, p, rhs, jac, s->rs,
-                                                     s->smem_warp);
+  kern<<<blocks, 128, smem, h->stream>>>(s->dev, state, ld, (int)ncells, p, rhs, jac, s->smem_warp);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "tng_solver_rhs_jac");
   return TNG_OK;
 }

@@ -33,45 +33,64 @@ namespace tng {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kQmax = 5;
 
-// Table view inside a kernel: hot tables in shared memory (staged per block), cold tables and
-// the layout in global/parameter space.
+// The solver tables of a handle as the host passes them: device pointers, the layout, precision.
 struct SvDev {
-  const double* __restrict__ hd;  // hot doubles (shared memory once staged)
-  const int* __restrict__ hi;     // hot ints (shared memory once staged)
-  const int* __restrict__ ci;     // cold ints (global, read through L1)
+  const double* __restrict__ hd;  // hot doubles
+  const int* __restrict__ hi;     // hot ints
+  const int* __restrict__ ci;     // cold ints
   SvLayout L;
   int mixed;  // rate-constant exponentials on the FP32 special-function unit (see rexp)
-  __device__ __forceinline__ const double* d(int k) const { return hd + L.hd[k]; }
-  __device__ __forceinline__ const int* i(int k) const { return hi + L.hi[k]; }
-  __device__ __forceinline__ const int* c(int k) const { return ci + L.ci[k]; }
 };
 
-// Copy the hot tables from global memory into the block's shared memory (all threads).
-__device__ __forceinline__ SvDev stage_tables(const SvDev& g, void* smem) {
-  double* d = reinterpret_cast<double*>(smem);
-  int* i = reinterpret_cast<int*>(d + g.L.nhd);
-  const double2* gs = reinterpret_cast<const double2*>(g.hd);
-  double2* ds = reinterpret_cast<double2*>(d);
-  for (int e = threadIdx.x; e < g.L.nhd / 2; e += blockDim.x) ds[e] = gs[e];
-  const int4* gi = reinterpret_cast<const int4*>(g.hi);
-  int4* di = reinterpret_cast<int4*>(i);
-  for (int e = threadIdx.x; e < g.L.nhi / 4; e += blockDim.x) di[e] = gi[e];
-  __syncthreads();
-  SvDev t = g;
-  t.hd = d;
-  t.hi = i;
-  return t;
-}
+// Table view inside a kernel, specialised on the mechanism's layout LY (generated SvL_<m>: the
+// sizes and table offsets are compile-time constants, so a table access is one shared-memory
+// load at a fixed offset and every loop bound is known): hot tables in shared memory (staged per
+// block), cold tables in shared memory when they fit, else global (read through L1).
+template <class LY>
+struct SvT {
+  static constexpr int NS = LY::size(SZ_NS), NV = LY::size(SZ_NV), NSLOT = LY::size(SZ_NSLOT);
+  static constexpr int NM = LY::size(SZ_NM), NFC = LY::size(SZ_NFC), NCD = LY::size(SZ_NCDCHUNK);
+  static constexpr int NGP = LY::size(SZ_NGPAIR);
+  static constexpr int RS = (NV % 2 == 0) ? NV + 1 : NV;  // matrix row stride (odd: fewer bank conflicts)
+  const double* __restrict__ hd;
+  const int* __restrict__ hi;
+  const int* __restrict__ ci;
+  int mixed;
+  __device__ __forceinline__ const double* d(int k) const { return hd + LY::hd(k); }
+  __device__ __forceinline__ const int* i(int k) const { return hi + LY::hi(k); }
+  __device__ __forceinline__ const int* c(int k) const { return ci + LY::ci(k); }
+};
 
 __host__ __device__ inline int hot_smem_bytes(const SvLayout& L) { return L.nhd * 8 + L.nhi * 4; }
 __host__ __device__ inline int cold_smem_doubles(const SvLayout& L) { return (L.nci * 4 + 15) / 16 * 2; }
 
+// Copy the hot tables from global memory into the block's shared memory (all threads).
+template <class LY>
+__device__ __forceinline__ SvT<LY> stage_tables(const SvDev& g, void* smem) {
+  double* d = reinterpret_cast<double*>(smem);
+  int* i = reinterpret_cast<int*>(d + LY::nhd);
+  const double2* gs = reinterpret_cast<const double2*>(g.hd);
+  double2* ds = reinterpret_cast<double2*>(d);
+  for (int e = threadIdx.x; e < LY::nhd / 2; e += blockDim.x) ds[e] = gs[e];
+  const int4* gi = reinterpret_cast<const int4*>(g.hi);
+  int4* di = reinterpret_cast<int4*>(i);
+  for (int e = threadIdx.x; e < LY::nhi / 4; e += blockDim.x) di[e] = gi[e];
+  __syncthreads();
+  SvT<LY> t;
+  t.hd = d;
+  t.hi = i;
+  t.ci = g.ci;
+  t.mixed = g.mixed;
+  return t;
+}
+
 // Copy the cold tables (the Jacobian's term lists) into shared memory at `at` (all threads),
 // when the block has room for them; otherwise they are read from global memory through L1,
 // which the shared-memory carve-out leaves small.
-__device__ __forceinline__ SvDev stage_cold_tables(SvDev t, double* at) {
+template <class LY>
+__device__ __forceinline__ SvT<LY> stage_cold_tables(SvT<LY> t, double* at) {
   int* d = reinterpret_cast<int*>(at);
-  for (int e = threadIdx.x; e < t.L.nci; e += blockDim.x) d[e] = t.ci[e];
+  for (int e = threadIdx.x; e < LY::nci; e += blockDim.x) d[e] = t.ci[e];
   __syncthreads();
   t.ci = d;
   return t;
@@ -129,18 +148,19 @@ __host__ __device__ inline int warp_mem_doubles(const SvLayout& L, int rs) {
          L.size[SZ_NGPAIR] + 3 * 64 + 64 /* pivots and permutation as ints */ + 8;
 }
 
-__device__ __forceinline__ WarpMem warp_mem(double* base, const SvLayout& L, int rs) {
+template <class LY>
+__device__ __forceinline__ WarpMem warp_mem(double* base) {
+  using T = SvT<LY>;
   WarpMem w;
-  const int nv = L.size[SZ_NV];
   double* p = base;
-  w.mat = p; p += nv * rs;
-  w.W = p; p += L.size[SZ_NSLOT];
+  w.mat = p; p += T::NV * T::RS;
+  w.W = p; p += T::NSLOT;
   w.C = p; p += 64;
-  w.Ms = p; p += L.size[SZ_NM];
-  w.lcm = p; p += L.size[SZ_NM];
-  w.fc = p; p += 3 * L.size[SZ_NFC];
-  w.part = p; p += L.size[SZ_NCDCHUNK];
-  w.G = p; p += L.size[SZ_NGPAIR];
+  w.Ms = p; p += T::NM;
+  w.lcm = p; p += T::NM;
+  w.fc = p; p += 3 * T::NFC;
+  w.part = p; p += T::NCD;
+  w.G = p; p += T::NGP;
   w.vb = p; p += 64;
   w.hb = p; p += 64;
   w.cb = p; p += 64;
@@ -169,7 +189,8 @@ __device__ __forceinline__ int nu_of(const int term) { return (int)(int8_t)(term
 // split into an exact power of two (FP64 scaling) and a fraction in [0, 1) evaluated by the FP32
 // ex2 unit, relative error about 3e-7. The exponent itself (ln A + n ln T - E/RT, where the
 // reverse rates' cancellations sit) is always formed in FP64.
-__device__ __forceinline__ double rexp(const SvDev& t, const double e) {
+template <class LY>
+__device__ __forceinline__ double rexp(const SvT<LY>& t, const double e) {
   if (!t.mixed) return exp(e);
   const double x = e * 1.4426950408889634;
   const double n = floor(x);
@@ -184,9 +205,10 @@ struct CellPrep {
 
 // Stage the state (two entries per lane) and fill C, third-body sums, falloff [M] logs and the
 // F_cent terms in shared memory.
-__device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+template <class LY>
+__device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
                                            const double p, const int lane) {
-  const int ns = t.L.size[SZ_NS], nv = ns + 1, nm = t.L.size[SZ_NM], nfc = t.L.size[SZ_NFC];
+  constexpr int ns = SvT<LY>::NS, nv = ns + 1, nm = SvT<LY>::NM, nfc = SvT<LY>::NFC;
   const double* sc = t.d(HD_SCAL);
   const double* invw = t.d(HD_INVW);
   if (lane < nv) w.vb[lane] = y0;
@@ -236,7 +258,8 @@ __device__ __forceinline__ CellPrep prepare(const SvDev& t, const WarpMem& w, co
 
 // Rate constant of the slot at position p (GETLINDRATECOEFF-equivalent for falloff slots);
 // also returns ln Pr for falloff slots.
-__device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, const CellPrep& c, const int p,
+template <class LY>
+__device__ __forceinline__ double rate_const(const SvT<LY>& t, const WarpMem& w, const CellPrep& c, const int p,
                                             const int w0, const int w1, double* lpr_out) {
   const int fl = w0 & 15;
   if (fl & 1) {
@@ -261,9 +284,10 @@ __device__ __forceinline__ double rate_const(const SvDev& t, const WarpMem& w, c
 }
 
 // finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
-__device__ __forceinline__ void rhs_warp(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+template <class LY>
+__device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
                                          const double p, double& f0, double& f1, const int lane) {
-  const int ns = t.L.size[SZ_NS], nslot = t.L.size[SZ_NSLOT];
+  constexpr int ns = SvT<LY>::NS, nslot = SvT<LY>::NSLOT;
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
   for (int q = lane; q < nslot; q += 32) {
@@ -330,8 +354,12 @@ __device__ __forceinline__ void rhs_warp(const SvDev& t, const WarpMem& w, const
 // One out-of-line copy of the right-hand side. The solver evaluates it from several places;
 // inlined at each of them, the kernel's code outgrows the instruction cache and the warps stall
 // on instruction fetch.
-static __device__ __noinline__ double2 rhs_call(const SvDev& t, const WarpMem& w, const double y0, const double y1,
+// (The workspace is passed as its base pointer and its regions are recomputed from the
+// compile-time layout, so that no descriptor goes through the stack.)
+template <class LY>
+static __device__ __noinline__ double2 rhs_call(const SvT<LY> t, double* wb, const double y0, const double y1,
                                                 const double p, const int lane) {
+  const WarpMem w = warp_mem<LY>(wb);
   double f0, f1;
   rhs_warp(t, w, y0, y1, p, f0, f1, lane);
   return make_double2(f0, f1);
@@ -339,10 +367,10 @@ static __device__ __noinline__ double2 rhs_call(const SvDev& t, const WarpMem& w
 
 // Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
 // row stride rs). Uses one extra right-hand side for the temperature column.
-__device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const int rs, const double y0,
-                                         const double y1, const double f0, const double f1, const double p,
-                                         const int lane) {
-  const int ns = t.L.size[SZ_NS], nv = ns + 1, nslot = t.L.size[SZ_NSLOT];
+template <class LY>
+__device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
+                                         const double f0, const double f1, const double p, const int lane) {
+  constexpr int ns = SvT<LY>::NS, nv = ns + 1, nslot = SvT<LY>::NSLOT, rs = SvT<LY>::RS;
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
   for (int q = lane; q < nslot; q += 32) w.W[q] = rate_const(t, w, c, q, sw[2 * q], sw[2 * q + 1], nullptr);
@@ -418,7 +446,7 @@ __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const
   }
   __syncwarp();
   {
-    const int ng = t.L.size[SZ_NGPAIR];
+    constexpr int ng = SvT<LY>::NGP;
     const int* gi = t.c(CI_G_I);
     const int* gm = t.c(CI_G_M);
     const double* eff = t.d(HD_EFF);
@@ -435,7 +463,7 @@ __device__ __forceinline__ void jac_warp(const SvDev& t, const WarpMem& w, const
   const double dlt = 1.4901161193847656e-08 * fmax(fabs(yN), 1e-30);
   const double yNp = yN + dlt;
   const double idl = 1.0 / (yNp - yN);
-  const double2 gg = rhs_call(t, w, lane == ns ? yNp : y0, lane + 32 == ns ? yNp : y1, p, lane);
+  const double2 gg = rhs_call(t, w.mat, lane == ns ? yNp : y0, lane + 32 == ns ? yNp : y1, p, lane);
   const double g0 = gg.x, g1 = gg.y;
   if (lane < nv) w.mat[lane * rs + ns] = (g0 - f0) * idl;
   if (lane + 32 < nv) w.mat[(lane + 32) * rs + ns] = (g1 - f1) * idl;
@@ -554,16 +582,18 @@ __device__ __forceinline__ void lu_finish(const double* a, const int n, const in
 }
 
 // Out-of-line Jacobian and factorisation (one copy each, as rhs_call).
-static __device__ __noinline__ void jac_call(const SvDev& t, const WarpMem& w, const int rs, const double y0,
-                                             const double y1, const double f0, const double f1, const double p,
-                                             const int lane) {
-  jac_warp(t, w, rs, y0, y1, f0, f1, p, lane);
+template <class LY>
+static __device__ __noinline__ void jac_call(const SvT<LY> t, double* wb, const double y0, const double y1,
+                                             const double f0, const double f1, const double p, const int lane) {
+  jac_warp<LY>(t, warp_mem<LY>(wb), y0, y1, f0, f1, p, lane);
 }
 
-static __device__ __noinline__ int lu_call(double* a, const int n, const int rs, int* piv, int* perm, double* dinv,
-                                           const int lane) {
-  const int sing = lu_warp(a, n, rs, piv, lane);
-  lu_finish(a, n, rs, piv, perm, dinv, lane);
+template <class LY>
+static __device__ __noinline__ int lu_call(double* wb, const int lane) {
+  using T = SvT<LY>;
+  const WarpMem w = warp_mem<LY>(wb);
+  const int sing = lu_warp(w.mat, T::NV, T::RS, w.piv, lane);
+  lu_finish(w.mat, T::NV, T::RS, w.piv, w.perm, w.cb, lane);
   return sing;
 }
 

@@ -11,8 +11,8 @@
 // Limits and contract:
 //   * at most kStaticMaxCells cells per call (TNG_ERR_ARG beyond that);
 //   * the first call on a device does the set-up: the symbol address, the BDF coefficients
-//     into this file's constant bank, and the solver tables of EVERY built-in mechanism (both
-//     literal modes) into their own fixed regions of the array. Those copies are synchronous,
+//     and the solver tables of EVERY built-in mechanism (both literal modes) into their own
+//     fixed regions of the array. Those copies are synchronous,
 //     so that first call should come before any stream capture the caller does. A later call
 //     only selects its mechanism's region: it copies no tables, so calls of different
 //     mechanisms can follow each other in any order (and a captured call stays valid);
@@ -35,8 +35,6 @@
 #include "tng_runtime.h"
 
 namespace tng {
-
-BdfCoef make_coef();  // solver.cu
 
 namespace {
 
@@ -64,9 +62,9 @@ struct StaticTab {
 struct StaticDev {
   bool ready = false;
   unsigned char* base = nullptr;
+  size_t coef = 0;  // the BDF coefficients (byte offset)
   StaticTab tab[kStaticMaxMechs];
   int ntab = 0;
-  size_t smem_set[9] = {};  // dynamic shared memory attribute per warp count
 };
 StaticDev g_dev[kStaticMaxDevices];
 std::mutex g_setup_mutex;
@@ -86,10 +84,8 @@ int static_setup(int device, StaticDev** out) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: scratch symbol address");
-    const BdfCoef coef = make_coef();
-    e = cudaMemcpyToSymbol(c_bdf, &coef, sizeof(coef));
-    if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: BDF coefficients");
-    // every built-in mechanism's tables into its own region, packed in registry order
+    // the BDF coefficients, then every built-in mechanism's tables into its own region, packed
+    // in registry order
     unsigned char* base = (unsigned char*)p;
     size_t off = kOffTab;
     int nt = 0;
@@ -102,6 +98,8 @@ int static_setup(int device, StaticDev** out) {
       off += (bytes + 255) & ~(size_t)255;
       return TNG_OK;
     };
+    const BdfCoef coef = make_coef();
+    if (int rc = place(&coef, sizeof(coef), &d.coef)) return rc;
     for (const MechOps* const* m = all_mechanisms(); *m; ++m) {
       if (nt == kStaticMaxMechs) return set_error(TNG_ERR_ARG, "tng_substep_batch_static: too many mechanisms");
       const MechOps* o = *m;
@@ -169,6 +167,7 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   const int warps = (h->cfg.solver_warps == 2 || h->cfg.solver_warps == 4) ? h->cfg.solver_warps : 8;
   BdfLaunch Lh;
   std::memset(&Lh, 0, sizeof(Lh));
+  Lh.coef = (const BdfCoef*)(d->base + d->coef);
   BdfArgs& a = Lh.a;
   a.tab.hd = tab_d;
   a.tab.hi = tab_i;
@@ -179,13 +178,10 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   a.rs = (nv % 2 == 0) ? nv + 1 : nv;
   a.smem_warp = (warp_mem_doubles(L, a.rs) + 3) & ~3;
   const size_t smem = ((size_t)hot_smem_doubles(L) + (size_t)warps * a.smem_warp) * sizeof(double);
-  // this file's own instantiations (TAG 1): they read this file's constant bank
-  void (*kern)(const BdfLaunch) = warps == 2 ? k_bdf<2, 1, 1> : warps == 4 ? k_bdf<4, 1, 1> : k_bdf<8, 1, 1>;
-  if (d->smem_set[warps] < smem) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: shared memory");
-    d->smem_set[warps] = smem;
-  }
+  const SolverKernels* sk = o->sk;
+  const BdfKernelFn kern = warps == 2 ? sk->bdf2 : warps == 4 ? sk->bdf4 : sk->bdf8;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: shared memory");
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
   if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: occupancy");

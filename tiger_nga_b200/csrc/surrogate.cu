@@ -613,27 +613,15 @@ static int sur_pack(tng_surrogate* s) {
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate weight packing");
 }
 
-static int launch_net(tng_chem* h, tng_surrogate* s, const Mlp& net, const __nv_bfloat16* wpack,
-                      const long long* w_off, const double* dstate, int64_t ncells, int64_t dld, const double* ddts,
-                      double dt, double p, float* out, int* err);
-
-static int launch_infer(tng_chem* h, tng_surrogate* s, int member, const double* dstate, int64_t ncells, int64_t dld,
-                        const double* ddts, double dt, double p, float* out, int* err) {
-  return launch_net(h, s, s->member(member), s->d_wpack[member], s->w_off, dstate, ncells, dld, ddts, dt, p, out, err);
-}
-
-// the gate's outputs for every cell into s->gout (no-op without a gate)
-static int launch_gate(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
-                       const double* ddts, double dt, double p, int* err) {
-  if (!s->has_gate) return TNG_OK;
-  if (!s->gout.reserve((size_t)ncells * s->gate.out_pad * sizeof(float)))
+// One launch of the tensor-core inference over nmembers ensemble members starting at
+// first_member (outputs at out + i * ncells * out_pad) and, with gate, the error gate (outputs in
+// s->gout): the cells' features are formed once for all of them.
+static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
+                        const double* ddts, double dt, double p, int first_member, int nmembers, float* out, bool gate,
+                        int* err) {
+  gate = gate && s->has_gate;
+  if (gate && !s->gout.reserve((size_t)ncells * s->gate.out_pad * sizeof(float)))
     return set_error(TNG_ERR_CUDA, "surrogate gate output allocation failed");
-  return launch_net(h, s, s->gate, s->d_gpack, s->g_off, dstate, ncells, dld, ddts, dt, p, (float*)s->gout.ptr, err);
-}
-
-static int launch_net(tng_chem* h, tng_surrogate* s, const Mlp& net, const __nv_bfloat16* wpack,
-                      const long long* w_off, const double* dstate, int64_t ncells, int64_t dld, const double* ddts,
-                      double dt, double p, float* out, int* err) {
   InferArgs ia{};
   ia.state = dstate;
   ia.ld = dld;
@@ -644,24 +632,30 @@ static int launch_net(tng_chem* h, tng_surrogate* s, const Mlp& net, const __nv_
   ia.ns = s->ns;
   ia.bath = s->bath;
   ia.n_in = s->n_in;
-  ia.in_pad = net.in_pad;
-  ia.hidden = net.hidden;
-  ia.out_pad = net.out_pad;
-  ia.nlin = net.nlin;
+  ia.in_pad = s->m.in_pad;
+  ia.hidden = s->m.hidden;
+  ia.nlin = s->m.nlin;
   ia.fmean = s->d_fnorm;
   ia.fistd = s->d_fnorm + s->m.in_pad;
-  ia.wpack = wpack;
-  for (int l = 0; l < net.nlin; ++l) {
-    ia.w_off[l] = w_off[l];
-    ia.b_off[l] = (int)net.b_off[l];
-  }
-  ia.bias = net.params;
-  ia.out = out;
+  auto add = [&](const Mlp& net, const __nv_bfloat16* wpack, const long long* w_off, float* o) {
+    InferNet& n = ia.net[ia.nnets++];
+    n.wpack = wpack;
+    for (int l = 0; l < net.nlin; ++l) {
+      n.w_off[l] = w_off[l];
+      n.b_off[l] = (int)net.b_off[l];
+    }
+    n.bias = net.params;
+    n.out_pad = net.out_pad;
+    n.out = o;
+  };
+  if (nmembers + (gate ? 1 : 0) < 1 || nmembers + (gate ? 1 : 0) > kMaxNets)
+    return set_error(TNG_ERR_ARG, "inference: 1..%d networks per launch", kMaxNets);
+  for (int i = 0; i < nmembers; ++i)
+    add(s->member(first_member + i), s->d_wpack[first_member + i], s->w_off, out + (size_t)i * ncells * s->m.out_pad);
+  if (gate) add(s->gate, s->d_gpack, s->g_off, (float*)s->gout.ptr);
   ia.error = err;
   ia.wait_limit = s->dbg_wait_limit;
   ia.fault = s->dbg_fault;
-  if ((net.nlin - 1) * net.hidden + net.out_pad > kInferMaxBias)
-    return set_error(TNG_ERR_ARG, "inference: the biases do not fit the kernel's shared-memory stage");
   cudaError_t e = cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
   if (e != cudaSuccess) return cuda_error(e, "inference shared memory");
   const int grid = (int)std::min<int64_t>(2 * h->sm_count, (ncells + kInferRows - 1) / kInferRows);
@@ -1261,7 +1255,7 @@ int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_
   if (!s->cnt.reserve(16 * sizeof(unsigned long long))) return set_error(TNG_ERR_CUDA, "scratch");
   int* err = (int*)((unsigned long long*)s->cnt.ptr + 8);
   cudaMemsetAsync(err, 0, sizeof(int), s->m.stream);
-  int rc = launch_infer(s->h, s, 0, state, n, ld, dts, dt, p, out, err);
+  int rc = launch_infer(s->h, s, state, n, ld, dts, dt, p, 0, 1, out, false, err);
   if (rc) return rc;
   int herr = 0;
   cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s->m.stream);
@@ -1348,10 +1342,7 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   s->calls++;
   // inference on the tensor cores
   cudaEventRecord(s->ev[0], st);
-  for (int i = 0; i < s->members && !rc; ++i)
-    rc = launch_infer(h, s, i, dstate, ncells, dld, ddts, dt, p,
-                      (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad, (int*)(cnt + 8));
-  if (!rc) rc = launch_gate(h, s, dstate, ncells, dld, ddts, dt, p, (int*)(cnt + 8));
+  rc = launch_infer(h, s, dstate, ncells, dld, ddts, dt, p, 0, s->members, (float*)s->out.ptr, true, (int*)(cnt + 8));
   if (rc) return rc;
   cudaEventRecord(s->ev[1], st);
   // post-processing and fallback list
@@ -1435,10 +1426,7 @@ int tng_surrogate_predict(tng_chem* h, tng_surrogate* s, const double* state, in
   if (rc) return rc;
   unsigned long long* cnt = (unsigned long long*)s->cnt.ptr;
   cudaMemsetAsync(cnt, 0, 16 * sizeof(unsigned long long), st);
-  for (int i = 0; i < s->members && !rc; ++i)
-    rc = launch_infer(h, s, i, state, ncells, ld, dts, dt, p, (float*)s->out.ptr + (size_t)i * ncells * s->m.out_pad,
-                      (int*)(cnt + 8));
-  if (!rc) rc = launch_gate(h, s, state, ncells, ld, dts, dt, p, (int*)(cnt + 8));
+  rc = launch_infer(h, s, state, ncells, ld, dts, dt, p, 0, s->members, (float*)s->out.ptr, true, (int*)(cnt + 8));
   if (rc) return rc;
   SurPost pa = post_args(h, s, const_cast<double*>(state), ld, ncells, dts, dt, p);
   pa.out_state = out;
