@@ -592,7 +592,7 @@ def main():
     ap.add_argument("--impl", default="tiger", choices=["tiger", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--e2e-steps", type=int, default=0, help="e2e steps (0: the timed steps of `value`)")
-    ap.add_argument("--plain-cells", type=int, default=262144,
+    ap.add_argument("--plain-cells", type=int, default=0,
                     help="gri-surrogate: cells of the strided subsample solved by the plain GPU path (0 = all)")
     ap.add_argument("--side", type=int, default=0, help="cube side override (small profiling cases)")
     ap.add_argument("--surrogate", default="", help="weights file (default: the workload's trained model)")

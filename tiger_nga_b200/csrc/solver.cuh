@@ -50,7 +50,7 @@ template <class LY>
 struct SvT {
   static constexpr int NS = LY::size(SZ_NS), NV = LY::size(SZ_NV), NSLOT = LY::size(SZ_NSLOT);
   static constexpr int NM = LY::size(SZ_NM), NFC = LY::size(SZ_NFC), NCD = LY::size(SZ_NCDCHUNK);
-  static constexpr int NGP = LY::size(SZ_NGPAIR);
+  static constexpr int NGP = LY::size(SZ_NGPAIR), NFO = LY::size(SZ_NFO);
   static constexpr int RS = (NV % 2 == 0) ? NV + 1 : NV;  // matrix row stride (odd: fewer bank conflicts)
   const double* __restrict__ hd;
   const int* __restrict__ hi;
@@ -283,6 +283,18 @@ __device__ __forceinline__ double rate_const(const SvT<LY>& t, const WarpMem& w,
   return rexp(t, expo(sd[0], sd[1], sd[2], fl, c.LT, c.invRT));
 }
 
+// Rate constant of a plain (Arrhenius or constant) slot without branches: the table holds
+// (ln A, E, n) with zeros for absent terms, so the FMA chain of expo() gives the same exponent;
+// constant slots hold A itself and take it.
+template <class LY>
+__device__ __forceinline__ double plain_const(const SvT<LY>& t, const CellPrep& c, const int p, const int w0) {
+  const double* sd = t.d(HD_SLOT) + 4 * p;
+  const double a = sd[0];
+  const double e = fma(sd[2], c.LT, fma(sd[1], c.invRT, a));
+  const double v = rexp(t, e);
+  return (w0 & 8) ? a : v;
+}
+
 // finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
 template <class LY>
 __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
@@ -290,15 +302,24 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
   constexpr int ns = SvT<LY>::NS, nslot = SvT<LY>::NSLOT;
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
-  for (int q = lane; q < nslot; q += 32) {
-    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
-    double v = rate_const(t, w, c, q, w0, w1, nullptr);
+  auto mass_action = [&](double v, const int w0, const int w1) {
     const int r0 = (w0 >> 4) & 127, r1 = (w0 >> 11) & 127, r2 = (w0 >> 18) & 127, mw = w1 & 127;
     if (r0 != kNone7) v = v * w.C[r0];
     if (r1 != kNone7) v = v * w.C[r1];
     if (r2 != kNone7) v = v * w.C[r2];
     if (mw != kNone7) v = v * w.Ms[mw];
-    w.W[q] = v;
+    return v;
+  };
+  // the falloff slots (processing positions 0 .. NFO-1), then the plain and constant slots in a
+  // loop without divergent paths, whose independent exponentials the compiler interleaves
+  for (int q = lane; q < SvT<LY>::NFO; q += 32) {
+    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
+    w.W[q] = mass_action(rate_const(t, w, c, q, w0, w1, nullptr), w0, w1);
+  }
+#pragma unroll 2
+  for (int q = SvT<LY>::NFO + lane; q < nslot; q += 32) {
+    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
+    w.W[q] = mass_action(plain_const(t, c, q, w0), w0, w1);
   }
   __syncwarp();
   {
@@ -307,16 +328,23 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
     const int* cb = t.i(HI_CD_BEG);
     const int* ce = t.i(HI_CD_END);
     const int* ct = t.i(HI_CD_TERM);
+    auto add = [&](double acc, const int term) {
+      const int nu = nu_of(term);
+      const double wv = w.W[term >> 8];
+      return nu == 1 ? acc + wv : (nu == -1 ? acc - wv : fma((double)nu, wv, acc));
+    };
     for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
       const int ch = ll[i];
-      double acc = 0.0;
-      for (int q = cb[ch]; q < ce[ch]; ++q) {
-        const int term = ct[q];
-        const int nu = nu_of(term);
-        const double wv = w.W[term >> 8];
-        acc = nu == 1 ? acc + wv : (nu == -1 ? acc - wv : fma((double)nu, wv, acc));
+      const int qe = ce[ch];
+      double a0 = 0.0, a1 = 0.0;  // two partial sums: independent chains
+      int q = cb[ch];
+      for (; q + 1 < qe; q += 2) {
+        const int t0 = ct[q], t1 = ct[q + 1];
+        a0 = add(a0, t0);
+        a1 = add(a1, t1);
       }
-      w.part[ch] = acc;
+      if (q < qe) a0 = add(a0, ct[q]);
+      w.part[ch] = a0 + a1;
     }
   }
   __syncwarp();
@@ -373,7 +401,9 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   constexpr int ns = SvT<LY>::NS, nv = ns + 1, nslot = SvT<LY>::NSLOT, rs = SvT<LY>::RS;
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
-  for (int q = lane; q < nslot; q += 32) w.W[q] = rate_const(t, w, c, q, sw[2 * q], sw[2 * q + 1], nullptr);
+  for (int q = lane; q < SvT<LY>::NFO; q += 32) w.W[q] = rate_const(t, w, c, q, sw[2 * q], sw[2 * q + 1], nullptr);
+#pragma unroll 2
+  for (int q = SvT<LY>::NFO + lane; q < nslot; q += 32) w.W[q] = plain_const(t, c, q, sw[2 * q]);
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
   // direct mass-action part: dW_p/dC_j for every reactant occurrence
@@ -384,25 +414,33 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
     const int* gb = t.c(CI_JD_BEG);
     const int* ge = t.c(CI_JD_END);
     const int* jt = t.c(CI_JD_TERM);
+    // nu * dW_p/dC_j of one term (the product of the slot's other reactant concentrations)
+    auto dterm = [&](const int term) {
+      const int pp = term >> 12, rp = (term >> 8) & 15;
+      const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
+      double d = w.W[pp];
+      const int mw = w1 & 127;
+      if (mw != kNone7) d *= w.Ms[mw];
+#pragma unroll
+      for (int o = 0; o < 3; ++o) {
+        const int r = (w0 >> (4 + 7 * o)) & 127;
+        if (o != rp && r != kNone7) d *= w.C[r];
+      }
+      return (double)nu_of(term) * d;
+    };
     for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
       const int g = ll[i];
-      double acc = 0.0;
-      for (int q = gb[g]; q < ge[g]; ++q) {
-        const int term = jt[q];
-        const int pp = term >> 12, rp = (term >> 8) & 15;
-        const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
-        double d = w.W[pp];
-        const int mw = w1 & 127;
-        if (mw != kNone7) d *= w.Ms[mw];
-#pragma unroll
-        for (int o = 0; o < 3; ++o) {
-          const int r = (w0 >> (4 + 7 * o)) & 127;
-          if (o != rp && r != kNone7) d *= w.C[r];
-        }
-        acc = fma((double)nu_of(term), d, acc);
+      const int qe = ge[g];
+      double a0 = 0.0, a1 = 0.0;  // two independent chains
+      int q = gb[g];
+      for (; q + 1 < qe; q += 2) {
+        const int t0 = jt[q], t1 = jt[q + 1];
+        a0 += dterm(t0);
+        a1 += dterm(t1);
       }
+      if (q < qe) a0 += dterm(jt[q]);
       const int tgt = tg[g];
-      w.mat[(tgt / nv) * rs + tgt % nv] = acc;
+      w.mat[(tgt / nv) * rs + tgt % nv] = a0 + a1;
     }
   }
   // third-body and falloff-[M] part: G[i][m] = sum_p nu_ip dW_p/dM_m
@@ -450,11 +488,22 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
     const int* gi = t.c(CI_G_I);
     const int* gm = t.c(CI_G_M);
     const double* eff = t.d(HD_EFF);
-    for (int j = lane; j < ns; j += 32)
+    // the pairs are sorted by row: each row's contributions are summed in a register and added
+    // to the matrix once (no read-modify-write chain through shared memory per pair)
+    for (int j = lane; j < ns; j += 32) {
+      int cur = gi[0];
+      double acc = 0.0;
       for (int g = 0; g < ng; ++g) {
-        const double v = w.G[g];
-        if (v != 0.0) w.mat[gi[g] * rs + j] = fma(v, eff[gm[g] * ns + j], w.mat[gi[g] * rs + j]);
+        const int row = gi[g];
+        if (row != cur) {
+          w.mat[cur * rs + j] += acc;
+          acc = 0.0;
+          cur = row;
+        }
+        acc = fma(w.G[g], eff[gm[g] * ns + j], acc);
       }
+      if (ng > 0) w.mat[cur * rs + j] += acc;
+    }
   }
   __syncwarp();
   // temperature column: forward difference (one right-hand side)
@@ -470,9 +519,10 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   __syncwarp();
   // species columns
   const double* wm = t.d(HD_WMOL);
+  const double* iw = t.d(HD_INVW);
   for (int e = lane; e < ns * ns; e += 32) {
     const int i = e / ns, j = e % ns;
-    w.mat[i * rs + j] = wm[i] * w.mat[i * rs + j] / wm[j] - T * w.mat[i * rs + ns];
+    w.mat[i * rs + j] = w.mat[i * rs + j] * (wm[i] * iw[j]) - T * w.mat[i * rs + ns];
   }
   // temperature row
   const double* sc = t.d(HD_SCAL);
@@ -502,8 +552,18 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   __syncwarp();
   const double dTdu = -T / rho;
   for (int j = lane; j < ns; j += 32) {
-    double s = 0.0;
-    for (int k = 0; k < ns; ++k) s += w.hb[k] * w.mat[k * rs + j];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four independent chains
+    int k = 0;
+#pragma unroll
+    for (; k + 3 < ns; k += 4) {
+      s0 = fma(w.hb[k], w.mat[k * rs + j], s0);
+      s1 = fma(w.hb[k + 1], w.mat[(k + 1) * rs + j], s1);
+      s2 = fma(w.hb[k + 2], w.mat[(k + 2) * rs + j], s2);
+      s3 = fma(w.hb[k + 3], w.mat[(k + 3) * rs + j], s3);
+    }
+#pragma unroll
+    for (; k < ns; ++k) s0 = fma(w.hb[k], w.mat[k * rs + j], s0);
+    double s = (s0 + s1) + (s2 + s3);
     s += dTdu * scp;
     const double dcpm = (w.cb[j] - cpm) / rho + dTdu * ydcp;
     w.mat[ns * rs + j] = -(s + fT * dcpm) / cpm;
@@ -553,7 +613,8 @@ __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int
       sing = 1;
       continue;
     }
-    for (int i = k + 1 + lane; i < n; i += 32) a[i * rs + k] = a[i * rs + k] / d;
+    const double rd = 1.0 / d;
+    for (int i = k + 1 + lane; i < n; i += 32) a[i * rs + k] *= rd;
     __syncwarp();
     for (int i = k + 1 + lr; i < n; i += 4) {
       const double l = a[i * rs + k];

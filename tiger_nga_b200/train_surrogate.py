@@ -56,7 +56,7 @@ def make_pairs(chem, n_pairs: int, seed: int, chunk: int = 1 << 21):
         sol, dts = state_batch(chem.mechanism, m, seed + 1000 * k, side=128 if m == 1 << 21 else 0)
         s0[:, done:done + m].copy_(torch.from_numpy(sol))
         d[done:done + m].copy_(torch.from_numpy(dts))
-        x = s0[:, done:done + m].contiguous()
+        x = s0[:, done:done + m].clone()  # a copy: s0 keeps the initial states (a view of all of s0 would be s0)
         t0 = time.perf_counter()
         chem.substep(x, d[done:done + m], P_ATM)
         torch.cuda.synchronize()
