@@ -303,16 +303,23 @@ def main(argv=None):
                   "losses": [float(v) for v in rl], "s": time.perf_counter() - t0}
     del s0, s1, d
     gate = {}
-    if a.gate_pairs > 0 and a.dist == "uneven":
+    if a.gate_pairs > 0:
         # the gate learns the ensemble's errors on pairs it was not trained on, and its threshold
-        # is calibrated on further held-out cells against the plain solve
+        # is calibrated on further held-out cells against the plain solve (pairs of the same
+        # distribution: the uneven batch, or mixing-layer trajectories of other seeds)
         import torch
 
         t0 = time.perf_counter()
-        g0, g1, gd, _ = make_pairs(chem, a.gate_pairs, a.seed + 50021)
+        if a.dist == "mixing-layer":
+            g0, g1, gd, _ = make_trajectory_pairs(chem, a.gate_pairs, a.seed + 50021)
+        else:
+            g0, g1, gd, _ = make_pairs(chem, a.gate_pairs, a.seed + 50021)
         gl = sur.train_gate(g0, g1, gd, P_ATM, epochs=a.gate_epochs, batch=a.batch, lr=a.lr, under=a.gate_under)
         del g0, g1, gd
-        c0, c1, cd, _ = make_pairs(chem, a.calib_cells, a.seed + 70001)
+        if a.dist == "mixing-layer":
+            c0, c1, cd, _ = make_trajectory_pairs(chem, a.calib_cells, a.seed + 70001)
+        else:
+            c0, c1, cd, _ = make_pairs(chem, a.calib_cells, a.seed + 70001)
         tol, acc, rmax = calibrate_gate(chem, sur, c0, cd, c1, margin=a.calib_margin)
         sur.set_gate_tol(tol)
         del c0, c1, cd
