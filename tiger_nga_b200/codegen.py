@@ -679,11 +679,13 @@ def solver_tables(name: str) -> dict:
             cend.append(len(cterm))
         spp.append(len(cbeg))
     lanes = _lpt([e - b for b, e in zip(cbeg, cend)])
-    hi["cd_lane_ptr"], hi["cd_lane_list"] = [0], []
-    for L in lanes:
-        hi["cd_lane_list"] += L
-        hi["cd_lane_ptr"].append(len(hi["cd_lane_list"]))
-    hi["cd_beg"], hi["cd_end"], hi["cd_sp_ptr"], hi["cd_term"] = cbeg, cend, spp, cterm
+    # interleaved: step s of lane L at [s * 32 + L]; a lane walks its chunks one after another,
+    # the last term of a chunk carries the chunk id (bit 20 set, id from bit 21); lanes are padded
+    # with no-op terms (nu = 0) to the same number of steps
+    seqs = [[[cterm[q] for q in range(cbeg[ch], cend[ch])] for ch in L] for L in lanes]
+    il, ncdstep = _interleave(seqs, lambda t: t >> 8, lambda t, ch: t | (1 << 20) | (ch << 21),
+                              [[ch for ch in L] for L in lanes], 0)
+    hi["cd_sp_ptr"], hi["cd_il"] = spp, il
 
     # Jacobian, direct mass-action part: groups per (i, j), balanced over lanes
     groups: dict[tuple, list] = {}
@@ -695,16 +697,23 @@ def solver_tables(name: str) -> dict:
                     groups.setdefault((i, j), []).append((p << 12) | (rp << 8) | _nu8(nu[i, r]))
     keys = sorted(groups)
     lanes = _lpt([len(groups[k]) for k in keys])
-    ci["jd_lane_ptr"], ci["jd_lane_list"] = [0], []
-    for L in lanes:
-        ci["jd_lane_list"] += L
-        ci["jd_lane_ptr"].append(len(ci["jd_lane_list"]))
-    ci["jd_tgt"], ci["jd_beg"], ci["jd_end"], ci["jd_term"] = [], [], [], []
-    for k in keys:
-        ci["jd_tgt"].append(k[0] * nv + k[1])
-        ci["jd_beg"].append(len(ci["jd_term"]))
-        ci["jd_term"] += groups[k]
-        ci["jd_end"].append(len(ci["jd_term"]))
+    rs = nv if nv % 2 else nv + 1  # the solver's matrix row stride
+    # interleaved int2 terms (x: slot | other reactant a << 10 | other reactant b << 17 | third-body
+    # set << 24, none = 127; y: nu | target matrix offset << 8 | last-of-group << 20), so that a
+    # term is decoded without looking up the slot's reactant word
+    def jd_word(p, rp, nu8):
+        s_ = m32.slots[order[p]]
+        others = [c for o, c in enumerate(s_.C) if o != rp] + [NONE7, NONE7]
+        mw = s_.M if s_.M >= 0 else NONE7
+        return (p | (others[0] << 10) | (others[1] << 17) | (mw << 24), nu8)
+
+    seqs = [[[jd_word(t >> 12, (t >> 8) & 15, t & 0xFF) for t in groups[keys[g]]] for g in L] for L in lanes]
+    tgt_of = {g: keys[g][0] * rs + keys[g][1] for g in range(len(keys))}
+    il, njdstep = _interleave(seqs, lambda w: w[0] & 1023, lambda w, g: (w[0], w[1] | (tgt_of[g] << 8) | (1 << 20)),
+                              [list(L) for L in lanes], (0 | (NONE7 << 10) | (NONE7 << 17) | (NONE7 << 24), 0))
+    if len(keys) and max(tgt_of.values()) >= 4096:
+        raise ValueError("solver matrix too large for the packed Jacobian terms")
+    ci["jd_il"] = [v for w in il for v in w]
 
     # Jacobian, third-body and falloff-[M] part: G[i][m] pairs
     pairs: dict[tuple, list] = {}
@@ -731,15 +740,50 @@ def solver_tables(name: str) -> dict:
         ci["g_term"] += pairs[k]
         ci["g_end"].append(len(ci["g_term"]))
     sizes = {"ns": ns, "nv": nv, "nslot": nslot, "nm": nm, "nfo": nfo, "nfc": nfc, "ncdchunk": len(cbeg),
-             "njdgrp": len(keys), "ngpair": len(pkeys)}
+             "njdgrp": len(keys), "ngpair": len(pkeys), "ncdstep": ncdstep, "njdstep": njdstep}
     return {"hd": hd, "hi": hi, "ci": ci, "sizes": sizes, "order": order}
 
 
 SV_HD_KEYS = ("slot", "fo", "fc", "eff", "th", "wmol", "invw", "scal")
-SV_HI_KEYS = ("slot", "fo", "fc", "cd_lane_ptr", "cd_lane_list", "cd_beg", "cd_end", "cd_sp_ptr", "cd_term")
-SV_CI_KEYS = ("jd_lane_ptr", "jd_lane_list", "jd_tgt", "jd_beg", "jd_end", "jd_term",
-              "g_lane_ptr", "g_lane_list", "g_i", "g_m", "g_beg", "g_end", "g_term")
-SV_SIZE_KEYS = ("ns", "nv", "nslot", "nm", "nfo", "nfc", "ncdchunk", "njdgrp", "ngpair")
+SV_HI_KEYS = ("slot", "fo", "fc", "cd_sp_ptr", "cd_il")
+SV_CI_KEYS = ("jd_il", "g_lane_ptr", "g_lane_list", "g_i", "g_m", "g_beg", "g_end", "g_term")
+SV_SIZE_KEYS = ("ns", "nv", "nslot", "nm", "nfo", "nfc", "ncdchunk", "njdgrp", "ngpair", "ncdstep", "njdstep")
+
+
+def _interleave(seqs, slot_of, mark_last, ids, pad):
+    """Per-lane term sequences -> one list with step s of lane L at [s * 32 + L].
+
+    seqs[L] is lane L's list of groups (each a list of terms summed into one output); the last
+    term of group g is replaced by mark_last(term, ids[L][g]). Terms within a group may be
+    reordered: at every step each lane picks, from its current group, a term whose slot falls in a
+    shared-memory bank (slot mod 16, 8-byte words) not yet used at this step by the other lanes of
+    its half-warp, so that the 64-bit reads of the slot values are as conflict-free as possible.
+    Lanes are padded to the same number of steps with `pad` (a no-op term)."""
+    nsteps = max([sum(len(g) for g in L) for L in seqs] + [0])
+    state = [[list(g) for g in L] for L in seqs]
+    gi = [0] * 32
+    out = [[pad] * 32 for _ in range(nsteps)]
+    for st in range(nsteps):
+        used = [set(), set()]
+        for lane in range(32):
+            L = state[lane] if lane < len(state) else []
+            while gi[lane] < len(L) and not L[gi[lane]]:
+                gi[lane] += 1
+            if gi[lane] >= len(L):
+                continue
+            grp = L[gi[lane]]
+            half = used[lane // 16]
+            pick = 0
+            for q, t in enumerate(grp):
+                if slot_of(t) % 16 not in half:
+                    pick = q
+                    break
+            t = grp.pop(pick)
+            half.add(slot_of(t) % 16)
+            if not grp:
+                t = mark_last(t, ids[lane][gi[lane]])
+            out[st][lane] = t
+    return [t for row in out for t in row], nsteps
 
 
 def solver_header(name: str) -> str:

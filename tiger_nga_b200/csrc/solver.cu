@@ -138,12 +138,12 @@ static size_t block_smem(const SolverState* s, int warps, int cold) {
 
 static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   SolverState* s = h->solver;
-  // the Jacobian's term lists go to shared memory when the blocks still leave the SM about a
-  // quarter of its shared/L1 capacity as L1 (measured: with GRI-Mech, 224 KB of shared memory
-  // per SM left too little L1 for the solver's stack and was slower; H2 gains 9 %)
+  // the Jacobian's term tables go to shared memory whenever the blocks still fit (the solver
+  // kernels keep no stack, so L1 has nothing else to hold; the staged static BDF coefficients
+  // take a further 1 KB)
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->cfg.device);
-  s->cold_in_smem = block_smem(s, warps, 1) * occ <= (size_t)optin * 7 / 8 ? 1 : 0;
+  s->cold_in_smem = (block_smem(s, warps, 1) + 1024) * occ <= (size_t)optin ? 1 : 0;
   const size_t smem = block_smem(s, warps, s->cold_in_smem);
   BdfKernelFn k = bdf_kernel(h, warps, occ);
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -345,11 +345,19 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
       bdf_kernel(h, warps, occ)<<<s->blocks, warps * 32, smem, st>>>(L);
       note(cudaGetLastError(), "solver kernel");
     }
-    cudaGraph_t graph;
+    cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(st, &graph);
-    if (first != cudaSuccess)
-      return set_error(TNG_ERR_CUDA, "solver graph capture, %s (%d blocks x %d threads, %zu B shared): %s", where,
-                       s->blocks, warps * 32, smem, cudaGetErrorString(first));
+    if (first != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      cudaFuncAttributes fa{};
+      cudaFuncGetAttributes(&fa, bdf_kernel(h, warps, occ));
+      cudaGetLastError();
+      return set_error(TNG_ERR_CUDA,
+                       "solver graph capture, %s (%d blocks x %d threads, %zu B shared; kernel: %d registers, %zu B "
+                       "static shared, %d B dynamic shared allowed, %d threads allowed): %s",
+                       where, s->blocks, warps * 32, smem, fa.numRegs, fa.sharedSizeBytes, fa.maxDynamicSharedSizeBytes,
+                       fa.maxThreadsPerBlock, cudaGetErrorString(first));
+    }
     if (e != cudaSuccess) return cuda_error(e, "solver graph capture");
     e = cudaGraphInstantiate(&s->graph[slot], graph, 0);
     cudaGraphDestroy(graph);

@@ -51,6 +51,7 @@ struct SvT {
   static constexpr int NS = LY::size(SZ_NS), NV = LY::size(SZ_NV), NSLOT = LY::size(SZ_NSLOT);
   static constexpr int NM = LY::size(SZ_NM), NFC = LY::size(SZ_NFC), NCD = LY::size(SZ_NCDCHUNK);
   static constexpr int NGP = LY::size(SZ_NGPAIR), NFO = LY::size(SZ_NFO);
+  static constexpr int NCDSTEP = LY::size(SZ_NCDSTEP), NJDSTEP = LY::size(SZ_NJDSTEP);
   static constexpr int RS = (NV % 2 == 0) ? NV + 1 : NV;  // matrix row stride (odd: fewer bank conflicts)
   const double* __restrict__ hd;
   const int* __restrict__ hi;
@@ -323,28 +324,20 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
   }
   __syncwarp();
   {
-    const int* lp = t.i(HI_CD_LANE_PTR);
-    const int* ll = t.i(HI_CD_LANE_LIST);
-    const int* cb = t.i(HI_CD_BEG);
-    const int* ce = t.i(HI_CD_END);
-    const int* ct = t.i(HI_CD_TERM);
-    auto add = [&](double acc, const int term) {
-      const int nu = nu_of(term);
-      const double wv = w.W[term >> 8];
-      return nu == 1 ? acc + wv : (nu == -1 ? acc - wv : fma((double)nu, wv, acc));
-    };
-    for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
-      const int ch = ll[i];
-      const int qe = ce[ch];
-      double a0 = 0.0, a1 = 0.0;  // two partial sums: independent chains
-      int q = cb[ch];
-      for (; q + 1 < qe; q += 2) {
-        const int t0 = ct[q], t1 = ct[q + 1];
-        a0 = add(a0, t0);
-        a1 = add(a1, t1);
+    // production-rate chunks: every lane walks the same number of steps over its interleaved
+    // terms (conflict-free term reads, compile-time trip count) and stores a chunk's sum at the
+    // chunk's last term
+    const int* ct = t.i(HI_CD_IL) + lane;
+    double acc = 0.0;
+#pragma unroll 4
+    for (int st = 0; st < SvT<LY>::NCDSTEP; ++st) {
+      const int term = ct[32 * st];
+      const double wv = w.W[(term >> 8) & 4095];
+      if (term & 0xFF) acc = fma((double)nu_of(term), wv, acc);  // nu = 0: a padding step
+      if (term & (1 << 20)) {
+        w.part[(unsigned)term >> 21] = acc;
+        acc = 0.0;
       }
-      if (q < qe) a0 = add(a0, ct[q]);
-      w.part[ch] = a0 + a1;
     }
   }
   __syncwarp();
@@ -406,41 +399,25 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   for (int q = SvT<LY>::NFO + lane; q < nslot; q += 32) w.W[q] = plain_const(t, c, q, sw[2 * q]);
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
-  // direct mass-action part: dW_p/dC_j for every reactant occurrence
+  // direct mass-action part: nu dW_p/dC_j for every reactant occurrence, the terms of one matrix
+  // entry summed by one lane; the terms are interleaved by lane with the other reactants decoded
+  // at generation time, so a step is one 8-byte term read and up to four independent loads
   {
-    const int* lp = t.c(CI_JD_LANE_PTR);
-    const int* ll = t.c(CI_JD_LANE_LIST);
-    const int* tg = t.c(CI_JD_TGT);
-    const int* gb = t.c(CI_JD_BEG);
-    const int* ge = t.c(CI_JD_END);
-    const int* jt = t.c(CI_JD_TERM);
-    // nu * dW_p/dC_j of one term (the product of the slot's other reactant concentrations)
-    auto dterm = [&](const int term) {
-      const int pp = term >> 12, rp = (term >> 8) & 15;
-      const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
-      double d = w.W[pp];
-      const int mw = w1 & 127;
+    const int2* jt = reinterpret_cast<const int2*>(t.c(CI_JD_IL)) + lane;
+    double acc = 0.0;
+#pragma unroll 4
+    for (int st = 0; st < SvT<LY>::NJDSTEP; ++st) {
+      const int2 tm = jt[32 * st];
+      const int pa = tm.x & 1023, ra = (tm.x >> 10) & 127, rb = (tm.x >> 17) & 127, mw = (tm.x >> 24) & 127;
+      double d = w.W[pa];
+      if (ra != kNone7) d *= w.C[ra];
+      if (rb != kNone7) d *= w.C[rb];
       if (mw != kNone7) d *= w.Ms[mw];
-#pragma unroll
-      for (int o = 0; o < 3; ++o) {
-        const int r = (w0 >> (4 + 7 * o)) & 127;
-        if (o != rp && r != kNone7) d *= w.C[r];
+      if (tm.y & 0xFF) acc = fma((double)nu_of(tm.y), d, acc);  // nu = 0: a padding step
+      if (tm.y & (1 << 20)) {
+        w.mat[(tm.y >> 8) & 4095] = acc;
+        acc = 0.0;
       }
-      return (double)nu_of(term) * d;
-    };
-    for (int i = lp[lane]; i < lp[lane + 1]; ++i) {
-      const int g = ll[i];
-      const int qe = ge[g];
-      double a0 = 0.0, a1 = 0.0;  // two independent chains
-      int q = gb[g];
-      for (; q + 1 < qe; q += 2) {
-        const int t0 = jt[q], t1 = jt[q + 1];
-        a0 += dterm(t0);
-        a1 += dterm(t1);
-      }
-      if (q < qe) a0 += dterm(jt[q]);
-      const int tgt = tg[g];
-      w.mat[(tgt / nv) * rs + tgt % nv] = a0 + a1;
     }
   }
   // third-body and falloff-[M] part: G[i][m] = sum_p nu_ip dW_p/dM_m

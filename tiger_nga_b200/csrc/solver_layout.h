@@ -6,20 +6,21 @@
 
 namespace tng {
 
-enum SvSize { SZ_NS, SZ_NV, SZ_NSLOT, SZ_NM, SZ_NFO, SZ_NFC, SZ_NCDCHUNK, SZ_NJDGRP, SZ_NGPAIR, SZ_COUNT };
+enum SvSize {
+  SZ_NS, SZ_NV, SZ_NSLOT, SZ_NM, SZ_NFO, SZ_NFC, SZ_NCDCHUNK, SZ_NJDGRP, SZ_NGPAIR, SZ_NCDSTEP, SZ_NJDSTEP, SZ_COUNT
+};
 // hot doubles: slot records (4 per slot: lnA|A, E, n, -), falloff (6: lnA0 E0 n0 lnAi Ei ni),
 // F_cent (6: a0 c0 a1 c1 a2 c2), dense efficiencies (nm x ns), thermo (ns x 24: hi 12, lo 12),
 // molar masses, their inverses, scalars
 enum SvHd { HD_SLOT, HD_FO, HD_FC, HD_EFF, HD_TH, HD_WMOL, HD_INVW, HD_SCAL, HD_COUNT };
 // hot ints: slot words (2 per slot: flags|r0<<4|r1<<11|r2<<18, mw|fo<<8), falloff word
-// (f0|f1<<4|(fc+1)<<8|m<<16), F_cent forms, production-rate chunk lists (terms p<<8|nu)
-enum SvHi { HI_SLOT, HI_FO, HI_FC, HI_CD_LANE_PTR, HI_CD_LANE_LIST, HI_CD_BEG, HI_CD_END, HI_CD_SP_PTR, HI_CD_TERM, HI_COUNT };
-// cold ints: Jacobian direct groups (terms p<<12|reactant position<<8|nu) and third-body pairs
-// (terms p<<12|kind<<8|nu)
-enum SvCi {
-  CI_JD_LANE_PTR, CI_JD_LANE_LIST, CI_JD_TGT, CI_JD_BEG, CI_JD_END, CI_JD_TERM,
-  CI_G_LANE_PTR, CI_G_LANE_LIST, CI_G_I, CI_G_M, CI_G_BEG, CI_G_END, CI_G_TERM, CI_COUNT
-};
+// (f0|f1<<4|(fc+1)<<8|m<<16), F_cent forms, chunks per species, and the production-rate terms
+// interleaved by lane (step s of lane L at [s*32 + L]: nu | p<<8 | last-of-chunk<<20 | chunk<<21)
+enum SvHi { HI_SLOT, HI_FO, HI_FC, HI_CD_SP_PTR, HI_CD_IL, HI_COUNT };
+// cold ints: the Jacobian's mass-action terms interleaved by lane as int2 (x: p | other reactant
+// a<<10 | other reactant b<<17 | third-body set<<24, 127 = none; y: nu | matrix offset<<8 |
+// last-of-group<<20), and the third-body pairs (terms p<<12|kind<<8|nu)
+enum SvCi { CI_JD_IL, CI_G_LANE_PTR, CI_G_LANE_LIST, CI_G_I, CI_G_M, CI_G_BEG, CI_G_END, CI_G_TERM, CI_COUNT };
 enum SvScal { SC_RGAS, SC_TMID, SC_TN0, SC_TN1, SC_TC0, SC_TC1, SC_TD, SC_LNKMIN, SC_INVLN10 };
 constexpr int kNone7 = 127;
 
