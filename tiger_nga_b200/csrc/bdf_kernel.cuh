@@ -478,6 +478,17 @@ __global__ void __launch_bounds__(WARPS * 32)
   }
 }
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`, never lower it: the batch
+// solver and the no-allocation entry launch the same kernels with different shared-memory
+// plans, and each must keep working after the other has run.
+inline cudaError_t ensure_dynamic_smem(const void* kernel, size_t bytes) {
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 // The solver kernels of one mechanism (instantiated in the mechanism's generated unit and
 // reached through its operation table).
 typedef void (*BdfKernelFn)(const BdfLaunch);

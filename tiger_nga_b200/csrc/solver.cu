@@ -146,7 +146,7 @@ static int configure_kernel(tng_chem* h, int warps, int occ, int* blocks_out) {
   s->cold_in_smem = (block_smem(s, warps, 1) + 1024) * occ <= (size_t)optin ? 1 : 0;
   const size_t smem = block_smem(s, warps, s->cold_in_smem);
   BdfKernelFn k = bdf_kernel(h, warps, occ);
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_dynamic_smem((const void*)k, smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, warps * 32, smem);
@@ -322,6 +322,8 @@ int substep_run(tng_chem* h, double* state, int64_t ncells, int64_t ld, const do
     const size_t smem = block_smem(s, warps, s->cold_in_smem);
     L.cold_in_smem = s->cold_in_smem;
     cudaStream_t st = h->stream;
+    if ((e = ensure_dynamic_smem((const void*)bdf_kernel(h, warps, occ), smem)) != cudaSuccess)
+      return cuda_error(e, "solver shared memory");
     cudaError_t pending = cudaGetLastError();  // an earlier asynchronous error is reported, not captured
     if (pending != cudaSuccess) return cuda_error(pending, "implicit substep (error pending before the graph capture)");
     cudaError_t first = cudaSuccess;            // the first error inside the capture, and where
@@ -418,7 +420,7 @@ extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncel
   SolverState* s = h->solver;
   const size_t smem = block_smem(s, 4, 0);
   const RhsJacFn kern = h->ops->sk->rhs_jac4;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_dynamic_smem((const void*)kern, smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   const int blocks = (int)std::min<int64_t>((ncells + 3) / 4, 148 * 8);
   kern<<<blocks, 128, smem, h->stream>>>(s->dev, state, ld, (int)ncells, p, rhs, jac, s->smem_warp);

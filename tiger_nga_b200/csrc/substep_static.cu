@@ -180,7 +180,7 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   const size_t smem = ((size_t)hot_smem_doubles(L) + (size_t)warps * a.smem_warp) * sizeof(double);
   const SolverKernels* sk = o->sk;
   const BdfKernelFn kern = warps == 2 ? sk->bdf2 : warps == 4 ? sk->bdf4 : sk->bdf8;
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = ensure_dynamic_smem((const void*)kern, smem);
   if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: shared memory");
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, warps * 32, smem);
