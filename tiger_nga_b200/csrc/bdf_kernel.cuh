@@ -32,6 +32,9 @@ __device__ __forceinline__ bool warp_all_finite(const double v0, const double v1
 
 #define TNG_ZLOOP(j) _Pragma("unroll") for (int j = 0; j <= kQmax + 1; ++j)
 
+// x^y of the step-size and order selection (x > 0), one out-of-line copy
+static __device__ __noinline__ double bdf_pow(const double x, const double y) { return pow(x, y); }
+
 __device__ __forceinline__ void z_predict(double (&z)[kQmax + 2][2], const int q) {
 #pragma unroll
   for (int k = 0; k < kQmax; ++k) {
@@ -228,6 +231,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
           }
           jac_call(t, w.mat, z[0][0], z[0][1], f[0], f[1], p, lane);
           ++nje;
+#pragma unroll 4
           for (int e = lane; e < nv * rs; e += 32) w.mat[e] = -gamma * w.mat[e];
           __syncwarp();
           for (int i = lane; i < nv; i += 32) w.mat[i * rs + i] += 1.0;
@@ -317,7 +321,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             qprev = 0;
             continue;
           }
-          double eta = 1.0 / (pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+          double eta = 1.0 / (bdf_pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
           eta = fmax(0.1, fmin(0.9, eta));
           if (nef >= 2) eta = fmin(eta, 0.2);
           z_rescale(z, q, eta);
@@ -345,18 +349,18 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
       ewt[1] = h1 ? 1.0 / (rtol * fabs(z[0][1]) + atol) : 0.0;
       if (tcur >= dt) break;
       --qwait;
-      const double eta_q = 1.0 / (pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+      const double eta_q = 1.0 / (bdf_pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
       double eta_m = 0.0, eta_p = 0.0;
       if (qwait <= 0) {
         if (q > 1) {
           const double ddn = C.dnc[q] * wrms2(zget(z, q, 0), zget(z, q, 1), ewt[0], ewt[1], nv, lane);
-          eta_m = 1.0 / (pow(6.0 * ddn, 1.0 / q) + 1e-6);
+          eta_m = 1.0 / (bdf_pow(6.0 * ddn, 1.0 / q) + 1e-6);
         }
         if (q < kQmax && qprev == q) {
-          const double r = pow(h / hprev, q + 1);
+          const double r = bdf_pow(h / hprev, q + 1);
           const double dup =
               C.upc[q] * wrms2(acor[0] - r * acorp[0], acor[1] - r * acorp[1], ewt[0], ewt[1], nv, lane);
-          eta_p = 1.0 / (pow(10.0 * dup, 1.0 / (q + 2)) + 1e-6);
+          eta_p = 1.0 / (bdf_pow(10.0 * dup, 1.0 / (q + 2)) + 1e-6);
         }
       }
       double eta = eta_q;

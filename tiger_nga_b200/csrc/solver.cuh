@@ -139,6 +139,8 @@ struct WarpMem {
   double* vb;   // 64 vector buffer
   double* hb;   // 64 enthalpies
   double* cb;   // 64 heat capacities (Jacobian), then the pivot reciprocals of the LU
+  double* lpr;  // nfo: ln Pr of the falloff slots (rate-constant pass of the Jacobian)
+  double* cp;   // 8: the cell's CellPrep from the last rate pass
   int* piv;     // 64 pivots
   int* perm;    // 64: the composed row permutation of the LU
 };
@@ -146,7 +148,7 @@ struct WarpMem {
 __host__ __device__ inline int warp_mem_doubles(const SvLayout& L, int rs) {
   const int nv = L.size[SZ_NV];
   return nv * rs + L.size[SZ_NSLOT] + 64 + 2 * L.size[SZ_NM] + 3 * L.size[SZ_NFC] + L.size[SZ_NCDCHUNK] +
-         L.size[SZ_NGPAIR] + 3 * 64 + 64 /* pivots and permutation as ints */ + 8;
+         L.size[SZ_NGPAIR] + 3 * 64 + L.size[SZ_NFO] + 8 + 64 /* pivots and permutation as ints */ + 8;
 }
 
 template <class LY>
@@ -165,6 +167,8 @@ __device__ __forceinline__ WarpMem warp_mem(double* base) {
   w.vb = p; p += 64;
   w.hb = p; p += 64;
   w.cb = p; p += 64;
+  w.lpr = p; p += T::NFO;
+  w.cp = p; p += 8;
   w.piv = reinterpret_cast<int*>(p);
   w.perm = w.piv + 64;
   return w;
@@ -296,11 +300,14 @@ __device__ __forceinline__ double plain_const(const SvT<LY>& t, const CellPrep& 
   return (w0 & 8) ? a : v;
 }
 
-// finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
+// The cell preparation and the slot loops, shared by the right-hand side and the Jacobian in one
+// out-of-line copy (the solver's code must fit the instruction cache): W[q] = the slot's rate
+// constant (products = 0; ln Pr of the falloff slots into w.lpr) or its rate (products = 1:
+// times the reactant concentrations and the third-body sum). The cell's CellPrep is left in w.cp.
 template <class LY>
-__device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
-                                         const double p, double& f0, double& f1, const int lane) {
-  constexpr int ns = SvT<LY>::NS, nslot = SvT<LY>::NSLOT;
+static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, const double y0, const double y1,
+                                               const double p, const int lane, const int products) {
+  const WarpMem w = warp_mem<LY>(wb);
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
   auto mass_action = [&](double v, const int w0, const int w1) {
@@ -315,21 +322,47 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
   // loop without divergent paths, whose independent exponentials the compiler interleaves
   for (int q = lane; q < SvT<LY>::NFO; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
-    w.W[q] = mass_action(rate_const(t, w, c, q, w0, w1, nullptr), w0, w1);
+    double lpr = 0.0;
+    const double k = rate_const(t, w, c, q, w0, w1, &lpr);
+    if (products) {
+      w.W[q] = mass_action(k, w0, w1);
+    } else {
+      w.W[q] = k;
+      w.lpr[q] = lpr;
+    }
   }
 #pragma unroll 2
-  for (int q = SvT<LY>::NFO + lane; q < nslot; q += 32) {
+  for (int q = SvT<LY>::NFO + lane; q < SvT<LY>::NSLOT; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
-    w.W[q] = mass_action(plain_const(t, c, q, w0), w0, w1);
+    const double k = plain_const(t, c, q, w0);
+    w.W[q] = products ? mass_action(k, w0, w1) : k;
+  }
+  if (lane == 0) {
+    w.cp[0] = c.rho, w.cp[1] = c.T, w.cp[2] = c.LT, w.cp[3] = c.invRT, w.cp[4] = c.invT, w.cp[5] = c.irho;
   }
   __syncwarp();
+}
+
+__device__ __forceinline__ CellPrep load_prep(const WarpMem& w) {
+  CellPrep c;
+  c.rho = w.cp[0], c.T = w.cp[1], c.LT = w.cp[2], c.invRT = w.cp[3], c.invT = w.cp[4], c.irho = w.cp[5];
+  return c;
+}
+
+// finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
+template <class LY>
+__device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
+                                         const double p, double& f0, double& f1, const int lane) {
+  constexpr int ns = SvT<LY>::NS;
+  prep_rates<LY>(t, w.mat, y0, y1, p, lane, 1);
+  const CellPrep c = load_prep(w);
   {
     // production-rate chunks: every lane walks the same number of steps over its interleaved
     // terms (conflict-free term reads, compile-time trip count) and stores a chunk's sum at the
     // chunk's last term
     const int* ct = t.i(HI_CD_IL) + lane;
     double acc = 0.0;
-#pragma unroll 4
+#pragma unroll 2
     for (int st = 0; st < SvT<LY>::NCDSTEP; ++st) {
       const int term = ct[32 * st];
       const double wv = w.W[(term >> 8) & 4095];
@@ -391,12 +424,11 @@ static __device__ __noinline__ double2 rhs_call(const SvT<LY> t, double* wb, con
 template <class LY>
 __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
                                          const double f0, const double f1, const double p, const int lane) {
-  constexpr int ns = SvT<LY>::NS, nv = ns + 1, nslot = SvT<LY>::NSLOT, rs = SvT<LY>::RS;
-  const CellPrep c = prepare(t, w, y0, y1, p, lane);
+  constexpr int ns = SvT<LY>::NS, nv = ns + 1, rs = SvT<LY>::RS;
+  prep_rates<LY>(t, w.mat, y0, y1, p, lane, 0);
+  const CellPrep c = load_prep(w);
   const int* sw = t.i(HI_SLOT);
-  for (int q = lane; q < SvT<LY>::NFO; q += 32) w.W[q] = rate_const(t, w, c, q, sw[2 * q], sw[2 * q + 1], nullptr);
-#pragma unroll 2
-  for (int q = SvT<LY>::NFO + lane; q < nslot; q += 32) w.W[q] = plain_const(t, c, q, sw[2 * q]);
+#pragma unroll 4
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
   // direct mass-action part: nu dW_p/dC_j for every reactant occurrence, the terms of one matrix
@@ -405,7 +437,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   {
     const int2* jt = reinterpret_cast<const int2*>(t.c(CI_JD_IL)) + lane;
     double acc = 0.0;
-#pragma unroll 4
+#pragma unroll 2
     for (int st = 0; st < SvT<LY>::NJDSTEP; ++st) {
       const int2 tm = jt[32 * st];
       const int pa = tm.x & 1023, ra = (tm.x >> 10) & 127, rb = (tm.x >> 17) & 127, mw = (tm.x >> 24) & 127;
@@ -447,9 +479,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
           const int fw = t.i(HI_FO)[w1 >> 8];
           const double Mf = w.Ms[fw >> 16];
           if (Mf > 0.0) {
-            double lpr;
-            rate_const(t, w, c, pp, w0, w1, &lpr);
-            const double pr = rexp(t, lpr);
+            const double pr = rexp(t, w.lpr[pp]);  // ln Pr from the rate-constant pass
             const int mw = w1 & 127;
             val = w.W[pp] / (Mf * (1.0 + pr)) * prodC * (mw != kNone7 ? w.Ms[mw] : 1.0);
           }
@@ -497,6 +527,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   // species columns
   const double* wm = t.d(HD_WMOL);
   const double* iw = t.d(HD_INVW);
+#pragma unroll 2
   for (int e = lane; e < ns * ns; e += 32) {
     const int i = e / ns, j = e % ns;
     w.mat[i * rs + j] = w.mat[i * rs + j] * (wm[i] * iw[j]) - T * w.mat[i * rs + ns];
@@ -553,6 +584,9 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
 __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int* piv, const int lane) {
   int sing = 0;
   const int lr = lane >> 3, lc = lane & 7;
+  // one copy of the pivot step: unrolled over the compile-time size the factorisation would
+  // not fit the instruction cache beside the rest of the solver
+#pragma unroll 1
   for (int k = 0; k < n; ++k) {
     double best = -1.0;
     int bi = n;
@@ -607,7 +641,9 @@ __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int
 __device__ __forceinline__ void lu_finish(const double* a, const int n, const int rs, const int* piv, int* perm,
                                           double* dinv, const int lane) {
   if (lane == 0) {
+#pragma unroll 1
     for (int i = 0; i < n; ++i) perm[i] = i;
+#pragma unroll 1
     for (int k = 0; k < n; ++k) {
       const int p = piv[k];
       const int t = perm[k];
@@ -646,11 +682,13 @@ __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const
   double b0 = i0 < n ? vb[perm[i0]] : 0.0;
   double b1 = i1 < n ? vb[perm[i1]] : 0.0;
   __syncwarp();
+#pragma unroll 2
   for (int k = 0; k < n - 1; ++k) {
     const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31);
     if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
     if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
+#pragma unroll 2
   for (int k = n - 1; k >= 0; --k) {
     const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31) * dinv[k];
     if (i0 == k) b0 = bk;
