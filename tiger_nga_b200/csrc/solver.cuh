@@ -360,15 +360,19 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
     // production-rate chunks: every lane walks the same number of steps over its interleaved
     // terms (conflict-free term reads, compile-time trip count) and stores a chunk's sum at the
     // chunk's last term
-    const int* ct = t.i(HI_CD_IL) + lane;
+    // (the chunk sums go to a region the walk never reads: distinct restrict pointers let the
+    // loads of later steps move ahead of the stores)
+    const int* __restrict__ ct = t.i(HI_CD_IL) + lane;
+    const double* __restrict__ Wr = w.W;
+    double* __restrict__ part = w.part;
     double acc = 0.0;
 #pragma unroll 2
     for (int st = 0; st < SvT<LY>::NCDSTEP; ++st) {
       const int term = ct[32 * st];
-      const double wv = w.W[(term >> 8) & 4095];
+      const double wv = Wr[(term >> 8) & 4095];
       if (term & 0xFF) acc = fma((double)nu_of(term), wv, acc);  // nu = 0: a padding step
       if (term & (1 << 20)) {
-        w.part[(unsigned)term >> 21] = acc;
+        part[(unsigned)term >> 21] = acc;
         acc = 0.0;
       }
     }
@@ -435,19 +439,25 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   // entry summed by one lane; the terms are interleaved by lane with the other reactants decoded
   // at generation time, so a step is one 8-byte term read and up to four independent loads
   {
-    const int2* jt = reinterpret_cast<const int2*>(t.c(CI_JD_IL)) + lane;
+    // (the matrix region never overlaps the slot, concentration and third-body regions read
+    // here: distinct restrict pointers let the loads of later steps move ahead of the stores)
+    const int2* __restrict__ jt = reinterpret_cast<const int2*>(t.c(CI_JD_IL)) + lane;
+    const double* __restrict__ Wr = w.W;
+    const double* __restrict__ Cr = w.C;
+    const double* __restrict__ Mr = w.Ms;
+    double* __restrict__ mat = w.mat;
     double acc = 0.0;
 #pragma unroll 2
     for (int st = 0; st < SvT<LY>::NJDSTEP; ++st) {
       const int2 tm = jt[32 * st];
       const int pa = tm.x & 1023, ra = (tm.x >> 10) & 127, rb = (tm.x >> 17) & 127, mw = (tm.x >> 24) & 127;
-      double d = w.W[pa];
-      if (ra != kNone7) d *= w.C[ra];
-      if (rb != kNone7) d *= w.C[rb];
-      if (mw != kNone7) d *= w.Ms[mw];
+      double d = Wr[pa];
+      if (ra != kNone7) d *= Cr[ra];
+      if (rb != kNone7) d *= Cr[rb];
+      if (mw != kNone7) d *= Mr[mw];
       if (tm.y & 0xFF) acc = fma((double)nu_of(tm.y), d, acc);  // nu = 0: a padding step
       if (tm.y & (1 << 20)) {
-        w.mat[(tm.y >> 8) & 4095] = acc;
+        mat[(tm.y >> 8) & 4095] = acc;
         acc = 0.0;
       }
     }
@@ -636,6 +646,71 @@ __device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int
   return sing;
 }
 
+// The same factorisation for a compile-time size N (row stride RS), as the solver runs it:
+//  * the pivot is the exact first maximum of |a[i][k]|, found with three warp reductions on the
+//    64-bit pattern of |a| (a non-negative double orders like its bit pattern; NaN counts as 0)
+//    instead of five rounds of shuffles;
+//  * each lane keeps the pivot-row entries of its columns in registers for the trailing update,
+//    so an update is one load and one store (4 x 8 lane tiles, rows walked at run time).
+// Returns nonzero if a pivot is zero or not finite.
+template <int N, int RS>
+__device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const int lane) {
+  constexpr int NC = (N + 7) / 8;  // columns of a lane (8 column groups)
+  int sing = 0;
+  const int lr = lane >> 3, lc = lane & 7;
+#pragma unroll 1
+  for (int k = 0; k < N; ++k) {
+    unsigned long long key = 0ULL;
+    int bi = N;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = k + lane + 32 * h;
+      if (i < N) {
+        const double v = fabs(a[i * RS + k]);
+        const unsigned long long kk = (v == v) ? (unsigned long long)__double_as_longlong(v) : 0ULL;
+        if (bi == N || kk > key) key = kk, bi = i;
+      }
+    }
+    const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(kFull, bi < N ? khi : 0u);
+    const unsigned mlo = __reduce_max_sync(kFull, (bi < N && khi == mhi) ? klo : 0u);
+    bi = (int)__reduce_min_sync(kFull, (bi < N && khi == mhi && klo == mlo) ? (unsigned)bi : 0xffffffffu);
+    if (bi >= N) bi = k;  // no row (cannot happen for k < N)
+    if (lane == 0) piv[k] = bi;
+    if (bi != k)
+      for (int j = lane; j < N; j += 32) {
+        const double tmp = a[k * RS + j];
+        a[k * RS + j] = a[bi * RS + j];
+        a[bi * RS + j] = tmp;
+      }
+    __syncwarp();
+    const double d = a[k * RS + k];
+    if (d == 0.0 || !isfinite(d)) {
+      sing = 1;
+      continue;
+    }
+    const double rd = 1.0 / d;
+    for (int i = k + 1 + lane; i < N; i += 32) a[i * RS + k] *= rd;
+    double u[NC];
+#pragma unroll
+    for (int p = 0; p < NC; ++p) {
+      const int j = k + 1 + lc + 8 * p;
+      u[p] = j < N ? a[k * RS + j] : 0.0;
+    }
+    __syncwarp();
+    for (int i = k + 1 + lr; i < N; i += 4) {
+      const double l = a[i * RS + k];
+#pragma unroll
+      for (int p = 0; p < NC; ++p) {
+        const int j = k + 1 + lc + 8 * p;
+        if (j < N) a[i * RS + j] = fma(-l, u[p], a[i * RS + j]);
+      }
+    }
+    __syncwarp();
+  }
+  return sing;
+}
+
 // After lu_warp: the composed permutation ((P b)[i] = b[perm[i]]) and the reciprocals of the
 // pivots, so that a solve runs in registers.
 __device__ __forceinline__ void lu_finish(const double* a, const int n, const int rs, const int* piv, int* perm,
@@ -666,7 +741,7 @@ template <class LY>
 static __device__ __noinline__ int lu_call(double* wb, const int lane) {
   using T = SvT<LY>;
   const WarpMem w = warp_mem<LY>(wb);
-  const int sing = lu_warp(w.mat, T::NV, T::RS, w.piv, lane);
+  const int sing = lu_warp_t<T::NV, T::RS>(w.mat, w.piv, lane);
   lu_finish(w.mat, T::NV, T::RS, w.piv, w.perm, w.cb, lane);
   return sing;
 }
