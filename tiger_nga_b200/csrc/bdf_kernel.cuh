@@ -17,8 +17,9 @@ struct BdfLaunch {
   int cold_in_smem;     // the Jacobian's term lists staged in shared memory (after the hot tables)
 };
 
-// two-entry-per-lane vector helpers
-__device__ __forceinline__ double wrms2(const double v0, const double v1, const double w0, const double w1,
+// two-entry-per-lane vector helpers (the weighted RMS norm out of line: it is evaluated at six
+// places of the step and each inlined copy carried its own square root and division)
+static __device__ __noinline__ double wrms2(const double v0, const double v1, const double w0, const double w1,
                                         const int nv, const int lane) {
   const double a = lane < nv ? v0 * w0 : 0.0;
   const double b = lane + 32 < nv ? v1 * w1 : 0.0;
@@ -89,6 +90,45 @@ __device__ __forceinline__ void zset(double (&z)[kQmax + 2][2], const int j, con
     if (k == j) z[k][h] = v;
 }
 
+// Initial step size from an estimate of ||y''|| at the cell's initial state u (f = rhs(u), ew the
+// error weights), at most dt. One out-of-line copy: it runs once per cell, and inlined (its loop
+// unrolled) it made up a tenth of the solver's code.
+template <class LY>
+static __device__ __noinline__ double bdf_initial_step(const SvT<LY> t, double* wb, const double u0, const double u1,
+                                                       const double f0, const double f1, const double ew0,
+                                                       const double ew1, const double dt, const double atol,
+                                                       const double p, const int lane) {
+  constexpr int nv = SvT<LY>::NV;
+  const bool h0 = lane < nv, h1 = lane + 32 < nv;
+  const double hlb = 100.0 * 2.220446049250313e-16 * dt;
+  double hub = 0.1 * dt;
+  double r = 0.0;
+  if (h0) r = fabs(f0) / (0.1 * fabs(u0) + atol);
+  if (h1) r = fmax(r, fabs(f1) / (0.1 * fabs(u1) + atol));
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(kFull, r, off));
+  if (hub * r > 1.0) hub = 1.0 / r;
+  double hg = sqrt(hlb * hub), hnew = hg;
+  if (hub < hlb) {
+    hnew = hlb;
+  } else {
+#pragma unroll 1
+    for (int it = 0; it < 4; ++it) {
+      const double2 gg = rhs_call(t, wb, u0 + hg * f0, u1 + hg * f1, p, lane);
+      const double ydd = wrms2((gg.x - f0) / hg, (gg.y - f1) / hg, ew0, ew1, nv, lane);
+      hnew = (ydd * hub * hub > 2.0) ? sqrt(2.0 / ydd) : sqrt(hg * hub);
+      if (!isfinite(hnew)) hnew = hg;
+      const double hrat = hnew / hg;
+      if (it == 3 || (hrat > 0.5 && hrat < 2.0)) break;
+      hg = hnew;
+    }
+    hnew *= 0.5;
+    if (hnew < hlb) hnew = hlb;
+    if (hnew > hub) hnew = hub;
+  }
+  return hnew < dt ? hnew : dt;
+}
+
 // Integrate one cell (warp-cooperative). Returns true when the cell is finished (any status),
 // false when it used up the pass budget and was saved for the next pass.
 template <class LY>
@@ -139,36 +179,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
       status = ST_NONFINITE;
       goto finish;
     }
-    // initial step from an estimate of ||y''||
-    {
-      const double hlb = 100.0 * 2.220446049250313e-16 * dt;
-      double hub = 0.1 * dt;
-      double r = 0.0;
-      if (h0) r = fabs(f[0]) / (0.1 * fabs(u0) + atol);
-      if (h1) r = fmax(r, fabs(f[1]) / (0.1 * fabs(u1) + atol));
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(kFull, r, off));
-      if (hub * r > 1.0) hub = 1.0 / r;
-      double hg = sqrt(hlb * hub), hnew = hg;
-      if (hub < hlb) {
-        hnew = hlb;
-      } else {
-        for (int it = 0; it < 4; ++it) {
-          const double2 gg = rhs_call(t, w.mat, u0 + hg * f[0], u1 + hg * f[1], p, lane);
-          const double g0 = gg.x, g1 = gg.y;
-          const double ydd = wrms2((g0 - f[0]) / hg, (g1 - f[1]) / hg, ewt[0], ewt[1], nv, lane);
-          hnew = (ydd * hub * hub > 2.0) ? sqrt(2.0 / ydd) : sqrt(hg * hub);
-          if (!isfinite(hnew)) hnew = hg;
-          const double hrat = hnew / hg;
-          if (it == 3 || (hrat > 0.5 && hrat < 2.0)) break;
-          hg = hnew;
-        }
-        hnew *= 0.5;
-        if (hnew < hlb) hnew = hlb;
-        if (hnew > hub) hnew = hub;
-      }
-      h = hnew < dt ? hnew : dt;
-    }
+    h = bdf_initial_step<LY>(t, w.mat, u0, u1, f[0], f[1], ewt[0], ewt[1], dt, atol, p, lane);
     z[1][0] = h * f[0];
     z[1][1] = h * f[1];
     hprev = h;
@@ -250,6 +261,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
           y[0] = z[0][0];
           y[1] = z[0][1];
           conv_fail = true;
+#pragma unroll 1
           for (int it = 0; it < maxcor; ++it) {
             {
               const double2 r = rhs_call(t, w.mat, y[0], y[1], p, lane);

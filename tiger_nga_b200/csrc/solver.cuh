@@ -190,17 +190,27 @@ __device__ __forceinline__ double expo(const double lnA, const double E, const d
 
 __device__ __forceinline__ int nu_of(const int term) { return (int)(int8_t)(term & 0xFF); }
 
-// exp of a rate-constant exponent in the handle's precision: FP64, or in mixed precision 2^x
-// split into an exact power of two (FP64 scaling) and a fraction in [0, 1) evaluated by the FP32
-// ex2 unit, relative error about 3e-7. The exponent itself (ln A + n ln T - E/RT, where the
-// reverse rates' cancellations sit) is always formed in FP64.
-template <class LY>
-__device__ __forceinline__ double rexp(const SvT<LY>& t, const double e) {
-  if (!t.mixed) return exp(e);
+// One out-of-line copy of each transcendental the solver evaluates: inlined at every call site,
+// the FP64 exp / log sequences made up a third of the right-hand side's code, and the solver's
+// warps stalled on instruction fetch.
+static __device__ __noinline__ double exp_ool(const double x) { return exp(x); }
+static __device__ __noinline__ double log_ool(const double x) { return log(x); }
+
+// exp in mixed precision: 2^x split into an exact power of two (FP64 scaling) and a fraction in
+// [0, 1) evaluated by the FP32 ex2 unit, relative error about 3e-7.
+static __device__ __noinline__ double exp_mixed_ool(const double e) {
   const double x = e * 1.4426950408889634;
   const double n = floor(x);
   if (!(n > -1100.0)) return 0.0;
   return ldexp((double)tng_ex2f((float)(x - n)), (int)fmin(n, 1100.0));
+}
+
+// exp of a rate-constant exponent in the handle's precision (FP64, or the mixed form above). The
+// exponent itself (ln A + n ln T - E/RT, where the reverse rates' cancellations sit) is always
+// formed in FP64.
+template <class LY>
+__device__ __forceinline__ double rexp(const SvT<LY>& t, const double e) {
+  return t.mixed ? exp_mixed_ool(e) : exp_ool(e);
 }
 
 // Per-cell thermochemical state shared by the rate and Jacobian evaluations.
@@ -223,20 +233,20 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
   __syncwarp();
   c.irho = 1.0 / c.rho;
   c.T = w.vb[ns] / c.rho;  // by division, as the reference (the T > 1000 range switch is strict)
-  c.LT = log(c.T);
+  c.LT = log_ool(c.T);
   c.invRT = 1.0 / (sc[SC_RGAS] * c.T);
   c.invT = sc[SC_RGAS] * c.invRT;
   if (lane < ns) w.C[lane] = y0 * invw[lane];
   if (lane + 32 < ns) w.C[lane + 32] = y1 * invw[lane + 32];
   __syncwarp();
-  const double lnprt = log(p * c.invRT);
+  const double prt = p * c.invRT;  // [M] of the ideal gas, for a third-body sum that is zero
   const double* eff = t.d(HD_EFF);
   for (int m = lane; m < nm; m += 32) {
     const double* e = eff + m * ns;
     double acc = 0.0;
     for (int j = 0; j < ns; ++j) acc = fma(e[j], w.C[j], acc);
     w.Ms[m] = acc;
-    w.lcm[m] = acc > 0.0 ? log(acc) : lnprt;
+    w.lcm[m] = log_ool(acc > 0.0 ? acc : prt);
   }
   const int* fcf = t.i(HI_FC);
   const double* fcd = t.d(HD_FC);
@@ -248,10 +258,10 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
       const int form = (forms >> (4 * q)) & 15;
       if (form == 15) break;
       const double a = fcd[6 * f + 2 * q], cc = fcd[6 * f + 2 * q + 1];
-      const double term = form == 2 ? a : (form == 0 ? a * exp(-c.T * cc) : a * exp(-cc * c.invT));
+      const double term = form == 2 ? a : a * exp_ool(form == 0 ? -c.T * cc : -cc * c.invT);
       v = q == 0 ? term : v + term;
     }
-    const double lfc = log(v);
+    const double lfc = log_ool(v);
     const double l10 = lfc * sc[SC_INVLN10];
     w.fc[3 * f] = lfc;
     w.fc[3 * f + 1] = sc[SC_TN0] - sc[SC_TN1] * l10;
@@ -506,10 +516,13 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
     const int* gm = t.c(CI_G_M);
     const double* eff = t.d(HD_EFF);
     // the pairs are sorted by row: each row's contributions are summed in a register and added
-    // to the matrix once (no read-modify-write chain through shared memory per pair)
+    // to the matrix once (no read-modify-write chain through shared memory per pair); the loops
+    // stay rolled (fully unrolled over the pairs they were a sixth of the solver's code)
+#pragma unroll 1
     for (int j = lane; j < ns; j += 32) {
       int cur = gi[0];
       double acc = 0.0;
+#pragma unroll 4
       for (int g = 0; g < ng; ++g) {
         const int row = gi[g];
         if (row != cur) {
