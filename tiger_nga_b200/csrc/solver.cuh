@@ -271,31 +271,28 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
   return c;
 }
 
-// Rate constant of the slot at position p (GETLINDRATECOEFF-equivalent for falloff slots);
-// also returns ln Pr for falloff slots.
+// Rate constant of a falloff slot from its falloff word w1 (GETLINDRATECOEFF-equivalent:
+// Lindemann, or Troe in log form); also returns ln Pr.
 template <class LY>
-__device__ __forceinline__ double rate_const(const SvT<LY>& t, const WarpMem& w, const CellPrep& c, const int p,
-                                            const int w0, const int w1, double* lpr_out) {
-  const int fl = w0 & 15;
-  if (fl & 1) {
-    const int f = w1 >> 8;
-    const double* par = t.d(HD_FO) + 6 * f;
-    const int fw = t.i(HI_FO)[f];
-    const double* sc = t.d(HD_SCAL);
-    const double lk0 = expo(par[0], par[1], par[2], fw & 15, c.LT, c.invRT);
-    const double lki = expo(par[3], par[4], par[5], (fw >> 4) & 15, c.LT, c.invRT);
-    const double lpr = lk0 + w.lcm[fw >> 16] - fmax(lki, sc[SC_LNKMIN]);
-    if (lpr_out) *lpr_out = lpr;
-    const double pr = rexp(t, lpr);
-    const int fid = ((fw >> 8) & 255) - 1;
-    if (fid < 0) return rexp(t, lki) * pr / (1.0 + pr);
+__device__ __forceinline__ double falloff_const(const SvT<LY>& t, const WarpMem& w, const CellPrep& c, const int w1,
+                                               double* lpr_out) {
+  const int f = w1 >> 8;
+  const double* par = t.d(HD_FO) + 6 * f;
+  const int fw = t.i(HI_FO)[f];
+  const double* sc = t.d(HD_SCAL);
+  const double lk0 = expo(par[0], par[1], par[2], fw & 15, c.LT, c.invRT);
+  const double lki = expo(par[3], par[4], par[5], (fw >> 4) & 15, c.LT, c.invRT);
+  const double lpr = lk0 + w.lcm[fw >> 16] - fmax(lki, sc[SC_LNKMIN]);
+  *lpr_out = lpr;
+  const double pr = rexp(t, lpr);
+  const int fid = ((fw >> 8) & 255) - 1;
+  double lk = lki;  // Lindemann: k_inf Pr / (1 + Pr)
+  if (fid >= 0) {   // Troe: k_inf F Pr / (1 + Pr), ln F = ln Fc / (1 + f^2)
     const double lg = lpr * sc[SC_INVLN10] + w.fc[3 * fid + 2];
     const double ff = lg / (w.fc[3 * fid + 1] - sc[SC_TD] * lg);
-    return rexp(t, lki + w.fc[3 * fid] / (ff * ff + 1.0)) * pr / (1.0 + pr);
+    lk = lki + w.fc[3 * fid] / (ff * ff + 1.0);
   }
-  const double* sd = t.d(HD_SLOT) + 4 * p;
-  if (fl & 8) return sd[0];
-  return rexp(t, expo(sd[0], sd[1], sd[2], fl, c.LT, c.invRT));
+  return rexp(t, lk) * pr / (1.0 + pr);
 }
 
 // Rate constant of a plain (Arrhenius or constant) slot without branches: the table holds
@@ -329,11 +326,14 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
     return v;
   };
   // the falloff slots (processing positions 0 .. NFO-1), then the plain and constant slots in a
-  // loop without divergent paths, whose independent exponentials the compiler interleaves
+  // loop without divergent paths. The loops here and in the rest of the right-hand side and
+  // the Jacobian stay rolled: with eight warps per SM the solver is bound by instruction supply,
+  // and every unrolled copy measured slower than the rolled loop (the latency it hides for one
+  // warp is hidden by the other warps)
   for (int q = lane; q < SvT<LY>::NFO; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
     double lpr = 0.0;
-    const double k = rate_const(t, w, c, q, w0, w1, &lpr);
+    const double k = falloff_const(t, w, c, w1, &lpr);
     if (products) {
       w.W[q] = mass_action(k, w0, w1);
     } else {
@@ -341,7 +341,7 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
       w.lpr[q] = lpr;
     }
   }
-#pragma unroll 2
+#pragma unroll 1
   for (int q = SvT<LY>::NFO + lane; q < SvT<LY>::NSLOT; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
     const double k = plain_const(t, c, q, w0);
@@ -376,7 +376,7 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
     const double* __restrict__ Wr = w.W;
     double* __restrict__ part = w.part;
     double acc = 0.0;
-#pragma unroll 2
+#pragma unroll 1
     for (int st = 0; st < SvT<LY>::NCDSTEP; ++st) {
       const int term = ct[32 * st];
       const double wv = Wr[(term >> 8) & 4095];
@@ -394,7 +394,7 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
   const int toff = c.T > sc[SC_TMID] ? 0 : 12;
   const double* th = t.d(HD_TH);
   double cpm = 0.0, tmp = 0.0, r0 = 0.0, r1 = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     const int k = lane + 32 * half;
     if (k < ns) {
@@ -442,7 +442,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   prep_rates<LY>(t, w.mat, y0, y1, p, lane, 0);
   const CellPrep c = load_prep(w);
   const int* sw = t.i(HI_SLOT);
-#pragma unroll 4
+#pragma unroll 1
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
   // direct mass-action part: nu dW_p/dC_j for every reactant occurrence, the terms of one matrix
@@ -457,7 +457,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
     const double* __restrict__ Mr = w.Ms;
     double* __restrict__ mat = w.mat;
     double acc = 0.0;
-#pragma unroll 2
+#pragma unroll 1
     for (int st = 0; st < SvT<LY>::NJDSTEP; ++st) {
       const int2 tm = jt[32 * st];
       const int pa = tm.x & 1023, ra = (tm.x >> 10) & 127, rb = (tm.x >> 17) & 127, mw = (tm.x >> 24) & 127;
@@ -550,7 +550,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   // species columns
   const double* wm = t.d(HD_WMOL);
   const double* iw = t.d(HD_INVW);
-#pragma unroll 2
+#pragma unroll 1
   for (int e = lane; e < ns * ns; e += 32) {
     const int i = e / ns, j = e % ns;
     w.mat[i * rs + j] = w.mat[i * rs + j] * (wm[i] * iw[j]) - T * w.mat[i * rs + ns];
@@ -560,7 +560,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   const int toff = T > sc[SC_TMID] ? 0 : 12;
   const double* th = t.d(HD_TH);
   double cpm = 0.0, ydcp = 0.0, scp = 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     const int k = lane + 32 * half;
     if (k < ns) {
@@ -585,7 +585,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   for (int j = lane; j < ns; j += 32) {
     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four independent chains
     int k = 0;
-#pragma unroll
+#pragma unroll 1
     for (; k + 3 < ns; k += 4) {
       s0 = fma(w.hb[k], w.mat[k * rs + j], s0);
       s1 = fma(w.hb[k + 1], w.mat[(k + 1) * rs + j], s1);
@@ -770,13 +770,13 @@ __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const
   double b0 = i0 < n ? vb[perm[i0]] : 0.0;
   double b1 = i1 < n ? vb[perm[i1]] : 0.0;
   __syncwarp();
-#pragma unroll 2
+#pragma unroll 1
   for (int k = 0; k < n - 1; ++k) {
     const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31);
     if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
     if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
-#pragma unroll 2
+#pragma unroll 1
   for (int k = n - 1; k >= 0; --k) {
     const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31) * dinv[k];
     if (i0 == k) b0 = bk;
