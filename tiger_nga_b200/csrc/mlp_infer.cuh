@@ -1,21 +1,27 @@
 // K4: surrogate inference on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
 // One launch evaluates every network of the surrogate (the ensemble members and the error gate)
-// on the same cells. Persistent CTAs (two per SM) walk tiles of 128 cells. For each tile:
-//   1. features: the 256 threads split each cell's species between two threads, issue all their
-//      FP64 state loads at once (one memory latency per tile, not one per species), form the
-//      density, temperature and the normalised inputs, and keep them packed as BF16 in registers;
-//   2. for each network, the features are written into shared memory (UMMA canonical K-major
-//      layout, 8-row x 16-byte core matrices) and every layer is D[128 x N] = H[128 x K] * W^T on
-//      tcgen05.mma (kind::f16, BF16 operands, FP32 accumulator in tensor memory); one elected
-//      thread issues the MMAs, weights stream from global memory (L2-resident, shared by all
-//      CTAs) into a two-stage shared-memory ring with cp.async.bulk + mbarrier transaction
-//      counts, and the next layer's (next network's, next tile's) first chunk is fetched while the
-//      epilogue runs; tcgen05.commit releases ring stages;
-//   3. the epilogue (8 warps, two per tensor-memory lane quarter) reads D with tcgen05.ld, adds
-//      the bias, applies GELU and writes the next layer's BF16 operand back into shared memory;
-//      the last layer's FP32 outputs go to the network's output array.
-// Every wait is bounded: on expiry the CTA records an error code and stops issuing work.
+// on the same cells. Persistent CTAs (two per SM) walk tiles of 128 cells; every layer of every
+// network is one step D[128 x N] = H[128 x K] * W^T on tcgen05.mma (kind::f16, BF16 operands,
+// FP32 accumulator in tensor memory, A in shared memory in the UMMA canonical K-major layout of
+// 8-row x 16-byte core matrices). The warps of a CTA have three roles:
+//   * the weight producer (one warp, one lane) streams the weights of every step, in step order,
+//     from global memory (L2-resident, shared by all CTAs) through a three-stage shared-memory
+//     ring of 32-wide K chunks with cp.async.bulk and mbarrier transaction counts; it runs up to
+//     three chunks ahead of the tensor core, across layers, networks and tiles;
+//   * the MMA issuer (one warp, one lane) waits for a step's A operand, then for each chunk, issues
+//     its MMAs, releases the chunk's stage with tcgen05.commit, and after the last chunk commits
+//     the accumulator to the epilogue;
+//   * eight feature/epilogue warps: per tile they form the features (the two threads of a cell,
+//     lanes 2r and 2r+1 of one warp, split its species, issue all their FP64 state loads at once
+//     and combine the density by a shuffle) and keep them packed as BF16 in registers; per step
+//     they read D with tcgen05.ld (two warps per tensor-memory lane quarter), add the bias, apply
+//     GELU and write the next step's A operand (or write the last layer's FP32 outputs and then
+//     the next network's or tile's features), and signal the MMA issuer.
+// So the tensor core never waits for a weight copy that the producer could have issued earlier,
+// and with two CTAs per SM one CTA's epilogue overlaps the other's MMAs. Every wait is bounded:
+// on expiry the waiting role records an error in shared memory, every role stops at its next
+// wait, the issued copies and MMAs drain, and the CTA reports the error.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -24,9 +30,10 @@
 namespace tng {
 
 constexpr int kInferRows = 128;
-constexpr int kInferThreads = 256;  // 8 warps: two per TMEM lane quarter
+constexpr int kEpiThreads = 256;                 // 8 feature/epilogue warps: two per TMEM lane quarter
+constexpr int kInferThreads = kEpiThreads + 64;  // + the weight producer warp and the MMA warp
 constexpr int kWChunkK = 32;   // K width of one streamed weight chunk (two MMAs)
-constexpr int kWStages = 2;    // weight stages: one chunk in flight ahead of the MMA
+constexpr int kWStages = 3;    // weight stages of the ring
 constexpr int kMaxLayers = 9;
 constexpr int kMaxNets = 5;    // ensemble members and the error gate
 constexpr int kFeatSpecies = 24;  // species per feature thread (two threads per cell): ns <= 48
@@ -114,8 +121,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 
 constexpr int kWaitPolls = 1 << 24;
 
-// bounded parity wait; returns false after `limit` unsuccessful polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int limit = kWaitPolls) {
+// bounded parity wait; returns false after `limit` unsuccessful polls, or (with a flag) as soon
+// as another role has recorded an error
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int limit = kWaitPolls,
+                                          const volatile int* stop = nullptr) {
   const uint32_t a = smem_u32(bar);
   for (int it = 0; it < limit; ++it) {
     uint32_t ok;
@@ -127,8 +136,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int lim
         : "r"(a), "r"(phase)
         : "memory");
     if (ok) return true;
+    if (stop && (it & 63) == 63 && *stop) return false;
   }
   return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
@@ -175,9 +189,9 @@ __device__ __forceinline__ float gelu_fast(float x) {
   return 0.5f * x * (1.0f + t);
 }
 
-// shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), two weight stages of
-// 256 x 32 bf16 (16 KB each), barriers and the TMEM address: 96 KB, two CTAs per SM (their
-// phases -- features, MMA, epilogue -- overlap), 2 x 256 TMEM columns.
+// shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), three weight stages of
+// 256 x 32 bf16 (16 KB each), barriers, the TMEM address and the error flag: 112.1 KB; two CTAs
+// per SM (with the per-block reserve, 226 KB of the SM's 228 KB), 2 x 256 TMEM columns.
 constexpr int kSmemA = kInferRows * 256 * 2;
 constexpr int kSmemStage = 256 * kWChunkK * 2;
 constexpr int kInferSmem = kSmemA + kWStages * kSmemStage + 128;
@@ -191,18 +205,29 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   uint8_t* sA = sm;
   uint8_t* sW = sm + kSmemA;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + kSmemA + kWStages * kSmemStage);
-  // bars[0..S): stage full, bars[S..2S): stage free, bars[2S]: layer done
+  // bars[0..S): stage full; [S..2S): stage free; [2S]: accumulator full (MMA -> epilogue);
+  // [2S+1]: A operand written and accumulator drained (epilogue -> MMA); [2S+2]: MMA drain
   uint64_t* bar_full = bars;
   uint64_t* bar_free = bars + kWStages;
-  uint64_t* bar_done = bars + 2 * kWStages;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kWStages + 1);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  __shared__ double s_part[2][kInferRows];  // the two halves of each cell's density
+  uint64_t* bar_acc = bars + 2 * kWStages;
+  uint64_t* bar_ain = bars + 2 * kWStages + 1;
+  uint64_t* bar_drain = bars + 2 * kWStages + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kWStages + 3);
+  volatile int* s_err = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int kProdWarp = kEpiThreads / 32, kMmaWarp = kProdWarp + 1;
   if (tid == 0) {
-    for (int i = 0; i < 2 * kWStages + 1; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < kWStages; ++i) {
+      mbar_init(&bar_full[i], 1);
+      mbar_init(&bar_free[i], 1);
+    }
+    mbar_init(bar_acc, 1);
+    mbar_init(bar_ain, kEpiThreads);
+    mbar_init(bar_drain, 1);
+    *s_err = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(tmem_slot)));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
@@ -211,61 +236,97 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const int wlim = a.wait_limit > 0 ? a.wait_limit : kWaitPolls;
-  // thread 0 only: parities, pending commits and copies per stage; chunks issued so far (stage =
-  // gc % kWStages); chunks of the coming layer already issued (pre) from gc = pre_base
-  uint32_t ph_full[kWStages] = {}, ph_free[kWStages] = {}, ph_done = 0;
-  int stage_busy[kWStages] = {}, inflight[kWStages] = {};
-  int gc = 0, pre = 0, pre_base = 0;
-  int err = 0;
-  // issue the bulk copy of weight chunk c of layer l of network ni into the next stage (thread 0)
-  auto issue = [&](int ni, int l, int c) {
-    const int K = l == 0 ? a.in_pad : a.hidden;
-    const int N = l == a.nlin - 1 ? a.net[ni].out_pad : a.hidden;
-    const int s = gc % kWStages;
-    ++gc;
-    if (stage_busy[s]) {  // wait for the MMA that read this stage
-      if (!mbar_wait(&bar_free[s], ph_free[s], wlim)) err = 1;
-      ph_free[s] ^= 1;
-      stage_busy[s] = 0;
-    }
-    const int kc = min(kWChunkK, K - c * kWChunkK);
-    const uint32_t bytes = (uint32_t)N * kc * 2;
-    mbar_expect_tx(&bar_full[s], bytes);
-    bulk_g2s(sW + s * kSmemStage, a.net[ni].wpack + a.net[ni].w_off[l] + (long long)c * N * kWChunkK, bytes,
-             &bar_full[s]);
-    inflight[s] = 1;
-  };
-  // this thread's share of a cell's inputs, normalised, kept as BF16 for every network: species
-  // k0 + j (j < kn) as (log10 Y, Y) pairs; thread part 0 also holds T, log P and log10 dt
-  const int row = tid & (kInferRows - 1), part = tid >> 7;
-  const int half = (a.ns + 1) >> 1, k0 = part * half, kn = min(half, a.ns - k0);
-  __nv_bfloat162 fsp[kFeatSpecies];
-  __nv_bfloat162 fx0 = __floats2bfloat162_rn(0.f, 0.f), fx1 = fx0;
-  // column of species k's log feature (k != bath); its linear feature is ns columns further
-  auto log_col = [&](int k) { return 2 + (k < a.bath ? k : k - 1); };
-  // the packed inputs into A (layer 0's operand, K = in_pad), zero padding included
-  auto write_inputs = [&]() {
-    const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
-#pragma unroll
-    for (int j = 0; j < kFeatSpecies; ++j) {
-      const int k = k0 + j;
-      if (j < kn && k != a.bath) {
-        st_bf16(sA, row, log_col(k), a.in_pad, __low2bfloat16(fsp[j]));
-        st_bf16(sA, row, log_col(k) + a.ns, a.in_pad, __high2bfloat16(fsp[j]));
+  const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
+  auto k_of = [&](int l) { return l == 0 ? a.in_pad : a.hidden; };
+  auto n_of = [&](int ni, int l) { return l == a.nlin - 1 ? a.net[ni].out_pad : a.hidden; };
+
+  if (warp == kProdWarp) {
+    // ---- weight producer: every chunk of every step, in step order, into the ring
+    if (lane == 0) {
+      int gc = 0;
+      bool bad = false;
+      for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x)
+        for (int ni = 0; ni < a.nnets && !bad; ++ni)
+          for (int l = 0; l < a.nlin && !bad; ++l) {
+            const int K = k_of(l), N = n_of(ni, l);
+            for (int c = 0; c * kWChunkK < K; ++c, ++gc) {
+              const int s = gc % kWStages;
+              const uint32_t use = (uint32_t)(gc / kWStages);
+              // the stage's previous chunk must have been consumed by its MMAs
+              if (use > 0 && !mbar_wait(&bar_free[s], (use - 1) & 1, wlim, s_err)) {
+                bad = true;
+                break;
+              }
+              const int kc = min(kWChunkK, K - c * kWChunkK);
+              const uint32_t bytes = (uint32_t)N * kc * 2;
+              mbar_expect_tx(&bar_full[s], bytes);
+              bulk_g2s(sW + s * kSmemStage, a.net[ni].wpack + a.net[ni].w_off[l] + (long long)c * N * kWChunkK, bytes,
+                       &bar_full[s]);
+            }
+          }
+      if (bad) *s_err = 1;
+      // drain: every issued copy lands before the CTA exits (the last use of each stage)
+      for (int s = 0; s < kWStages && s < gc; ++s) {
+        const int last = gc - 1 - ((gc - 1 - s) % kWStages);
+        if (!mbar_wait(&bar_full[s], (uint32_t)(last / kWStages) & 1)) *s_err = 1;
       }
     }
-    if (part == 0) {
-      st_bf16(sA, row, 0, a.in_pad, __low2bfloat16(fx0));
-      st_bf16(sA, row, 1, a.in_pad, __high2bfloat16(fx0));
-      st_bf16(sA, row, a.ns + 1, a.in_pad, __low2bfloat16(fx1));
-    } else {
-      for (int i = a.n_in; i < a.in_pad; ++i) st_bf16(sA, row, i, a.in_pad, z);
+    __syncwarp();
+  } else if (warp == kMmaWarp) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      int gc = 0, step = 0;
+      bool bad = false;
+      const uint32_t abase = smem_u32(sA);
+      for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x)
+        for (int ni = 0; ni < a.nnets && !bad; ++ni)
+          for (int l = 0; l < a.nlin && !bad; ++l, ++step) {
+            const int K = k_of(l), N = n_of(ni, l);
+            // the step's A operand is written and the accumulator has been read out
+            if (!mbar_wait(bar_ain, (uint32_t)step & 1, wlim, s_err)) {
+              bad = true;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t idesc = umma_idesc(kInferRows, N);
+            const uint32_t a_sbo = (uint32_t)K * 16;
+            for (int c = 0; c * kWChunkK < K; ++c, ++gc) {
+              const int s = gc % kWStages;
+              if (!mbar_wait(&bar_full[s], (uint32_t)(gc / kWStages) & 1, wlim, s_err)) {
+                bad = true;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              const int kc = min(kWChunkK, K - c * kWChunkK);
+              const uint32_t wbase = smem_u32(sW + s * kSmemStage);
+              for (int kk = 0; kk < kc; kk += 16) {
+                const int kg = c * kWChunkK + kk;
+                const uint64_t ad = umma_desc(abase + (uint32_t)(kg >> 3) * 128, 128, a_sbo);
+                const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
+                umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+              }
+              umma_commit(&bar_free[s]);
+            }
+            // test hook: the first step's completion signal withheld (its MMAs run and drain)
+            if (!bad && !(a.fault == 1 && step == 0)) umma_commit(bar_acc);
+          }
+      if (bad) *s_err = 1;
+      // drain: every issued MMA completes before the tensor memory is freed
+      umma_commit(bar_drain);
+      if (!mbar_wait(bar_drain, 0)) *s_err = 1;
     }
-  };
-  const int ntiles = (a.ncells + kInferRows - 1) / kInferRows;
-  for (int tile = blockIdx.x; tile < ntiles && !err; tile += gridDim.x) {
-    // ---- 1. features of the tile's cells (once for all networks)
-    {
+    __syncwarp();
+  } else {
+    // ---- features and epilogue: the two threads of a cell are lanes 2r and 2r + 1 of one warp
+    const int row = tid >> 1, part = tid & 1;
+    const int half = (a.ns + 1) >> 1, k0 = part * half, kn = min(half, a.ns - k0);
+    __nv_bfloat162 fsp[kFeatSpecies];
+    __nv_bfloat162 fx0 = __floats2bfloat162_rn(0.f, 0.f), fx1 = fx0;
+    // column of species k's log feature (k != bath); its linear feature is ns columns further
+    auto log_col = [&](int k) { return 2 + (k < a.bath ? k : k - 1); };
+    // this thread's share of the tile's inputs, normalised, packed as BF16: species k0 + j as
+    // (log10 Y, Y) pairs; thread part 0 also holds T, log P and log10 dt
+    auto features = [&](int tile) {
       const int cell = tile * kInferRows + row;
       const bool live = cell < a.ncells;
       double x[kFeatSpecies];
@@ -276,9 +337,8 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
       double ps = 0.0;
 #pragma unroll
       for (int j = 0; j < kFeatSpecies; ++j) ps += x[j];
-      s_part[part][row] = ps;
-      __syncthreads();
-      const double rho = live ? s_part[0][row] + s_part[1][row] : 1.0;
+      const double other = __shfl_xor_sync(0xffffffffu, ps, 1);
+      const double rho = live ? (part == 0 ? ps + other : other + ps) : 1.0;
       const double irho = 1.0 / rho;
 #pragma unroll
       for (int j = 0; j < kFeatSpecies; ++j) {
@@ -293,145 +353,125 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
         }
         fsp[j] = __floats2bfloat162_rn(fl, fn);
       }
-      if (part == 0) {
-        float f0 = 0.f, f1 = 0.f, f2 = 0.f;
-        if (live) {
-          f0 = ((float)(xT / rho) - a.fmean[0]) * a.fistd[0];
-          f1 = ((float)a.logp - a.fmean[1]) * a.fistd[1];
-          f2 = ((float)log10(fmax(dt, 1e-30)) - a.fmean[a.ns + 1]) * a.fistd[a.ns + 1];
-        }
-        fx0 = __floats2bfloat162_rn(f0, f1);
-        fx1 = __floats2bfloat162_rn(f2, 0.f);
+      float f0 = 0.f, f1 = 0.f, f2 = 0.f;
+      if (live && part == 0) {
+        f0 = ((float)(xT / rho) - a.fmean[0]) * a.fistd[0];
+        f1 = ((float)a.logp - a.fmean[1]) * a.fistd[1];
+        f2 = ((float)log10(fmax(dt, 1e-30)) - a.fmean[a.ns + 1]) * a.fistd[a.ns + 1];
       }
-    }
-    // ---- 2./3. networks and their layers
-    for (int ni = 0; ni < a.nnets && !err; ++ni) {
-      const InferNet& net = a.net[ni];
-      write_inputs();
+      fx0 = __floats2bfloat162_rn(f0, f1);
+      fx1 = __floats2bfloat162_rn(f2, 0.f);
+    };
+    // the packed inputs into A (layer 0's operand, K = in_pad), zero padding included
+    auto write_inputs = [&]() {
+      const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
+#pragma unroll
+      for (int j = 0; j < kFeatSpecies; ++j) {
+        const int k = k0 + j;
+        if (j < kn && k != a.bath) {
+          st_bf16(sA, row, log_col(k), a.in_pad, __low2bfloat16(fsp[j]));
+          st_bf16(sA, row, log_col(k) + a.ns, a.in_pad, __high2bfloat16(fsp[j]));
+        }
+      }
+      if (part == 0) {
+        st_bf16(sA, row, 0, a.in_pad, __low2bfloat16(fx0));
+        st_bf16(sA, row, 1, a.in_pad, __high2bfloat16(fx0));
+        st_bf16(sA, row, a.ns + 1, a.in_pad, __low2bfloat16(fx1));
+      } else {
+        for (int i = a.n_in; i < a.in_pad; ++i) st_bf16(sA, row, i, a.in_pad, z);
+      }
+    };
+    // hand the A operand to the MMA issuer: the generic-proxy writes are made visible to the
+    // tensor core, and this thread's tensor-memory reads are ordered before the signal
+    auto signal_a = [&]() {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncthreads();
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int l = 0; l < a.nlin && !err; ++l) {
-        const int K = l == 0 ? a.in_pad : a.hidden;
-        const int N = l == a.nlin - 1 ? net.out_pad : a.hidden;
-        const int nchunk = (K + kWChunkK - 1) / kWChunkK;
-        if (tid == 0) {
-          const uint32_t idesc = umma_idesc(kInferRows, N);
-          const uint32_t a_sbo = (uint32_t)K * 16;
-          // chunk c sits in stage (base + c) % S; after chunk c's MMA is queued the copies of the
-          // chunks up to c + S - 1 are issued, so they load while the tensor core works
-          const int base = pre ? pre_base : gc;
-          int issued = pre;
-          pre = 0;
-          if (issued == 0) issue(ni, l, issued++);
-          for (int c = 0; c < nchunk && !err; ++c) {
-            const int s = (base + c) % kWStages;
-            const int kc = min(kWChunkK, K - c * kWChunkK);
-            if (!mbar_wait(&bar_full[s], ph_full[s], wlim)) err = 1;
-            ph_full[s] ^= 1;
-            inflight[s] = 0;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t wbase = smem_u32(sW + s * kSmemStage);
-            const uint32_t abase = smem_u32(sA);
-            for (int kk = 0; kk < kc; kk += 16) {
-              const int kg = c * kWChunkK + kk;
-              const uint64_t ad = umma_desc(abase + (uint32_t)(kg >> 3) * 128, 128, a_sbo);
-              const uint64_t bd = umma_desc(wbase + (uint32_t)(kk >> 3) * 128, 128, (uint32_t)kc * 16);
-              umma_bf16(tmem, ad, bd, idesc, (c > 0 || kk > 0) ? 1u : 0u);
+      mbar_arrive(bar_ain);
+    };
+    if (blockIdx.x < ntiles) {
+      features(blockIdx.x);
+      write_inputs();
+      signal_a();
+    }
+    const int erow = (warp & 3) * 32 + lane;
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    int step = 0;
+    bool bad = false;
+    for (int tile = blockIdx.x; tile < ntiles && !bad; tile += gridDim.x)
+      for (int ni = 0; ni < a.nnets && !bad; ++ni)
+        for (int l = 0; l < a.nlin && !bad; ++l, ++step) {
+          const InferNet& net = a.net[ni];
+          const int N = n_of(ni, l);
+          // one lane per warp polls the accumulator barrier, the warp follows
+          bool ok = true;
+          if (lane == 0) ok = mbar_wait(bar_acc, (uint32_t)step & 1, wlim, s_err);
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          if (!ok) {
+            bad = true;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
+          const float* bl = net.bias + net.b_off[l];
+          const bool last = l == a.nlin - 1;
+          const int cell = tile * kInferRows + erow;
+          for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 64) {
+            float v[32];
+            tmem_ld32(trow + (uint32_t)c0, v);
+            const int nc = min(32, N - c0);
+            if (last) {
+              if (cell < a.ncells) {
+                float* o = net.out + (long long)cell * net.out_pad + c0;
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                  if (i < nc) o[i] = v[i] + __ldg(bl + c0 + i);
+              }
+            } else {
+              const float4* b4 = reinterpret_cast<const float4*>(bl + c0);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const float4 ba = __ldg(b4 + 2 * q), bb = __ldg(b4 + 2 * q + 1);
+                const float bq[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
+                float xq[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) xq[i] = gelu_fast(v[q * 8 + i] + bq[i]);
+                __nv_bfloat162 p0 = __floats2bfloat162_rn(xq[0], xq[1]);
+                __nv_bfloat162 p1 = __floats2bfloat162_rn(xq[2], xq[3]);
+                __nv_bfloat162 p2 = __floats2bfloat162_rn(xq[4], xq[5]);
+                __nv_bfloat162 p3 = __floats2bfloat162_rn(xq[6], xq[7]);
+                uint4 u;
+                u.x = *reinterpret_cast<uint32_t*>(&p0);
+                u.y = *reinterpret_cast<uint32_t*>(&p1);
+                u.z = *reinterpret_cast<uint32_t*>(&p2);
+                u.w = *reinterpret_cast<uint32_t*>(&p3);
+                *reinterpret_cast<uint4*>(sA + canon_off(erow, c0 + q * 8, a.hidden)) = u;
+              }
             }
-            umma_commit(&bar_free[s]);
-            stage_busy[s] = 1;
-            while (issued < nchunk && issued < c + kWStages) issue(ni, l, issued++);
           }
-          if (!(a.fault == 1 && ni == 0 && l == 0 && tile == (int)blockIdx.x)) umma_commit(bar_done);
-        }
-        // epilogue: one lane per warp polls the layer barrier, the warp follows
-        bool ok = true;
-        if ((tid & 31) == 0) ok = mbar_wait(bar_done, ph_done, wlim);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        __syncwarp();
-        ph_done ^= 1;
-        if (!ok) err = 1;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // after a timed-out wait the layer's MMAs may still read the A operand: no epilogue
-        if (__syncthreads_or(err)) {
-          err = 1;
-          break;
-        }
-        // the next layer's (next network's, next tile's) first chunks load during the epilogue
-        if (tid == 0) {
-          int nn = ni, nl = l + 1;
-          if (nl == a.nlin) nl = 0, nn = ni + 1;
-          if (nn == a.nnets) nn = 0;
-          const bool more = l + 1 < a.nlin || ni + 1 < a.nnets || tile + (int)gridDim.x < ntiles;
-          if (more) {
-            const int nk = ((nl == 0 ? a.in_pad : a.hidden) + kWChunkK - 1) / kWChunkK;
-            pre_base = gc;
-            pre = min(nk, kWStages - 1);
-            for (int c = 0; c < pre; ++c) issue(nn, nl, c);
-          }
-        }
-        // warps w and w + 4 read the same TMEM lane quarter (rows), alternate 32-column groups
-        const float* bl = net.bias + net.b_off[l];
-        const int erow = (warp & 3) * 32 + (tid & 31);
-        const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-        const bool last = l == a.nlin - 1;
-        const int cell = tile * kInferRows + erow;
-        for (int c0 = (warp >> 2) * 32; c0 < N; c0 += 64) {
-          float v[32];
-          tmem_ld32(trow + (uint32_t)c0, v);
-          const int nc = min(32, N - c0);
+          // the next step's A operand: the next layer's input is written above; after a
+          // network's last layer (which writes only the outputs, so nothing else touches A) the
+          // next network's inputs, or the next tile's features. The MMA issuer starts the next
+          // step once all 256 threads have signalled, i.e. have also finished reading TMEM.
           if (last) {
-            if (cell < a.ncells) {
-              float* o = net.out + (long long)cell * net.out_pad + c0;
-              for (int i = 0; i < nc; ++i) o[i] = v[i] + __ldg(bl + c0 + i);
-            }
-          } else {
-            const float4* b4 = reinterpret_cast<const float4*>(bl + c0);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const float4 ba = __ldg(b4 + 2 * q), bb = __ldg(b4 + 2 * q + 1);
-              const float bq[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
-              float xq[8];
-#pragma unroll
-              for (int i = 0; i < 8; ++i) xq[i] = gelu_fast(v[q * 8 + i] + bq[i]);
-              __nv_bfloat162 p0 = __floats2bfloat162_rn(xq[0], xq[1]);
-              __nv_bfloat162 p1 = __floats2bfloat162_rn(xq[2], xq[3]);
-              __nv_bfloat162 p2 = __floats2bfloat162_rn(xq[4], xq[5]);
-              __nv_bfloat162 p3 = __floats2bfloat162_rn(xq[6], xq[7]);
-              uint4 u;
-              u.x = *reinterpret_cast<uint32_t*>(&p0);
-              u.y = *reinterpret_cast<uint32_t*>(&p1);
-              u.z = *reinterpret_cast<uint32_t*>(&p2);
-              u.w = *reinterpret_cast<uint32_t*>(&p3);
-              *reinterpret_cast<uint4*>(sA + canon_off(erow, c0 + q * 8, a.hidden)) = u;
+            if (ni + 1 < a.nnets) {
+              write_inputs();
+            } else if (tile + (int)gridDim.x < ntiles) {
+              features(tile + (int)gridDim.x);
+              write_inputs();
+            } else {
+              continue;  // the CTA's last step: nothing follows
             }
           }
+          signal_a();
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        err = __syncthreads_or(err);
-      }
-    }
+    if (bad) *s_err = 1;
   }
-  // drain: weight copies still in flight (after an error) and the last commits on the stage
-  // barriers must complete before the CTA exits; every wait is bounded
-  if (tid == 0) {
-    for (int s = 0; s < kWStages; ++s) {
-      if (inflight[s] && !mbar_wait(&bar_full[s], ph_full[s])) err = 1;
-      if (stage_busy[s]) {
-        if (!mbar_wait(&bar_free[s], ph_free[s])) err = 1;
-        ph_free[s] ^= 1;
-      }
-    }
-  }
-  if (err && tid == 0 && a.error) atomicExch(a.error, 1);
+  // all roles finished (after an error every role stops at its next wait and drains its own work)
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (tid == 0 && *s_err && a.error) atomicExch(a.error, 1);
+  if (warp == kMmaWarp) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem));
 }
 
 }  // namespace tng
