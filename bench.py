@@ -796,16 +796,22 @@ def main():
         extra["surrogate"]["fallback_fraction"] = 1.0 - stats_last["accepted"] / ncells
         extra["surrogate"]["weights"] = os.path.relpath(args.surrogate, REPO)
         # tensor roofline of the inference chain (reported beside the dominant solver kernel):
-        # algorithmic flops = 2 x (weights of the unpadded layers) per cell and ensemble member;
-        # ms_infer covers the inference of every member
-        alg = 2.0 * sur.weights_unpadded * sur.members
+        # algorithmic flops = 2 x (weights of the unpadded layers) per cell, summed over the
+        # networks of the launch (the ensemble members and the error gate, whose two outputs are
+        # the predicted errors); ms_infer covers the one launch that evaluates all of them
+        has_gate = sur.gate_info()[0]
+        H, nh = sur.cfg.hidden, sur.cfg.layers
+        gate_w = (sur.n_in * H + (nh - 1) * H * H + H * 2) if has_gate else 0
+        alg = 2.0 * (sur.weights_unpadded * sur.members + gate_w)
         t_inf = stats_last["ms_infer"] * 1e-3
         if t_inf > 0 and bf16_peak:
             ach = alg * ncells / t_inf / 1e12
             extra["inference_roofline"] = {"bound": "tensor", "achieved": ach, "peak": bf16_peak, "unit": "TFLOP/s",
                                            "frac": ach / bf16_peak, "peak_source": peak_src,
-                                           "kernel": "k_mlp_infer", "members": sur.members,
+                                           "kernel": "k_mlp_infer", "networks": sur.members + (1 if has_gate else 0),
+                                           "alg_flops_per_cell": alg,
                                            "alg_flops_per_cell_per_member": 2.0 * sur.weights_unpadded,
+                                           "alg_flops_per_cell_gate": 2.0 * gate_w,
                                            "executed_flops_per_cell_per_member": 2.0 * sur.weights_padded}
 
     # ---- e2e through the C-ABI with pinned host buffers -----------------------------------------

@@ -182,11 +182,43 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float gelu_fast(float x) {
-  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return 0.5f * x * (1.0f + t);
+// Packed FP32 pairs (sm_100 f32x2 instructions: one FMA / MUL / ADD for two values; each lane is
+// rounded as the scalar instruction would round it). Element 0 in the low 32 bits.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float x, float y) {
+  return (f32x2)__float_as_uint(x) | ((f32x2)__float_as_uint(y) << 32);
+}
+__device__ __forceinline__ float f2_lo(f32x2 v) { return __uint_as_float((unsigned)v); }
+__device__ __forceinline__ float f2_hi(f32x2 v) { return __uint_as_float((unsigned)(v >> 32)); }
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+
+// GELU in its tanh form, 0.5 x (1 + tanh(u)), u = sqrt(2/pi) (x + 0.044715 x^3), of two values:
+// u = x (c0 + c1 x^2) with c0 = sqrt(2/pi), c1 = 0.044715 sqrt(2/pi), and 0.5 x + 0.5 x tanh(u);
+// five packed instructions and two tanh.approx for the pair
+__device__ __forceinline__ f32x2 gelu2(f32x2 x) {
+  const f32x2 c0 = f2_pack(0.7978845608028654f, 0.7978845608028654f);
+  const f32x2 c1 = f2_pack(0.035677408136300125f, 0.035677408136300125f);
+  const f32x2 hf = f2_pack(0.5f, 0.5f);
+  const f32x2 u = f2_mul(x, f2_fma(f2_mul(x, x), c1, c0));
+  float t0, t1;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(f2_lo(u)));
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(f2_hi(u)));
+  const f32x2 h = f2_mul(x, hf);
+  return f2_fma(h, f2_pack(t0, t1), h);
 }
 
 // shared-memory plan (bytes): A operand (128 x 256 bf16 = 64 KB), three weight stages of
@@ -427,24 +459,20 @@ __global__ void __launch_bounds__(kInferThreads, 2) k_mlp_infer(const InferArgs 
                   if (i < nc) o[i] = v[i] + __ldg(bl + c0 + i);
               }
             } else {
+              // bias and GELU on pairs of columns (packed FP32), packed to BF16 pairs
               const float4* b4 = reinterpret_cast<const float4*>(bl + c0);
 #pragma unroll
               for (int q = 0; q < 4; ++q) {
                 const float4 ba = __ldg(b4 + 2 * q), bb = __ldg(b4 + 2 * q + 1);
-                const float bq[8] = {ba.x, ba.y, ba.z, ba.w, bb.x, bb.y, bb.z, bb.w};
-                float xq[8];
+                const f32x2 bp[4] = {f2_pack(ba.x, ba.y), f2_pack(ba.z, ba.w), f2_pack(bb.x, bb.y), f2_pack(bb.z, bb.w)};
+                uint32_t w[4];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) xq[i] = gelu_fast(v[q * 8 + i] + bq[i]);
-                __nv_bfloat162 p0 = __floats2bfloat162_rn(xq[0], xq[1]);
-                __nv_bfloat162 p1 = __floats2bfloat162_rn(xq[2], xq[3]);
-                __nv_bfloat162 p2 = __floats2bfloat162_rn(xq[4], xq[5]);
-                __nv_bfloat162 p3 = __floats2bfloat162_rn(xq[6], xq[7]);
-                uint4 u;
-                u.x = *reinterpret_cast<uint32_t*>(&p0);
-                u.y = *reinterpret_cast<uint32_t*>(&p1);
-                u.z = *reinterpret_cast<uint32_t*>(&p2);
-                u.w = *reinterpret_cast<uint32_t*>(&p3);
-                *reinterpret_cast<uint4*>(sA + canon_off(erow, c0 + q * 8, a.hidden)) = u;
+                for (int i = 0; i < 4; ++i) {
+                  const f32x2 g = gelu2(f2_add(f2_pack(v[q * 8 + 2 * i], v[q * 8 + 2 * i + 1]), bp[i]));
+                  const __nv_bfloat162 pb = __floats2bfloat162_rn(f2_lo(g), f2_hi(g));
+                  w[i] = *reinterpret_cast<const uint32_t*>(&pb);
+                }
+                *reinterpret_cast<uint4*>(sA + canon_off(erow, c0 + q * 8, a.hidden)) = make_uint4(w[0], w[1], w[2], w[3]);
               }
             }
           }
