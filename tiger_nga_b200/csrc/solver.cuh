@@ -602,64 +602,8 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   __syncwarp();
 }
 
-// In-place LU with partial pivoting (first maximum) of the n x n matrix a (row stride rs).
-// Returns nonzero if a pivot is zero or not finite.
-__device__ __forceinline__ int lu_warp(double* a, const int n, const int rs, int* piv, const int lane) {
-  int sing = 0;
-  const int lr = lane >> 3, lc = lane & 7;
-  // one copy of the pivot step: unrolled over the compile-time size the factorisation would
-  // not fit the instruction cache beside the rest of the solver
-#pragma unroll 1
-  for (int k = 0; k < n; ++k) {
-    double best = -1.0;
-    int bi = n;
-    for (int i = k + lane; i < n; i += 32) {
-      const double v = fabs(a[i * rs + k]);
-      if (v > best || (v == best && i < bi)) {
-        best = v;
-        bi = i;
-      }
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ob = __shfl_down_sync(kFull, best, off);
-      const int oi = __shfl_down_sync(kFull, bi, off);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
-      }
-    }
-    bi = __shfl_sync(kFull, bi, 0);
-    if (bi >= n) {  // the column holds only NaNs
-      bi = k;
-      sing = 1;
-    }
-    if (lane == 0) piv[k] = bi;
-    if (bi != k)
-      for (int j = lane; j < n; j += 32) {
-        const double tmp = a[k * rs + j];
-        a[k * rs + j] = a[bi * rs + j];
-        a[bi * rs + j] = tmp;
-      }
-    __syncwarp();
-    const double d = a[k * rs + k];
-    if (d == 0.0 || !isfinite(d)) {
-      sing = 1;
-      continue;
-    }
-    const double rd = 1.0 / d;
-    for (int i = k + 1 + lane; i < n; i += 32) a[i * rs + k] *= rd;
-    __syncwarp();
-    for (int i = k + 1 + lr; i < n; i += 4) {
-      const double l = a[i * rs + k];
-      for (int j = k + 1 + lc; j < n; j += 8) a[i * rs + j] = fma(-l, a[k * rs + j], a[i * rs + j]);
-    }
-    __syncwarp();
-  }
-  return sing;
-}
-
-// The same factorisation for a compile-time size N (row stride RS), as the solver runs it:
+// In-place LU with partial pivoting (first maximum) of the N x N matrix a (row stride RS), for
+// the compile-time size N, as the solver runs it:
 //  * the pivot is the exact first maximum of |a[i][k]|, found with three warp reductions on the
 //    64-bit pattern of |a| (a non-negative double orders like its bit pattern; NaN counts as 0)
 //    instead of five rounds of shuffles;
@@ -724,7 +668,7 @@ __device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const
   return sing;
 }
 
-// After lu_warp: the composed permutation ((P b)[i] = b[perm[i]]) and the reciprocals of the
+// After the factorisation: the composed permutation ((P b)[i] = b[perm[i]]) and the reciprocals of the
 // pivots, so that a solve runs in registers.
 __device__ __forceinline__ void lu_finish(const double* a, const int n, const int rs, const int* piv, int* perm,
                                           double* dinv, const int lane) {

@@ -68,6 +68,12 @@ __device__ __forceinline__ void nasa(const double* th, double tmid, int k, doubl
   *h = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
 }
 
+// the enthalpy alone (the same expression as nasa's h)
+__device__ __forceinline__ double nasa_h(const double* th, double tmid, int k, double T) {
+  const double* a = th + 24 * k + (T > tmid ? 0 : 12);
+  return a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
+}
+
 // raw features of one cell (same formulas as the inference kernel's featurisation)
 __device__ __forceinline__ int raw_features(const double* state, long long ld, int cell, int ns, int bath, double logp,
                                             double dt, float* f, double* rho_out, double* T_out) {
@@ -185,9 +191,7 @@ __device__ __forceinline__ void constraint_col(const SurPost& a, int k, double T
     if (e < a.nel) {
       c[e] = a.E[e * a.ns + k];
     } else {
-      double hk, cpk;
-      nasa(a.th, a.tmid, k, Th, &hk, &cpk);
-      c[e] = hk * hsc;
+      c[e] = nasa_h(a.th, a.tmid, k, Th) * hsc;
     }
   }
 }
@@ -379,9 +383,7 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
       sY = fmax(sY, hi - lo);
       D[k] = (float)(fabs(Y0[k]) + fabs(Y0[k] + dY[k]) + 1e-12);
       if (Y0[k] + dY[k] < 0.0) neg -= Y0[k] + dY[k];
-      double hk, cpk;
-      nasa(a.th, a.tmid, k, T0, &hk, &cpk);
-      h0 = fma(Y0[k], hk, h0);
+      h0 = fma(Y0[k], nasa_h(a.th, a.tmid, k, T0), h0);
     }
     // species the network drives below zero are pinned at zero before the first pass (the
     // projection would pin them one pass at a time otherwise)
