@@ -3,6 +3,9 @@
     python -m tiger_nga_b200.train_surrogate --mech grimech30 --pairs 8388608 \\
         --out tiger_nga_b200/models/grimech30.tngs
 
+With --gate-only MODEL the ensemble of a trained surrogate is kept and only its error gate is
+trained again (on --gate-pairs held-out pairs) and recalibrated, then saved to --out.
+
 Pairs (--dist uneven, the default): seeded states of the uneven-stiffness batch -- 128^3 grids
 of a smooth Fourier-mode mixture-fraction field (CH4 fuel / air at 300 K for GRI-Mech, DME at
 400 K for DME39),
@@ -241,6 +244,73 @@ def evaluate(chem, sur, n: int, seed: int, tolerances=(2.0, 5.0), ens_K=(0.5, 1.
     return summary, cells
 
 
+def train_and_calibrate_gate(a, chem, sur):
+    """The error gate: trained on the ensemble's errors on pairs the ensemble was not trained on,
+    its threshold calibrated on further held-out cells against the plain solve (pairs of the same
+    distribution: the uneven batch, or mixing-layer trajectories of other seeds)."""
+    import torch
+
+    t0 = time.perf_counter()
+    gseed = a.gate_seed or a.seed + 50021
+    if a.dist == "mixing-layer":
+        g0, g1, gd, _ = make_trajectory_pairs(chem, a.gate_pairs, gseed)
+    else:
+        g0, g1, gd, _ = make_pairs(chem, a.gate_pairs, gseed)
+    n_hard = 0
+    if a.gate_boost > 1:
+        # the pairs whose ensemble error is near or above the bars are repeated gate_boost times:
+        # the calibrated threshold is set by the lowest-scored of those, so the gate's ranking of
+        # them matters more than its fit of the bulk
+        r = []
+        for lo in range(0, g0.shape[1], 1 << 21):
+            hi = min(lo + (1 << 21), g0.shape[1])
+            pred, _, _ = sur.predict(g0[:, lo:hi], gd[lo:hi], P_ATM)
+            eT, eY = errors_vs(chem, pred, g1[:, lo:hi])
+            r.append(np.maximum(eT, eY))
+            del pred
+        hard = torch.from_numpy(np.nonzero(np.concatenate(r) > a.gate_boost_min)[0]).to(g0.device)
+        n_hard = int(hard.numel())
+        if n_hard:
+            rep = hard.repeat(int(a.gate_boost) - 1)
+            g0, g1, gd = torch.cat([g0, g0[:, rep]], 1), torch.cat([g1, g1[:, rep]], 1), torch.cat([gd, gd[rep]])
+    gl = sur.train_gate(g0, g1, gd, P_ATM, epochs=a.gate_epochs, batch=a.batch, lr=a.lr, under=a.gate_under)
+    del g0, g1, gd
+    if a.dist == "mixing-layer":
+        c0, c1, cd, _ = make_trajectory_pairs(chem, a.calib_cells, a.seed + 70001)
+    else:
+        c0, c1, cd, _ = make_pairs(chem, a.calib_cells, a.seed + 70001)
+    tol, acc, rmax = calibrate_gate(chem, sur, c0, cd, c1, margin=a.calib_margin)
+    sur.set_gate_tol(tol)
+    del c0, c1, cd
+    torch.cuda.empty_cache()
+    return {"pairs": a.gate_pairs, "seed": gseed, "epochs": a.gate_epochs, "under": a.gate_under,
+            "boost": a.gate_boost, "boost_min": a.gate_boost_min, "boosted_pairs": n_hard,
+            "losses": [float(v) for v in gl], "calib_cells": a.calib_cells, "calib_margin": a.calib_margin,
+            "tol": tol, "calib_accepted": acc, "calib_max_err_ratio": rmax, "s": time.perf_counter() - t0}
+
+
+def retrain_gate(a, chem):
+    """--gate-only: the ensemble of a.gate_only kept, its error gate trained and calibrated again;
+    the log of the original training is kept in the new JSON log with the new gate and evaluation."""
+    sur = capi.Surrogate(chem, members=a.members)
+    sur.load(a.gate_only)
+    gate = train_and_calibrate_gate(a, chem, sur)
+    sur.save(a.out)
+    ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991, dist=a.dist)
+    if a.cells_out:
+        np.savez_compressed(a.cells_out, **cells)
+    try:
+        with open(a.gate_only + ".json") as f:
+            log = json.load(f)
+    except OSError:
+        log = {"mechanism": a.mech}
+    log["gate"], log["eval"], log["gate_retrained_from"] = gate, ev, a.gate_only
+    with open(a.out + ".json", "w") as f:
+        json.dump(log, f, indent=1)
+    print(json.dumps({"gate": gate, "eval": ev}))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--mech", default="grimech30")
@@ -272,8 +342,17 @@ def main(argv=None):
     ap.add_argument("--calib-cells", type=int, default=1 << 21, help="held-out cells that calibrate the gate")
     ap.add_argument("--calib-margin", type=float, default=0.7, help="accepted cells stay within this fraction of "
                     "the bars on the calibration cells")
+    ap.add_argument("--gate-only", default="", help="a trained surrogate: keep its ensemble, train and calibrate "
+                    "its error gate again")
+    ap.add_argument("--gate-boost", type=float, default=1.0, help="copies of the gate pairs whose ensemble error "
+                    "exceeds --gate-boost-min of the bars")
+    ap.add_argument("--gate-boost-min", type=float, default=0.3)
+    ap.add_argument("--gate-seed", type=int, default=0, help="seed of the gate's training pairs (0: derived from "
+                    "--seed)")
     a = ap.parse_args(argv)
     chem = capi.FiniteChem(a.mech, "fp64")
+    if a.gate_only:
+        return retrain_gate(a, chem)
     t0 = time.perf_counter()
     if a.dist == "mixing-layer":
         n_on = int(a.pairs * a.onpolicy_frac) if a.onpolicy else 0
@@ -302,31 +381,7 @@ def main(argv=None):
         refine = {"epochs": a.refine_epochs, "lr": a.refine_lr, "boost": a.boost, "population": pop,
                   "losses": [float(v) for v in rl], "s": time.perf_counter() - t0}
     del s0, s1, d
-    gate = {}
-    if a.gate_pairs > 0:
-        # the gate learns the ensemble's errors on pairs it was not trained on, and its threshold
-        # is calibrated on further held-out cells against the plain solve (pairs of the same
-        # distribution: the uneven batch, or mixing-layer trajectories of other seeds)
-        import torch
-
-        t0 = time.perf_counter()
-        if a.dist == "mixing-layer":
-            g0, g1, gd, _ = make_trajectory_pairs(chem, a.gate_pairs, a.seed + 50021)
-        else:
-            g0, g1, gd, _ = make_pairs(chem, a.gate_pairs, a.seed + 50021)
-        gl = sur.train_gate(g0, g1, gd, P_ATM, epochs=a.gate_epochs, batch=a.batch, lr=a.lr, under=a.gate_under)
-        del g0, g1, gd
-        if a.dist == "mixing-layer":
-            c0, c1, cd, _ = make_trajectory_pairs(chem, a.calib_cells, a.seed + 70001)
-        else:
-            c0, c1, cd, _ = make_pairs(chem, a.calib_cells, a.seed + 70001)
-        tol, acc, rmax = calibrate_gate(chem, sur, c0, cd, c1, margin=a.calib_margin)
-        sur.set_gate_tol(tol)
-        del c0, c1, cd
-        torch.cuda.empty_cache()
-        gate = {"pairs": a.gate_pairs, "epochs": a.gate_epochs, "under": a.gate_under, "losses": [float(v) for v in gl],
-                "calib_cells": a.calib_cells, "calib_margin": a.calib_margin, "tol": tol,
-                "calib_accepted": acc, "calib_max_err_ratio": rmax, "s": time.perf_counter() - t0}
+    gate = train_and_calibrate_gate(a, chem, sur) if a.gate_pairs > 0 else {}
     sur.save(a.out)
     ev, cells = evaluate(chem, sur, a.eval_cells, a.seed + 99991, dist=a.dist)
     if a.cells_out:
