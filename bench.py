@@ -212,11 +212,13 @@ def cpu_rates_runner(mech):
     return "port", Oracle(mech)
 
 
-def cpu_step(wl, impl, sol, dts, lo, m, nthreads):
-    """One bounded sample of the workload on the host cores (cells lo .. lo+m, wrapping).
-    Returns (cells, seconds of the compute call); gathering the sample is not timed."""
+def cpu_step(wl, impl, sol, dts, lo, m, nthreads, stride=1):
+    """One bounded sample of the workload on the host cores: cells lo, lo + stride, ... (m of
+    them, wrapping). With stride = ncells / m the sample spans the whole batch, so that it sees
+    the batch's mix of easy and stiff cells. Returns (cells, seconds of the compute call);
+    gathering the sample is not timed."""
     n = sol.shape[1]
-    idx = (lo + np.arange(m)) % n
+    idx = (lo + stride * np.arange(m)) % n
     sub = np.ascontiguousarray(sol[:, idx])
     d = None if dts is None or np.ndim(dts) == 0 else np.ascontiguousarray(dts[idx])
     y, t = (np.ascontiguousarray(sub[:-1]), np.ascontiguousarray(sub[-1])) if wl["kind"] == "props" else (None, None)
@@ -243,10 +245,10 @@ def time_cpu(wl, sol, dts, seconds: float, nthreads: int):
     kind, impl = cpu_impl(wl)
     m = min(wl["ref_sample"], sol.shape[1])
     stride = max(1, sol.shape[1] // m)
-    cpu_step(wl, impl, sol, dts, 0, min(m, 256), nthreads)  # warm-up
+    cpu_step(wl, impl, sol, dts, 0, min(m, 256), nthreads, stride)  # warm-up
     done, el, i = 0, 0.0, 0
     while el < seconds:
-        c, s = cpu_step(wl, impl, sol, dts, (i * 7919 * stride) % sol.shape[1], m, nthreads)
+        c, s = cpu_step(wl, impl, sol, dts, (1 + i * 7919) % stride, m, nthreads, stride)
         done, el, i = done + c, el + s, i + 1
     return kind, done / el, done, el
 
@@ -267,12 +269,14 @@ def reference_arm(args, wl, config, metric, unit):
     nthreads = os.cpu_count() or 1
     kind, impl = cpu_impl(wl)
     m = min(wl["ref_sample"], sol.shape[1])
+    stride = max(1, sol.shape[1] // m)
     for w in range(args.warmup):
-        cpu_step(wl, impl, sol, dts, w * m, m, nthreads)
-    el = sum(cpu_step(wl, impl, sol, dts, (k * 7919 * m) % sol.shape[1], m, nthreads)[1] for k in range(args.steps))
+        cpu_step(wl, impl, sol, dts, (104729 * (w + 1)) % stride, m, nthreads, stride)
+    el = sum(cpu_step(wl, impl, sol, dts, (1 + k * 7919) % stride, m, nthreads, stride)[1] for k in range(args.steps))
     val = m * args.steps / el
     what = cpu_what(wl, kind)
-    sample = f"{m} cells of the workload per step, {what}, OpenMP over cells"
+    sample = (f"{m} cells of the workload per step (every {stride}th cell of the batch, a new offset per step), "
+              f"{what}, OpenMP over cells")
     print(json.dumps({"impl": "reference", "metric": metric, "value": val, "unit": unit, "n_gpus": args.gpus,
                       "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
                       "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -429,8 +433,8 @@ def run_sweep(args, wl, config, metric, unit, ws, rank, local, dev, pg):
     if rank == 0 and ws == 1 and args.cpu_seconds > 0:
         kind, cval, cdone, cel = time_cpu(wl, sol, dt, args.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": f"{cdone} cells ({cel:.1f} s) of the initial mixing layer, one implicit BDF/Newton "
-                         "substep each (no surrogate), OpenMP over cells"}
+               "sample": f"{cdone} cells ({cel:.1f} s) of the initial mixing layer in strided samples spanning "
+                         "the layer, one implicit BDF/Newton substep each (no surrogate), OpenMP over cells"}
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -559,7 +563,8 @@ def run_props(args, wl, config, metric, unit, ws, rank, local, dev, pg):
     if rank == 0 and ws == 1 and args.cpu_seconds > 0:
         kind, cval, cdone, cel = time_cpu(wl, sol, None, args.cpu_seconds, os.cpu_count() or 1)
         cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, {cpu_what(wl, kind)}, OpenMP over cells"}
+               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload in strided samples spanning the "
+                         f"batch, {cpu_what(wl, kind)}, OpenMP over cells"}
     if rank == 0:
         print(json.dumps({"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
                           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -858,7 +863,8 @@ def main():
         kind, cval, cdone, cel = time_cpu(wl, sol, dts, args.cpu_seconds, os.cpu_count() or 1)
         what = cpu_what(wl, kind) if wl["kind"] in ("rates", "props") else "implicit BDF/Newton substep (no surrogate)"
         cpu = {"value": cval, "unit": unit, "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload, {what}, OpenMP over cells"}
+               "sample": f"{cdone} cells ({cel:.1f} s) of the same workload in strided samples of "
+                         f"{min(wl['ref_sample'], ncells)} cells spanning the batch, {what}, OpenMP over cells"}
     if rank == 0:
         line = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
