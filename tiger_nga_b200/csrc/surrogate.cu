@@ -56,6 +56,7 @@ struct SurPost {
   long long ld_out;
   int* reason_out;    // per cell, nullable
   double* ind_out;    // per cell kIndicators values, nullable
+  int cell_base;      // added to the fallback list's entries (the cells' place in the whole batch)
 };
 
 // per-cell indicators of tng_surrogate_predict: consistency (K), ensemble T spread (K), ensemble
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(128) k_sur_post(const SurPost a) {
       a.out_state[(long long)a.ns * a.ld_out + cell] = rho * T1;
     } else if (reason) {
       const int slot = atomicAdd(a.fb_count, 1);
-      a.fb_list[slot] = cell;
+      a.fb_list[slot] = a.cell_base + cell;
       atomicAdd(&a.cnt[reason], 1ULL);
     } else {
       for (int k = 0; k < a.ns; ++k) a.state[(long long)k * a.ld + cell] = rho * y_new(Y0, dY, k, inv_sum);
@@ -577,6 +578,10 @@ struct tng_surrogate {
   __nv_bfloat16* d_gpack = nullptr;
   long long g_off[kMaxLayers] = {};
   DevBuf gout;
+  // the host-pointer substep's upload in chunks: a copy stream and one event per chunk (+ start)
+  static constexpr int kPipeChunks = 16;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t pev[kPipeChunks + 1] = {};
 };
 
 static int sur_upload_norm(tng_surrogate* s) {
@@ -620,9 +625,9 @@ static int sur_pack(tng_surrogate* s) {
 // s->gout): the cells' features are formed once for all of them.
 static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int64_t ncells, int64_t dld,
                         const double* ddts, double dt, double p, int first_member, int nmembers, float* out, bool gate,
-                        int* err) {
+                        int* err, int64_t gate_off = 0) {
   gate = gate && s->has_gate;
-  if (gate && !s->gout.reserve((size_t)ncells * s->gate.out_pad * sizeof(float)))
+  if (gate && !s->gout.reserve((size_t)(gate_off + ncells) * s->gate.out_pad * sizeof(float)))
     return set_error(TNG_ERR_CUDA, "surrogate gate output allocation failed");
   InferArgs ia{};
   ia.state = dstate;
@@ -654,7 +659,7 @@ static int launch_infer(tng_chem* h, tng_surrogate* s, const double* dstate, int
     return set_error(TNG_ERR_ARG, "inference: 1..%d networks per launch", kMaxNets);
   for (int i = 0; i < nmembers; ++i)
     add(s->member(first_member + i), s->d_wpack[first_member + i], s->w_off, out + (size_t)i * ncells * s->m.out_pad);
-  if (gate) add(s->gate, s->d_gpack, s->g_off, (float*)s->gout.ptr);
+  if (gate) add(s->gate, s->d_gpack, s->g_off, (float*)s->gout.ptr + gate_off * s->gate.out_pad);
   ia.error = err;
   ia.wait_limit = s->dbg_wait_limit;
   ia.fault = s->dbg_fault;
@@ -706,6 +711,73 @@ static SurPost post_args(tng_chem* h, tng_surrogate* s, double* state, int64_t l
     pa.gate_log_tol = std::log10(tol);
   }
   return pa;
+}
+
+// The front of the surrogate substep with host pointers, overlapped with the state's upload: the
+// state (and per-cell dt) go to the device in chunks on the surrogate's copy stream, and on the
+// handle's stream each chunk's judged cells are gathered and its cells inferred and
+// post-processed as soon as its copy has landed. The judged cells (jidx on the device, ascending:
+// joff + j * jstride) are gathered into jdst / jdts (leading dimension jld). ev[0] .. ev[1] bracket
+// the interleaved front (ev[2] = ev[1]).
+static int sur_front_pipelined(tng_chem* h, tng_surrogate* s, const double* state, int64_t ld, int64_t ncells,
+                               const double* dts, double dt, double p, double* dstate, double* ddts, int J,
+                               int64_t joff, int64_t jstride, double* jdst, int64_t jld, double* jdts, int* fb_list,
+                               int* fb_count, unsigned long long* cnt) {
+  cudaStream_t st = h->stream;
+  const int nv = s->ns + 1;
+  constexpr int kMax = tng_surrogate::kPipeChunks;
+  int64_t chunk = (int64_t)1 << 18;
+  if ((ncells + chunk - 1) / chunk > kMax) chunk = ((ncells + kMax - 1) / kMax + 127) / 128 * 128;
+  const int nch = (int)((ncells + chunk - 1) / chunk);
+  cudaError_t e = cudaSuccess;
+  if (!s->copy_stream && (e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_error(e, "surrogate copy stream");
+  for (auto& ev : s->pev)
+    if (!ev && (e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_error(e, "surrogate copy events");
+  if (s->has_gate && !s->gout.reserve((size_t)ncells * s->gate.out_pad * sizeof(float)))
+    return set_error(TNG_ERR_CUDA, "surrogate gate output allocation failed");
+  // the uploads start after the handle's stream reached this point (the previous call may still
+  // read the device buffers)
+  cudaEventRecord(s->pev[0], st);
+  cudaStreamWaitEvent(s->copy_stream, s->pev[0], 0);
+  for (int k = 0; k < nch; ++k) {
+    const int64_t a = k * chunk, n = std::min(chunk, ncells - a);
+    cudaMemcpy2DAsync(dstate + a, ncells * sizeof(double), state + a, ld * sizeof(double), n * sizeof(double), nv,
+                      cudaMemcpyHostToDevice, s->copy_stream);
+    if (dts) cudaMemcpyAsync(ddts + a, dts + a, n * sizeof(double), cudaMemcpyHostToDevice, s->copy_stream);
+    cudaEventRecord(s->pev[1 + k], s->copy_stream);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "surrogate state upload");
+  cudaEventRecord(s->ev[0], st);
+  for (int k = 0; k < nch; ++k) {
+    const int64_t a = k * chunk, n = std::min(chunk, ncells - a);
+    cudaStreamWaitEvent(st, s->pev[1 + k], 0);
+    if (J > 0) {  // the judged cells of this chunk, before the post-processing overwrites them
+      const int64_t j0 = a <= joff ? 0 : std::min<int64_t>(J, (a - joff + jstride - 1) / jstride);
+      const int64_t j1 = std::min<int64_t>(J, (a + n - joff + jstride - 1) / jstride);
+      if (j1 > j0)
+        k_gather_cells<<<(int)((j1 - j0 + 127) / 128), 128, 0, st>>>(
+            dstate, ncells, nv, (const int*)s->judge_idx.ptr + j0, (int)(j1 - j0), jdst + j0, jld, ddts, dt,
+            jdts + j0);
+    }
+    float* out_k = (float*)s->out.ptr + (size_t)a * s->m.out_pad * s->members;
+    int rc = launch_infer(h, s, dstate + a, n, ncells, ddts ? ddts + a : nullptr, dt, p, 0, s->members, out_k, true,
+                          (int*)(cnt + 8), a);
+    if (rc) return rc;
+    SurPost pa = post_args(h, s, dstate + a, ncells, n, ddts ? ddts + a : nullptr, dt, p);
+    pa.out = out_k;
+    if (s->has_gate) pa.gate_out = (const float*)s->gout.ptr + a * s->gate.out_pad;
+    pa.cell_base = (int)a;
+    pa.fb_list = fb_list;
+    pa.fb_count = fb_count;
+    pa.cnt = cnt;
+    k_sur_post<<<(int)std::min<int64_t>(4096, (n + 127) / 128), 128, 0, st>>>(pa);
+  }
+  cudaEventRecord(s->ev[1], st);
+  cudaEventRecord(s->ev[2], st);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate kernels");
 }
 }  // namespace tng
 
@@ -815,6 +887,12 @@ int tng_surrogate_destroy(tng_surrogate* s) {
     b->release();
   for (auto& ev : s->ev)
     if (ev) cudaEventDestroy(ev);
+  for (auto& ev : s->pev)
+    if (ev) cudaEventDestroy(ev);
+  if (s->copy_stream) {
+    cudaStreamSynchronize(s->copy_stream);
+    cudaStreamDestroy(s->copy_stream);
+  }
   if (s->h) s->h->dependents--;
   delete s;
   return TNG_OK;
@@ -1281,6 +1359,8 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
   cudaStream_t st = h->stream;
   const int nv = s->ns + 1;
   cudaError_t e;
+  // with host pointers and a large batch the upload is overlapped with the front of the substep
+  const bool pipelined = flags == TNG_HOST_PTRS && ncells >= ((int64_t)1 << 19);
   double* dstate = state;
   const double* ddts = dts;
   int64_t dld = ld;
@@ -1290,11 +1370,11 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
       return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: device state allocation failed");
     dstate = (double*)h->bufs[6].ptr;
     dld = ncells;
-    cudaMemcpy2DAsync(dstate, ncells * sizeof(double), state, ld * sizeof(double), ncells * sizeof(double), nv,
-                      cudaMemcpyHostToDevice, st);
-    if (dts) {
-      cudaMemcpyAsync(h->bufs[7].ptr, dts, ncells * sizeof(double), cudaMemcpyHostToDevice, st);
-      ddts = (const double*)h->bufs[7].ptr;
+    if (dts) ddts = (const double*)h->bufs[7].ptr;
+    if (!pipelined) {
+      cudaMemcpy2DAsync(dstate, ncells * sizeof(double), state, ld * sizeof(double), ncells * sizeof(double), nv,
+                        cudaMemcpyHostToDevice, st);
+      if (dts) cudaMemcpyAsync(h->bufs[7].ptr, dts, ncells * sizeof(double), cudaMemcpyHostToDevice, st);
     }
   }
   const int J = (int)std::min<int64_t>(ncells, std::max(0, s->cfg.judge_cells));
@@ -1333,7 +1413,9 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
     const int64_t off = (int64_t)(s->calls * 7919) % stride;
     for (int j = 0; j < J; ++j) idx[j] = (int)((off + (int64_t)j * stride) % ncells);
     cudaMemcpyAsync(s->judge_idx.ptr, idx.data(), sizeof(int) * J, cudaMemcpyHostToDevice, st);
-    if (joint)
+    if (pipelined)
+      ;  // gathered chunk by chunk below
+    else if (joint)
       k_gather_cells<<<(J + 127) / 128, 128, 0, st>>>(dstate, dld, nv, (const int*)s->judge_idx.ptr, J, comp, ldc,
                                                       ddts, dt, comp_dts);
     else
@@ -1342,19 +1424,29 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
                                                       (double*)s->judge_dts.ptr);
   }
   s->calls++;
-  // inference on the tensor cores
-  cudaEventRecord(s->ev[0], st);
-  rc = launch_infer(h, s, dstate, ncells, dld, ddts, dt, p, 0, s->members, (float*)s->out.ptr, true, (int*)(cnt + 8));
-  if (rc) return rc;
-  cudaEventRecord(s->ev[1], st);
-  // post-processing and fallback list
-  SurPost pa = post_args(h, s, dstate, dld, ncells, ddts, dt, p);
-  pa.fb_list = fb_list;
-  pa.fb_count = fb_count;
-  pa.cnt = cnt;
-  k_sur_post<<<(int)std::min<int64_t>(4096, (ncells + 127) / 128), 128, 0, st>>>(pa);
-  cudaEventRecord(s->ev[2], st);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "surrogate kernels");
+  if (pipelined) {
+    const int64_t jstride = J > 0 ? std::max<int64_t>(1, ncells / J) : 1;
+    const int64_t joff = J > 0 ? (int64_t)((s->calls - 1) * 7919) % jstride : 0;
+    rc = sur_front_pipelined(h, s, state, ld, ncells, dts, dt, p, dstate, (double*)ddts, J, joff, jstride,
+                             joint ? comp : (double*)s->judge_state.ptr, joint ? ldc : J,
+                             joint ? comp_dts : (double*)s->judge_dts.ptr, fb_list, fb_count, cnt);
+    if (rc) return rc;
+  } else {
+    // inference on the tensor cores
+    cudaEventRecord(s->ev[0], st);
+    rc = launch_infer(h, s, dstate, ncells, dld, ddts, dt, p, 0, s->members, (float*)s->out.ptr, true,
+                      (int*)(cnt + 8));
+    if (rc) return rc;
+    cudaEventRecord(s->ev[1], st);
+    // post-processing and fallback list
+    SurPost pa = post_args(h, s, dstate, dld, ncells, ddts, dt, p);
+    pa.fb_list = fb_list;
+    pa.fb_count = fb_count;
+    pa.cnt = cnt;
+    k_sur_post<<<(int)std::min<int64_t>(4096, (ncells + 127) / 128), 128, 0, st>>>(pa);
+    cudaEventRecord(s->ev[2], st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "surrogate kernels");
+  }
   tng_substep_stats fst;
   if (joint) {
     // fallback cells and the judged sample in one implicit solve, then the fallback cells back
