@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -582,6 +583,12 @@ struct tng_surrogate {
   static constexpr int kPipeChunks = 16;
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t pev[kPipeChunks + 1] = {};
+  // ... and its download: the state after the post-processing goes back during the fallback
+  // solve, then only the solved fallback cells (pinned staging, grown as needed)
+  cudaEvent_t ev_front = nullptr, ev_down = nullptr;
+  double* h_comp = nullptr;
+  int* h_list = nullptr;
+  size_t h_cap = 0;  // cells
 };
 
 static int sur_upload_norm(tng_surrogate* s) {
@@ -779,6 +786,27 @@ static int sur_front_pipelined(tng_chem* h, tng_surrogate* s, const double* stat
   e = cudaGetLastError();
   return e == cudaSuccess ? TNG_OK : cuda_error(e, "surrogate kernels");
 }
+
+// The solved fallback cells into the host state: row v of the compact block (n cells, in list
+// order) to state[v * ld + list[i]]. The cells are visited in increasing order (the list comes
+// from atomics) and the species rows are split over a few threads.
+static void scatter_fallback_host(double* state, int64_t ld, int nv, const double* comp, const int* list, int n) {
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return list[a] < list[b]; });
+  const int nt = std::max(1, std::min<int>({nv, 8, (int)std::thread::hardware_concurrency()}));
+  auto work = [&](int t) {
+    for (int v = t; v < nv; v += nt) {
+      double* row = state + (int64_t)v * ld;
+      const double* src = comp + (int64_t)v * n;
+      for (int i : ord) row[list[i]] = src[i];
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+}
 }  // namespace tng
 
 extern "C" {
@@ -889,6 +917,10 @@ int tng_surrogate_destroy(tng_surrogate* s) {
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : s->pev)
     if (ev) cudaEventDestroy(ev);
+  for (auto ev : {s->ev_front, s->ev_down})
+    if (ev) cudaEventDestroy(ev);
+  if (s->h_comp) cudaFreeHost(s->h_comp);
+  if (s->h_list) cudaFreeHost(s->h_list);
   if (s->copy_stream) {
     cudaStreamSynchronize(s->copy_stream);
     cudaStreamDestroy(s->copy_stream);
@@ -1431,6 +1463,18 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
                              joint ? comp : (double*)s->judge_state.ptr, joint ? ldc : J,
                              joint ? comp_dts : (double*)s->judge_dts.ptr, fb_list, fb_count, cnt);
     if (rc) return rc;
+    if (joint) {
+      // every accepted cell is final now: the state goes back during the fallback solve, which
+      // works on its own batch (the fallback cells are patched on the host afterwards)
+      for (auto* ev : {&s->ev_front, &s->ev_down})
+        if (!*ev && (e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess)
+          return cuda_error(e, "surrogate download events");
+      cudaEventRecord(s->ev_front, st);
+      cudaStreamWaitEvent(s->copy_stream, s->ev_front, 0);
+      cudaMemcpy2DAsync(state, ld * sizeof(double), dstate, ncells * sizeof(double), ncells * sizeof(double), nv,
+                        cudaMemcpyDeviceToHost, s->copy_stream);
+      cudaEventRecord(s->ev_down, s->copy_stream);
+    }
   } else {
     // inference on the tensor cores
     cudaEventRecord(s->ev[0], st);
@@ -1454,7 +1498,11 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
     k_joint_order<<<(int)std::min<int64_t>(4096, (ldc + 255) / 256), 256, 0, st>>>(comp_iota, fb_count, J, ldc);
     rc = substep_run(h, comp, ldc, ldc, comp_dts, 0.0, p, TNG_DEVICE_PTRS, comp_iota, comp_n, nullptr, nullptr, nullptr,
                      &fst);
-    if (rc) return rc;
+    if (rc) {
+      if (pipelined) cudaStreamSynchronize(s->copy_stream);  // no copy into the caller's buffer after return
+      return rc;
+    }
+    if (pipelined) cudaStreamWaitEvent(st, s->ev_down, 0);  // the download has read the state
     k_scatter_list<<<1184, 128, 0, st>>>(dstate, dld, nv, fb_list, fb_count, J, comp, ldc);
     cudaEventRecord(s->ev[3], st);
     // judge: the implicit solve of the sample against the surrogate(+fallback) result
@@ -1468,14 +1516,43 @@ int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t 
     cudaEventRecord(s->ev[3], st);
   }
   cudaEventRecord(s->ev[4], st);
-  if (flags == TNG_HOST_PTRS)
+  const bool patch = pipelined && joint;  // download overlapped, fallback cells patched on the host
+  if (flags == TNG_HOST_PTRS && !patch)
     cudaMemcpy2DAsync(state, ld * sizeof(double), dstate, ncells * sizeof(double), ncells * sizeof(double), nv,
                       cudaMemcpyDeviceToHost, st);
   if (stats || flags == TNG_HOST_PTRS) {
     unsigned long long hc[16];
+    int nfb = 0;
     cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "surrogate substep");
+    if (patch) cudaMemcpyAsync(&nfb, fb_count, sizeof(int), cudaMemcpyDeviceToHost, st);
+    e = cudaStreamSynchronize(st);
+    if (patch && (e != cudaSuccess || hc[8])) cudaStreamSynchronize(s->copy_stream);
+    if (e != cudaSuccess) return cuda_error(e, "surrogate substep");
     if (hc[8]) return set_error(TNG_ERR_CUDA, "tng_substep_surrogate: tensor-core inference timed out");
+    if (patch) {
+      if (nfb > 0) {
+        if ((size_t)nfb > s->h_cap) {
+          if (s->h_comp) cudaFreeHost(s->h_comp);
+          if (s->h_list) cudaFreeHost(s->h_list);
+          s->h_comp = nullptr, s->h_list = nullptr, s->h_cap = 0;
+          if ((e = cudaMallocHost(&s->h_comp, (size_t)nfb * nv * sizeof(double))) != cudaSuccess ||
+              (e = cudaMallocHost(&s->h_list, (size_t)nfb * sizeof(int))) != cudaSuccess) {
+            cudaStreamSynchronize(s->copy_stream);
+            return cuda_error(e, "surrogate fallback staging");
+          }
+          s->h_cap = (size_t)nfb;
+        }
+        cudaMemcpy2DAsync(s->h_comp, (size_t)nfb * sizeof(double), comp + J, ldc * sizeof(double),
+                          (size_t)nfb * sizeof(double), nv, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(s->h_list, fb_list, (size_t)nfb * sizeof(int), cudaMemcpyDeviceToHost, st);
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {
+          cudaStreamSynchronize(s->copy_stream);
+          return cuda_error(e, "surrogate fallback download");
+        }
+      }
+      if ((e = cudaEventSynchronize(s->ev_down)) != cudaSuccess) return cuda_error(e, "surrogate state download");
+      if (nfb > 0) scatter_fallback_host(state, ld, nv, s->h_comp, s->h_list, nfb);
+    }
     if (stats) {
       stats->cells = ncells;
       stats->accepted = (int64_t)hc[0];
