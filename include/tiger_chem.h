@@ -391,7 +391,12 @@ int tng_surrogate_debug_waits(tng_surrogate* s, int wait_limit, int fault);
 int tng_surrogate_infer(tng_surrogate* s, const double* state, int64_t n, int64_t ld, const double* dts, double dt,
                         double p, float* out);
 /* The substep through the surrogate with fallback; same state convention as tng_substep_batch.
- * flags: TNG_DEVICE_PTRS or TNG_HOST_PTRS. stats may be null. */
+ * flags: TNG_DEVICE_PTRS or TNG_HOST_PTRS. stats may be null. With host pointers and a batch of
+ * 2^19 cells or more the state is uploaded in chunks that overlap the inference and
+ * post-processing of the chunks already on the device (stats->ms_infer then covers both and
+ * ms_post is 0), and with stats the post-processed state is downloaded during the fallback solve,
+ * the solved fallback cells being patched into the host state afterwards; the results are the
+ * same as with device pointers. */
 int tng_substep_surrogate(tng_chem* h, tng_surrogate* s, double* state, int64_t ncells, int64_t ld, const double* dts,
                           double dt, double p, int flags, tng_surrogate_stats* stats);
 
