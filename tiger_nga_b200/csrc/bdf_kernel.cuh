@@ -265,7 +265,9 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
           conv_fail = true;
 #pragma unroll 1
           for (int it = 0; it < maxcor; ++it) {
-            {
+            // the first iterate is the predicted state: after a new Jacobian, f already holds
+            // the right-hand side there (the Jacobian was formed around it)
+            if (it > 0 || !jcur) {
               const double2 r = rhs_call(t, w.mat, y[0], y[1], p, lane);
               f[0] = r.x, f[1] = r.y;
             }
