@@ -239,7 +239,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         bool jcur = false;
         if (need_j || nst >= nst_lu + msbp || fabs(gamma / gamma_lu - 1.0) > dgmax) {
           {
-            const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane);
+            const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane, 1);  // keeps the rate constants
             f[0] = r.x, f[1] = r.y;
           }
           jac_call(t, w.mat, z[0][0], z[0][1], f[0], f[1], p, lane);
@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(WARPS * 32)
   for (int cell = blockIdx.x * WARPS + warp; cell < n; cell += gridDim.x * WARPS) {
     const double y0 = lane < nv ? state[(long long)lane * ld + cell] : 0.0;
     const double y1 = lane + 32 < nv ? state[(long long)(lane + 32) * ld + cell] : 0.0;
-    const double2 r = rhs_call(t, w.mat, y0, y1, p, lane);
+    const double2 r = rhs_call(t, w.mat, y0, y1, p, lane, jac != nullptr);  // keeps the rate constants
     const double f0 = r.x, f1 = r.y;
     if (lane < nv) rhs[(long long)lane * ld + cell] = f0;
     if (lane + 32 < nv) rhs[(long long)(lane + 32) * ld + cell] = f1;

@@ -307,13 +307,15 @@ __device__ __forceinline__ double plain_const(const SvT<LY>& t, const CellPrep& 
   return (w0 & 8) ? a : v;
 }
 
-// The cell preparation and the slot loops, shared by the right-hand side and the Jacobian in one
-// out-of-line copy (the solver's code must fit the instruction cache): W[q] = the slot's rate
-// constant (products = 0; ln Pr of the falloff slots into w.lpr) or its rate (products = 1:
-// times the reactant concentrations and the third-body sum). The cell's CellPrep is left in w.cp.
+// The cell preparation and the slot loops of the right-hand side, one out-of-line copy (the
+// solver's code must fit the instruction cache): W[q] = the slot's rate (its rate constant times
+// the reactant concentrations and the third-body sum). With keep, the rate constants are also
+// left in the matrix area (mat[q]) with ln Pr of the falloff slots (mat[NSLOT + q]), for the
+// Jacobian formed next at the same state. The cell's CellPrep is left in w.cp.
 template <class LY>
 static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, const double y0, const double y1,
-                                               const double p, const int lane, const int products) {
+                                               const double p, const int lane, const int keep) {
+  static_assert(SvT<LY>::NV * SvT<LY>::RS >= SvT<LY>::NSLOT + SvT<LY>::NFO, "kept constants fit the matrix area");
   const WarpMem w = warp_mem<LY>(wb);
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
   const int* sw = t.i(HI_SLOT);
@@ -334,18 +336,18 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
     double lpr = 0.0;
     const double k = falloff_const(t, w, c, w1, &lpr);
-    if (products) {
-      w.W[q] = mass_action(k, w0, w1);
-    } else {
-      w.W[q] = k;
-      w.lpr[q] = lpr;
+    w.W[q] = mass_action(k, w0, w1);
+    if (keep) {
+      w.mat[q] = k;
+      w.mat[SvT<LY>::NSLOT + q] = lpr;
     }
   }
 #pragma unroll 1
   for (int q = SvT<LY>::NFO + lane; q < SvT<LY>::NSLOT; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
     const double k = plain_const(t, c, q, w0);
-    w.W[q] = products ? mass_action(k, w0, w1) : k;
+    w.W[q] = mass_action(k, w0, w1);
+    if (keep) w.mat[q] = k;
   }
   if (lane == 0) {
     w.cp[0] = c.rho, w.cp[1] = c.T, w.cp[2] = c.LT, w.cp[3] = c.invRT, w.cp[4] = c.invT, w.cp[5] = c.irho;
@@ -362,9 +364,9 @@ __device__ __forceinline__ CellPrep load_prep(const WarpMem& w) {
 // finitechem_compute_rhs for one cell, warp-cooperative. Input/output two entries per lane.
 template <class LY>
 __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
-                                         const double p, double& f0, double& f1, const int lane) {
+                                         const double p, double& f0, double& f1, const int lane, const int keep) {
   constexpr int ns = SvT<LY>::NS;
-  prep_rates<LY>(t, w.mat, y0, y1, p, lane, 1);
+  prep_rates<LY>(t, w.mat, y0, y1, p, lane, keep);
   const CellPrep c = load_prep(w);
   {
     // production-rate chunks: every lane walks the same number of steps over its interleaved
@@ -426,20 +428,24 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
 // compile-time layout, so that no descriptor goes through the stack.)
 template <class LY>
 static __device__ __noinline__ double2 rhs_call(const SvT<LY> t, double* wb, const double y0, const double y1,
-                                                const double p, const int lane) {
+                                                const double p, const int lane, const int keep = 0) {
   const WarpMem w = warp_mem<LY>(wb);
   double f0, f1;
-  rhs_warp(t, w, y0, y1, p, f0, f1, lane);
+  rhs_warp(t, w, y0, y1, p, f0, f1, lane, keep);
   return make_double2(f0, f1);
 }
 
 // Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
-// row stride rs). Uses one extra right-hand side for the temperature column.
+// row stride rs). Uses one extra right-hand side for the temperature column. It must follow the
+// right-hand side at y evaluated with keep: the rate constants, ln Pr, concentrations, third-body
+// sums and cell preparation are that evaluation's (the same values a new evaluation would give).
 template <class LY>
 __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
                                          const double f0, const double f1, const double p, const int lane) {
   constexpr int ns = SvT<LY>::NS, nv = ns + 1, rs = SvT<LY>::RS;
-  prep_rates<LY>(t, w.mat, y0, y1, p, lane, 0);
+  for (int q = lane; q < SvT<LY>::NSLOT; q += 32) w.W[q] = w.mat[q];
+  for (int q = lane; q < SvT<LY>::NFO; q += 32) w.lpr[q] = w.mat[SvT<LY>::NSLOT + q];
+  __syncwarp();
   const CellPrep c = load_prep(w);
   const int* sw = t.i(HI_SLOT);
 #pragma unroll 1
