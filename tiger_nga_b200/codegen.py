@@ -535,6 +535,18 @@ def write_all(out_dir: str, names=("hydrogen", "grimech30", "dme39")) -> list[st
 NONE7 = 127
 
 
+def _layout_const(name: str) -> int:
+    """A record stride of csrc/solver_layout.h (the one place it is defined)."""
+    import re
+    src = open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "solver_layout.h")).read()
+    return int(re.search(rf"\b{name} = (\d+)", src).group(1))
+
+
+# Odd record strides: the lanes reading one field of consecutive records hit distinct banks.
+SLOT_REC, FO_REC, FC_REC, TH_STRIDE = (_layout_const(k) for k in ("kSlotRec", "kFoRec", "kFcRec", "kThStride"))
+assert SLOT_REC == 3 and FO_REC == 7 and FC_REC == 7 and TH_STRIDE >= 24
+
+
 def _lpt(sizes: list[int], nlanes: int = 32) -> list[list[int]]:
     """Longest-processing-time assignment of tasks to lanes (deterministic)."""
     order = sorted(range(len(sizes)), key=lambda t: (-sizes[t], t))
@@ -583,22 +595,20 @@ def solver_tables(name: str) -> dict:
         s32, s64 = m32.slots[r], m64.slots[r]
         reac = (s32.C + [NONE7] * 3)[:3]
         mw = s32.M if s32.M >= 0 else NONE7
-        if s32.kind == "falloff":
+        if s32.kind == "falloff":  # the falloff slots come first and have no plain record
             flags, fo = 1, len(fos)
             fos.append((s32, s64))
-            sd32 += [0.0] * 4
-            sd64 += [0.0] * 4
         else:
             a, b = s32.arr, s64.arr
             flags = (2 if a.n is not None else 0) | (4 if a.E is not None else 0)
             fo = 0
             if flags == 0:
                 flags = 8
-                sd32 += [a.A, 0.0, 0.0, 0.0]
-                sd64 += [b.A, 0.0, 0.0, 0.0]
+                sd32 += [a.A, 0.0, 0.0]
+                sd64 += [b.A, 0.0, 0.0]
             else:
-                sd32 += [math.log(a.A), a.E or 0.0, a.n or 0.0, 0.0]
-                sd64 += [math.log(b.A), b.E or 0.0, b.n or 0.0, 0.0]
+                sd32 += [math.log(a.A), a.E or 0.0, a.n or 0.0]
+                sd64 += [math.log(b.A), b.E or 0.0, b.n or 0.0]
         si += [flags | (reac[0] << 4) | (reac[1] << 11) | (reac[2] << 18), mw | (fo << 8)]
     HD("slot", sd32, sd64)
     hi["slot"] = si
@@ -612,6 +622,7 @@ def solver_tables(name: str) -> dict:
             fl.append((2 if a.n is not None else 0) | (4 if a.E is not None else 0))
             fod32 += [math.log(a.A), a.E or 0.0, a.n or 0.0]
             fod64 += [math.log(b.A), b.E or 0.0, b.n or 0.0]
+        fod32.append(0.0), fod64.append(0.0)  # pad to FO_REC
         key = s32.fc_key
         if key == ((1.0, 1, 0.0),):
             fcid = -1
@@ -634,8 +645,8 @@ def solver_tables(name: str) -> dict:
                 while len(forms) < 3:
                     forms.append(15), r32.append((0.0, 0.0)), r64.append((0.0, 0.0))
                 fci.append(forms[0] | (forms[1] << 4) | (forms[2] << 8))
-                fcd32 += [v for t in r32 for v in t]
-                fcd64 += [v for t in r64 for v in t]
+                fcd32 += [v for t in r32 for v in t] + [0.0]  # pad to FC_REC
+                fcd64 += [v for t in r64 for v in t] + [0.0]
             fcid = fc_ids[key]
         foi.append(fl[0] | (fl[1] << 4) | ((fcid + 1) << 8) | (s32.M_fall << 16))
     HD("fo", fod32, fod64)
@@ -644,15 +655,16 @@ def solver_tables(name: str) -> dict:
     hi["fc"] = fci
     nfo, nfc = len(fos), len(fc_ids)
 
-    eff32 = np.zeros((max(nm, 1), ns))
-    eff64 = np.zeros((max(nm, 1), ns))
+    eff32 = np.zeros((max(nm, 1), ns | 1))  # rows of eff_stride(ns) = ns | 1
+    eff64 = np.zeros((max(nm, 1), ns | 1))
     for j, (t32, t64) in enumerate(zip(m32.third_body, m64.third_body)):
         for (s_, c), (_, c6) in zip(t32, t64):
             eff32[j, s_] += c
             eff64[j, s_] += c6
     HD("eff", eff32.reshape(-1), eff64.reshape(-1))
-    th32 = np.concatenate([m32.th_hi, m32.th_lo], axis=1).reshape(-1)
-    th64 = np.concatenate([m64.th_hi, m64.th_lo], axis=1).reshape(-1)
+    pad = np.zeros((ns, TH_STRIDE - 24))
+    th32 = np.concatenate([m32.th_hi, m32.th_lo, pad], axis=1).reshape(-1)
+    th64 = np.concatenate([m64.th_hi, m64.th_lo, pad], axis=1).reshape(-1)
     HD("th", th32, th64)
     HD("wmol", m32.wmol, m64.wmol)
     HD("invw", 1.0 / m32.wmol, 1.0 / m64.wmol)

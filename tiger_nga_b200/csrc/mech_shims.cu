@@ -27,7 +27,7 @@ std::atomic<tng_chem*> g_handle{nullptr};
 __global__ void k_thermo_one(const double* __restrict__ th, double tmid, int ns, double T, double* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= ns) return;
-  const double* a = th + 24 * k + (T > tmid ? 0 : 12);  // T > 1000 strict, as COMPTHERMODATA
+  const double* a = th + kThStride * k + (T > tmid ? 0 : 12);  // T > 1000 strict, as COMPTHERMODATA
   out[k] = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
   out[ns + k] = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
 }

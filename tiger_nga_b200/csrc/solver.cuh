@@ -139,7 +139,7 @@ struct WarpMem {
   double* vb;   // 64 vector buffer
   double* hb;   // 64 enthalpies
   double* cb;   // 64 heat capacities (Jacobian), then the pivot reciprocals of the LU
-  double* lpr;  // nfo: ln Pr of the falloff slots (rate-constant pass of the Jacobian)
+  double* pr;   // nfo: Pr of the falloff slots (from the rate pass the Jacobian follows)
   double* cp;   // 8: the cell's CellPrep from the last rate pass
   int* piv;     // 64 pivots
   int* perm;    // 64: the composed row permutation of the LU
@@ -167,7 +167,7 @@ __device__ __forceinline__ WarpMem warp_mem(double* base) {
   w.vb = p; p += 64;
   w.hb = p; p += 64;
   w.cb = p; p += 64;
-  w.lpr = p; p += T::NFO;
+  w.pr = p; p += T::NFO;
   w.cp = p; p += 8;
   w.piv = reinterpret_cast<int*>(p);
   w.perm = w.piv + 64;
@@ -242,7 +242,7 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
   const double prt = p * c.invRT;  // [M] of the ideal gas, for a third-body sum that is zero
   const double* eff = t.d(HD_EFF);
   for (int m = lane; m < nm; m += 32) {
-    const double* e = eff + m * ns;
+    const double* e = eff + m * eff_stride(ns);
     double acc = 0.0;
     for (int j = 0; j < ns; ++j) acc = fma(e[j], w.C[j], acc);
     w.Ms[m] = acc;
@@ -257,7 +257,7 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
     for (int q = 0; q < 3; ++q) {
       const int form = (forms >> (4 * q)) & 15;
       if (form == 15) break;
-      const double a = fcd[6 * f + 2 * q], cc = fcd[6 * f + 2 * q + 1];
+      const double a = fcd[kFcRec * f + 2 * q], cc = fcd[kFcRec * f + 2 * q + 1];
       const double term = form == 2 ? a : a * exp_ool(form == 0 ? -c.T * cc : -cc * c.invT);
       v = q == 0 ? term : v + term;
     }
@@ -272,19 +272,19 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
 }
 
 // Rate constant of a falloff slot from its falloff word w1 (GETLINDRATECOEFF-equivalent:
-// Lindemann, or Troe in log form); also returns ln Pr.
+// Lindemann, or Troe in log form); also returns Pr.
 template <class LY>
 __device__ __forceinline__ double falloff_const(const SvT<LY>& t, const WarpMem& w, const CellPrep& c, const int w1,
-                                               double* lpr_out) {
+                                               double* pr_out) {
   const int f = w1 >> 8;
-  const double* par = t.d(HD_FO) + 6 * f;
+  const double* par = t.d(HD_FO) + kFoRec * f;
   const int fw = t.i(HI_FO)[f];
   const double* sc = t.d(HD_SCAL);
   const double lk0 = expo(par[0], par[1], par[2], fw & 15, c.LT, c.invRT);
   const double lki = expo(par[3], par[4], par[5], (fw >> 4) & 15, c.LT, c.invRT);
   const double lpr = lk0 + w.lcm[fw >> 16] - fmax(lki, sc[SC_LNKMIN]);
-  *lpr_out = lpr;
   const double pr = rexp(t, lpr);
+  *pr_out = pr;
   const int fid = ((fw >> 8) & 255) - 1;
   double lk = lki;  // Lindemann: k_inf Pr / (1 + Pr)
   if (fid >= 0) {   // Troe: k_inf F Pr / (1 + Pr), ln F = ln Fc / (1 + f^2)
@@ -295,22 +295,22 @@ __device__ __forceinline__ double falloff_const(const SvT<LY>& t, const WarpMem&
   return rexp(t, lk) * pr / (1.0 + pr);
 }
 
-// Rate constant of a plain (Arrhenius or constant) slot without branches: the table holds
-// (ln A, E, n) with zeros for absent terms, so the FMA chain of expo() gives the same exponent;
-// constant slots hold A itself and take it.
+// Rate constant of a plain (Arrhenius or constant) slot: the table holds (ln A, E, n) with zeros
+// for absent terms, so the FMA chain of expo() gives the same exponent; constant slots hold A
+// itself. The constant slots come last in processing order, so the rounds of 32 slots that hold
+// only constants skip the exponential (one round per mechanism mixes the two kinds).
 template <class LY>
 __device__ __forceinline__ double plain_const(const SvT<LY>& t, const CellPrep& c, const int p, const int w0) {
-  const double* sd = t.d(HD_SLOT) + 4 * p;
+  const double* sd = t.d(HD_SLOT) + kSlotRec * (p - SvT<LY>::NFO);
   const double a = sd[0];
-  const double e = fma(sd[2], c.LT, fma(sd[1], c.invRT, a));
-  const double v = rexp(t, e);
-  return (w0 & 8) ? a : v;
+  if (w0 & 8) return a;
+  return rexp(t, fma(sd[2], c.LT, fma(sd[1], c.invRT, a)));
 }
 
 // The cell preparation and the slot loops of the right-hand side, one out-of-line copy (the
 // solver's code must fit the instruction cache): W[q] = the slot's rate (its rate constant times
 // the reactant concentrations and the third-body sum). With keep, the rate constants are also
-// left in the matrix area (mat[q]) with ln Pr of the falloff slots (mat[NSLOT + q]), for the
+// left in the matrix area (mat[q]) with Pr of the falloff slots (mat[NSLOT + q]), for the
 // Jacobian formed next at the same state. The cell's CellPrep is left in w.cp.
 template <class LY>
 static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, const double y0, const double y1,
@@ -334,12 +334,12 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
   // warp is hidden by the other warps)
   for (int q = lane; q < SvT<LY>::NFO; q += 32) {
     const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
-    double lpr = 0.0;
-    const double k = falloff_const(t, w, c, w1, &lpr);
+    double pr = 0.0;
+    const double k = falloff_const(t, w, c, w1, &pr);
     w.W[q] = mass_action(k, w0, w1);
     if (keep) {
       w.mat[q] = k;
-      w.mat[SvT<LY>::NSLOT + q] = lpr;
+      w.mat[SvT<LY>::NSLOT + q] = pr;
     }
   }
 #pragma unroll 1
@@ -402,7 +402,7 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
     if (k < ns) {
       double cd = 0.0;
       for (int q = spp[k]; q < spp[k + 1]; ++q) cd += w.part[q];
-      const double* a = th + 24 * k + toff;
+      const double* a = th + kThStride * k + toff;
       const double T = c.T;
       const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
       const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
@@ -437,14 +437,14 @@ static __device__ __noinline__ double2 rhs_call(const SvT<LY> t, double* wb, con
 
 // Jacobian of the right-hand side at y (f = rhs(y) given), assembled into w.mat (row-major,
 // row stride rs). Uses one extra right-hand side for the temperature column. It must follow the
-// right-hand side at y evaluated with keep: the rate constants, ln Pr, concentrations, third-body
+// right-hand side at y evaluated with keep: the rate constants, Pr, concentrations, third-body
 // sums and cell preparation are that evaluation's (the same values a new evaluation would give).
 template <class LY>
 __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, const double y0, const double y1,
                                          const double f0, const double f1, const double p, const int lane) {
   constexpr int ns = SvT<LY>::NS, nv = ns + 1, rs = SvT<LY>::RS;
   for (int q = lane; q < SvT<LY>::NSLOT; q += 32) w.W[q] = w.mat[q];
-  for (int q = lane; q < SvT<LY>::NFO; q += 32) w.lpr[q] = w.mat[SvT<LY>::NSLOT + q];
+  for (int q = lane; q < SvT<LY>::NFO; q += 32) w.pr[q] = w.mat[SvT<LY>::NSLOT + q];
   __syncwarp();
   const CellPrep c = load_prep(w);
   const int* sw = t.i(HI_SLOT);
@@ -505,7 +505,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
           const int fw = t.i(HI_FO)[w1 >> 8];
           const double Mf = w.Ms[fw >> 16];
           if (Mf > 0.0) {
-            const double pr = rexp(t, w.lpr[pp]);  // ln Pr from the rate-constant pass
+            const double pr = w.pr[pp];  // from the rate pass
             const int mw = w1 & 127;
             val = w.W[pp] / (Mf * (1.0 + pr)) * prodC * (mw != kNone7 ? w.Ms[mw] : 1.0);
           }
@@ -536,7 +536,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
           acc = 0.0;
           cur = row;
         }
-        acc = fma(w.G[g], eff[gm[g] * ns + j], acc);
+        acc = fma(w.G[g], eff[gm[g] * eff_stride(ns) + j], acc);
       }
       if (ng > 0) w.mat[cur * rs + j] += acc;
     }
@@ -570,7 +570,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   for (int half = 0; half < 2; ++half) {
     const int k = lane + 32 * half;
     if (k < ns) {
-      const double* a = th + 24 * k + toff;
+      const double* a = th + kThStride * k + toff;
       const double cpk = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
       const double hk = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
       const double dcp = a[0] * (a[8] + T * (2.0 * a[9] + T * (3.0 * a[10] + T * (4.0 * a[11]))));

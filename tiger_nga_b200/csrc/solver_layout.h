@@ -9,10 +9,16 @@ namespace tng {
 enum SvSize {
   SZ_NS, SZ_NV, SZ_NSLOT, SZ_NM, SZ_NFO, SZ_NFC, SZ_NCDCHUNK, SZ_NJDGRP, SZ_NGPAIR, SZ_NCDSTEP, SZ_NJDSTEP, SZ_COUNT
 };
-// hot doubles: slot records (4 per slot: lnA|A, E, n, -), falloff (6: lnA0 E0 n0 lnAi Ei ni),
-// F_cent (6: a0 c0 a1 c1 a2 c2), dense efficiencies (nm x ns), thermo (ns x 24: hi 12, lo 12),
-// molar masses, their inverses, scalars
+// hot doubles: plain-slot records (kSlotRec per plain slot, from position NFO: lnA|A, E, n),
+// falloff (kFoRec: lnA0 E0 n0 lnAi Ei ni, pad), F_cent (kFcRec: a0 c0 a1 c1 a2 c2, pad), dense
+// efficiencies (nm rows of eff_stride(ns)), thermo (ns rows of kThStride: hi 12, lo 12, pad),
+// molar masses, their inverses, scalars.
+// The record strides are odd: lanes that read the same field of consecutive records then hit 16
+// distinct bank pairs per half-warp (an even stride such as 24 or 36 doubles puts eight lanes of a
+// half-warp on one bank pair).
 enum SvHd { HD_SLOT, HD_FO, HD_FC, HD_EFF, HD_TH, HD_WMOL, HD_INVW, HD_SCAL, HD_COUNT };
+constexpr int kSlotRec = 3, kFoRec = 7, kFcRec = 7, kThStride = 25;
+__host__ __device__ constexpr int eff_stride(int ns) { return ns | 1; }
 // hot ints: slot words (2 per slot: flags|r0<<4|r1<<11|r2<<18, mw|fo<<8), falloff word
 // (f0|f1<<4|(fc+1)<<8|m<<16), F_cent forms, chunks per species, and the production-rate terms
 // interleaved by lane (step s of lane L at [s*32 + L]: nu | p<<8 | last-of-chunk<<20 | chunk<<21)

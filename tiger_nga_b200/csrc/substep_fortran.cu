@@ -75,7 +75,7 @@ __global__ void k_fortran_scatter(FortranView v, const double* __restrict__ rho,
     for (int s = 0; s < ns; ++s) {
       const double y = state[(long long)s * n + c] / r;
       spec[(long long)s * v.vol + o] = y;
-      const double* a = th + 24 * s + toff;
+      const double* a = th + kThStride * s + toff;
       cpm += y * (a[0] * (a[7] + Tn * (a[8] + Tn * (a[9] + Tn * (a[10] + Tn * a[11])))));
     }
     temp[o] = Tn;

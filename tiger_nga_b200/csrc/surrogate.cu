@@ -65,14 +65,14 @@ struct SurPost {
 constexpr int kIndicators = 5;
 
 __device__ __forceinline__ void nasa(const double* th, double tmid, int k, double T, double* h, double* cp) {
-  const double* a = th + 24 * k + (T > tmid ? 0 : 12);
+  const double* a = th + kThStride * k + (T > tmid ? 0 : 12);
   *cp = a[0] * (a[7] + T * (a[8] + T * (a[9] + T * (a[10] + T * a[11]))));
   *h = a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
 }
 
 // the enthalpy alone (the same expression as nasa's h)
 __device__ __forceinline__ double nasa_h(const double* th, double tmid, int k, double T) {
-  const double* a = th + 24 * k + (T > tmid ? 0 : 12);
+  const double* a = th + kThStride * k + (T > tmid ? 0 : 12);
   return a[0] * (T * (a[1] + T * (a[2] + T * (a[3] + T * (a[4] + T * a[5])))) + a[6]);
 }
 
@@ -327,7 +327,7 @@ __device__ double enthalpy_T(const SurPost& a, const CellY& Y0, const double* dY
 #pragma unroll
       for (int i = 0; i < 5; ++i) cc[i] = 0.0;
       for (int k = 0; k < a.ns; ++k) {
-        const double* t = a.th + 24 * k + 12 * r;
+        const double* t = a.th + kThStride * k + 12 * r;
         const double w = y_new(Y0, dY, k, inv_sum) * t[0];
 #pragma unroll
         for (int i = 0; i < 6; ++i) ch[i] = fma(w, t[1 + i], ch[i]);
