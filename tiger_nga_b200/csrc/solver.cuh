@@ -318,7 +318,8 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
   static_assert(SvT<LY>::NV * SvT<LY>::RS >= SvT<LY>::NSLOT + SvT<LY>::NFO, "kept constants fit the matrix area");
   const WarpMem w = warp_mem<LY>(wb);
   const CellPrep c = prepare(t, w, y0, y1, p, lane);
-  const int* sw = t.i(HI_SLOT);
+  static_assert(LY::hi(HI_SLOT) % 2 == 0, "slot words are read as int2");
+  const int2* sw = reinterpret_cast<const int2*>(t.i(HI_SLOT));  // (w0, w1) per slot, one 8-byte read
   auto mass_action = [&](double v, const int w0, const int w1) {
     const int r0 = (w0 >> 4) & 127, r1 = (w0 >> 11) & 127, r2 = (w0 >> 18) & 127, mw = w1 & 127;
     if (r0 != kNone7) v = v * w.C[r0];
@@ -333,7 +334,8 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
   // and every unrolled copy measured slower than the rolled loop (the latency it hides for one
   // warp is hidden by the other warps)
   for (int q = lane; q < SvT<LY>::NFO; q += 32) {
-    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
+    const int2 sq = sw[q];
+    const int w0 = sq.x, w1 = sq.y;
     double pr = 0.0;
     const double k = falloff_const(t, w, c, w1, &pr);
     w.W[q] = mass_action(k, w0, w1);
@@ -344,7 +346,8 @@ static __device__ __noinline__ void prep_rates(const SvT<LY> t, double* wb, cons
   }
 #pragma unroll 1
   for (int q = SvT<LY>::NFO + lane; q < SvT<LY>::NSLOT; q += 32) {
-    const int w0 = sw[2 * q], w1 = sw[2 * q + 1];
+    const int2 sq = sw[q];
+    const int w0 = sq.x, w1 = sq.y;
     const double k = plain_const(t, c, q, w0);
     w.W[q] = mass_action(k, w0, w1);
     if (keep) w.mat[q] = k;
@@ -447,7 +450,7 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   for (int q = lane; q < SvT<LY>::NFO; q += 32) w.pr[q] = w.mat[SvT<LY>::NSLOT + q];
   __syncwarp();
   const CellPrep c = load_prep(w);
-  const int* sw = t.i(HI_SLOT);
+  const int2* sw = reinterpret_cast<const int2*>(t.i(HI_SLOT));
 #pragma unroll 1
   for (int e = lane; e < nv * rs; e += 32) w.mat[e] = 0.0;
   __syncwarp();
@@ -491,7 +494,8 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
       for (int q = gb[g]; q < ge[g]; ++q) {
         const int term = gt[q];
         const int pp = term >> 12, kind = (term >> 8) & 15;
-        const int w0 = sw[2 * pp], w1 = sw[2 * pp + 1];
+        const int2 sq = sw[pp];
+        const int w0 = sq.x, w1 = sq.y;
         double prodC = 1.0;
 #pragma unroll
         for (int o = 0; o < 3; ++o) {
@@ -710,7 +714,11 @@ static __device__ __noinline__ int lu_call(double* wb, const int lane) {
 }
 
 // Solve (LU) x = b with b and x two entries per lane in registers: permutation by one gather,
-// forward and backward substitution by shuffles (no shared-memory round trips per step).
+// forward and backward substitution by shuffles (no shared-memory round trips per step). Each
+// substitution runs in two parts, over the pivots held in b0 (k < 32) and in b1 (k >= 32): the
+// rows a pivot updates are then known per part (in the forward pass the pivots k >= 32 touch
+// only rows of b1, in the backward pass the pivots k < 32 only rows of b0), and no part pays
+// for the other's predicated-off loads and FMAs. The arithmetic per entry is unchanged.
 __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const int rs, const int* perm,
                                              const double* dinv, double* vb, double& x0, double& x1, const int lane) {
   const int i0 = lane, i1 = lane + 32;
@@ -720,19 +728,30 @@ __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const
   double b0 = i0 < n ? vb[perm[i0]] : 0.0;
   double b1 = i1 < n ? vb[perm[i1]] : 0.0;
   __syncwarp();
+  const int nlo = n - 1 < 32 ? n - 1 : 32;  // forward pivots held in b0
 #pragma unroll 1
-  for (int k = 0; k < n - 1; ++k) {
-    const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31);
+  for (int k = 0; k < nlo; ++k) {
+    const double bk = __shfl_sync(kFull, b0, k);
     if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
+  }
+#pragma unroll 1
+  for (int k = 32; k < n - 1; ++k) {
+    const double bk = __shfl_sync(kFull, b1, k - 32);
     if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
 #pragma unroll 1
-  for (int k = n - 1; k >= 0; --k) {
-    const double bk = __shfl_sync(kFull, k < 32 ? b0 : b1, k & 31) * dinv[k];
-    if (i0 == k) b0 = bk;
+  for (int k = n - 1; k >= 32; --k) {
+    const double bk = __shfl_sync(kFull, b1, k - 32) * dinv[k];
     if (i1 == k) b1 = bk;
-    if (i0 < k) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
     if (i1 < k) b1 = fma(-a[i1 * rs + k], bk, b1);
+  }
+#pragma unroll 1
+  for (int k = (n - 1 < 31 ? n - 1 : 31); k >= 0; --k) {
+    const double bk = __shfl_sync(kFull, b0, k) * dinv[k];
+    if (i0 == k) b0 = bk;
+    if (i0 < k) b0 = fma(-a[i0 * rs + k], bk, b0);
   }
   x0 = b0;
   x1 = b1;
