@@ -374,21 +374,29 @@ __device__ __forceinline__ void rhs_warp(const SvT<LY>& t, const WarpMem& w, con
   {
     // production-rate chunks: every lane walks the same number of steps over its interleaved
     // terms (conflict-free term reads, compile-time trip count) and stores a chunk's sum at the
-    // chunk's last term
-    // (the chunk sums go to a region the walk never reads: distinct restrict pointers let the
-    // loads of later steps move ahead of the stores)
-    const int* __restrict__ ct = t.i(HI_CD_IL) + lane;
-    const double* __restrict__ Wr = w.W;
-    double* __restrict__ part = w.part;
-    double acc = 0.0;
+    // chunk's last term. The walk is software-pipelined: the term of step st+2 and the rate of
+    // step st+1 are requested before step st's arithmetic, so that a step waits on neither of
+    // its two dependent shared-memory reads (with two warps per scheduler the walk is bound by
+    // that latency, not by issue). The chunk sums go to a region the walk never reads.
+    constexpr int nst = SvT<LY>::NCDSTEP;
+    if constexpr (nst > 0) {
+      const int* __restrict__ ct = t.i(HI_CD_IL) + lane;
+      const double* __restrict__ Wr = w.W;
+      double* __restrict__ part = w.part;
+      double acc = 0.0;
+      int term = ct[0];
+      double wv = Wr[(term >> 8) & 4095];
+      int tn = nst > 1 ? ct[32] : 0;
 #pragma unroll 1
-    for (int st = 0; st < SvT<LY>::NCDSTEP; ++st) {
-      const int term = ct[32 * st];
-      const double wv = Wr[(term >> 8) & 4095];
-      if (term & 0xFF) acc = fma((double)nu_of(term), wv, acc);  // nu = 0: a padding step
-      if (term & (1 << 20)) {
-        part[(unsigned)term >> 21] = acc;
-        acc = 0.0;
+      for (int st = 0; st < nst; ++st) {
+        const double wn = Wr[(tn >> 8) & 4095];
+        const int tnn = st + 2 < nst ? ct[32 * (st + 2)] : 0;
+        if (term & 0xFF) acc = fma((double)nu_of(term), wv, acc);  // nu = 0: a padding step
+        if (term & (1 << 20)) {
+          part[(unsigned)term >> 21] = acc;
+          acc = 0.0;
+        }
+        term = tn, wv = wn, tn = tnn;
       }
     }
   }
@@ -456,29 +464,44 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   __syncwarp();
   // direct mass-action part: nu dW_p/dC_j for every reactant occurrence, the terms of one matrix
   // entry summed by one lane; the terms are interleaved by lane with the other reactants decoded
-  // at generation time, so a step is one 8-byte term read and up to four independent loads
-  {
-    // (the matrix region never overlaps the slot, concentration and third-body regions read
-    // here: distinct restrict pointers let the loads of later steps move ahead of the stores)
+  // at generation time, so a step is one 8-byte term read and up to four independent loads.
+  // Software-pipelined like the production-rate walk: the operands of step st+1 and the term of
+  // step st+2 are requested before step st's arithmetic. An absent factor is read as 1.0 (a
+  // product with 1.0 is exact, so the value is that of the skipped multiplication).
+  constexpr int njs = SvT<LY>::NJDSTEP;
+  if constexpr (njs > 0) {
+    // (the matrix region never overlaps the slot, concentration and third-body regions read here)
     const int2* __restrict__ jt = reinterpret_cast<const int2*>(t.c(CI_JD_IL)) + lane;
     const double* __restrict__ Wr = w.W;
     const double* __restrict__ Cr = w.C;
     const double* __restrict__ Mr = w.Ms;
     double* __restrict__ mat = w.mat;
-    double acc = 0.0;
-#pragma unroll 1
-    for (int st = 0; st < SvT<LY>::NJDSTEP; ++st) {
-      const int2 tm = jt[32 * st];
+    const int2 pad = make_int2(kNone7 << 10 | kNone7 << 17 | kNone7 << 24, 0);
+    auto operands = [&](const int2 tm, double& wv, double& ca, double& cb, double& mm) {
       const int pa = tm.x & 1023, ra = (tm.x >> 10) & 127, rb = (tm.x >> 17) & 127, mw = (tm.x >> 24) & 127;
-      double d = Wr[pa];
-      if (ra != kNone7) d *= Cr[ra];
-      if (rb != kNone7) d *= Cr[rb];
-      if (mw != kNone7) d *= Mr[mw];
+      wv = Wr[pa];
+      ca = ra != kNone7 ? Cr[ra] : 1.0;
+      cb = rb != kNone7 ? Cr[rb] : 1.0;
+      mm = mw != kNone7 ? Mr[mw] : 1.0;
+    };
+    double acc = 0.0;
+    int2 tm = jt[0];
+    double wv, ca, cb, mm;
+    operands(tm, wv, ca, cb, mm);
+    int2 tn = njs > 1 ? jt[32] : pad;
+#pragma unroll 1
+    for (int st = 0; st < njs; ++st) {
+      double wv1, ca1, cb1, mm1;
+      operands(tn, wv1, ca1, cb1, mm1);
+      const int2 tnn = st + 2 < njs ? jt[32 * (st + 2)] : pad;
+      const double d = ((wv * ca) * cb) * mm;
       if (tm.y & 0xFF) acc = fma((double)nu_of(tm.y), d, acc);  // nu = 0: a padding step
       if (tm.y & (1 << 20)) {
         mat[(tm.y >> 8) & 4095] = acc;
         acc = 0.0;
       }
+      tm = tn, tn = tnn;
+      wv = wv1, ca = ca1, cb = cb1, mm = mm1;
     }
   }
   // third-body and falloff-[M] part: G[i][m] = sum_p nu_ip dW_p/dM_m
@@ -718,40 +741,65 @@ static __device__ __noinline__ int lu_call(double* wb, const int lane) {
 // substitution runs in two parts, over the pivots held in b0 (k < 32) and in b1 (k >= 32): the
 // rows a pivot updates are then known per part (in the forward pass the pivots k >= 32 touch
 // only rows of b1, in the backward pass the pivots k < 32 only rows of b0), and no part pays
-// for the other's predicated-off loads and FMAs. The arithmetic per entry is unchanged.
+// for the other's predicated-off loads and FMAs. The loops are software-pipelined: the matrix
+// entries (and pivot reciprocal) of the next column are read before this column's shuffle and
+// FMAs, so the chain per column is the shuffle and the FMA alone. The arithmetic per entry is
+// unchanged.
 __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const int rs, const int* perm,
                                              const double* dinv, double* vb, double& x0, double& x1, const int lane) {
   const int i0 = lane, i1 = lane + 32;
-  if (i0 < n) vb[i0] = x0;
-  if (i1 < n) vb[i1] = x1;
+  const bool r0 = i0 < n, r1 = i1 < n;
+  if (r0) vb[i0] = x0;
+  if (r1) vb[i1] = x1;
   __syncwarp();
-  double b0 = i0 < n ? vb[perm[i0]] : 0.0;
-  double b1 = i1 < n ? vb[perm[i1]] : 0.0;
+  double b0 = r0 ? vb[perm[i0]] : 0.0;
+  double b1 = r1 ? vb[perm[i1]] : 0.0;
   __syncwarp();
+  const double* a0 = a + i0 * rs;  // this lane's rows
+  const double* a1 = a + i1 * rs;
   const int nlo = n - 1 < 32 ? n - 1 : 32;  // forward pivots held in b0
+  double p0 = r0 ? a0[0] : 0.0, p1 = r1 ? a1[0] : 0.0;  // column k of the two rows
 #pragma unroll 1
   for (int k = 0; k < nlo; ++k) {
+    const double q0 = r0 ? a0[k + 1] : 0.0, q1 = r1 ? a1[k + 1] : 0.0;
     const double bk = __shfl_sync(kFull, b0, k);
-    if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
-    if (i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
+    if (i0 > k && r0) b0 = fma(-p0, bk, b0);
+    if (r1) b1 = fma(-p1, bk, b1);
+    p0 = q0, p1 = q1;
   }
 #pragma unroll 1
-  for (int k = 32; k < n - 1; ++k) {
+  for (int k = 32; k < n - 1; ++k) {  // p1 holds column k
+    const double q1 = r1 ? a1[k + 1] : 0.0;
     const double bk = __shfl_sync(kFull, b1, k - 32);
-    if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
+    if (i1 > k && r1) b1 = fma(-p1, bk, b1);
+    p1 = q1;
   }
+  if (n - 1 >= 32) {
+    int k = n - 1;
+    p0 = r0 ? a0[k] : 0.0, p1 = r1 ? a1[k] : 0.0;
+    double dk = dinv[k];
 #pragma unroll 1
-  for (int k = n - 1; k >= 32; --k) {
-    const double bk = __shfl_sync(kFull, b1, k - 32) * dinv[k];
-    if (i1 == k) b1 = bk;
-    if (i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
-    if (i1 < k) b1 = fma(-a[i1 * rs + k], bk, b1);
+    for (; k >= 32; --k) {
+      const double q0 = r0 ? a0[k - 1] : 0.0, q1 = r1 ? a1[k - 1] : 0.0, dq = dinv[k - 1];
+      const double bk = __shfl_sync(kFull, b1, k - 32) * dk;
+      if (i1 == k) b1 = bk;
+      if (r0) b0 = fma(-p0, bk, b0);
+      if (i1 < k) b1 = fma(-p1, bk, b1);
+      p0 = q0, p1 = q1, dk = dq;
+    }
   }
+  {
+    int k = n - 1 < 31 ? n - 1 : 31;
+    p0 = r0 ? a0[k] : 0.0;
+    double dk = dinv[k];
 #pragma unroll 1
-  for (int k = (n - 1 < 31 ? n - 1 : 31); k >= 0; --k) {
-    const double bk = __shfl_sync(kFull, b0, k) * dinv[k];
-    if (i0 == k) b0 = bk;
-    if (i0 < k) b0 = fma(-a[i0 * rs + k], bk, b0);
+    for (; k >= 0; --k) {
+      const double q0 = (r0 && k > 0) ? a0[k - 1] : 0.0, dq = k > 0 ? dinv[k - 1] : 0.0;
+      const double bk = __shfl_sync(kFull, b0, k) * dk;
+      if (i0 == k) b0 = bk;
+      if (i0 < k) b0 = fma(-p0, bk, b0);
+      p0 = q0, dk = dq;
+    }
   }
   x0 = b0;
   x1 = b1;
