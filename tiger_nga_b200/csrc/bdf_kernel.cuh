@@ -162,8 +162,8 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
     q = (int)s[5], qwait = (int)s[6], qprev = (int)s[7], nst = (int)s[8], nni = (int)s[9], nje = (int)s[10];
     need_j = 1;
     nst_lu = nst;
-    ewt[0] = h0 ? 1.0 / (rtol * fabs(z[0][0]) + atol) : 0.0;
-    ewt[1] = h1 ? 1.0 / (rtol * fabs(z[0][1]) + atol) : 0.0;
+    ewt[0] = h0 ? div_ool(1.0, rtol * fabs(z[0][0]) + atol) : 0.0;
+    ewt[1] = h1 ? div_ool(1.0, rtol * fabs(z[0][1]) + atol) : 0.0;
   } else {
     const long long ld = a.ld;
     const double u0 = h0 ? a.state[(long long)lane * ld + cell] : 0.0;
@@ -171,8 +171,8 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
     z[0][0] = u0;
     z[0][1] = u1;
     if (!(dt > 0.0)) goto finish;
-    ewt[0] = h0 ? 1.0 / (rtol * fabs(u0) + atol) : 0.0;
-    ewt[1] = h1 ? 1.0 / (rtol * fabs(u1) + atol) : 0.0;
+    ewt[0] = h0 ? div_ool(1.0, rtol * fabs(u0) + atol) : 0.0;
+    ewt[1] = h1 ? div_ool(1.0, rtol * fabs(u1) + atol) : 0.0;
     {
       const double2 r = rhs_call(t, w.mat, u0, u1, p, lane);
       f[0] = r.x, f[1] = r.y;
@@ -219,7 +219,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         return false;
       }
       if (tcur + h > dt) {
-        const double eta = (dt - tcur) / h;
+        const double eta = div_ool(dt - tcur, h);
         z_rescale(z, q, eta);
         h = dt - tcur;
       }
@@ -237,7 +237,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         const double gamma = h * l0;
         bool conv_fail = false;
         bool jcur = false;
-        if (need_j || nst >= nst_lu + msbp || fabs(gamma / gamma_lu - 1.0) > dgmax) {
+        if (need_j || nst >= nst_lu + msbp || fabs(div_ool(gamma, gamma_lu) - 1.0) > dgmax) {
           {
             const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane, 1);  // keeps the rate constants
             f[0] = r.x, f[1] = r.y;
@@ -278,7 +278,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             if (!h0) x[0] = 0.0;
             if (!h1) x[1] = 0.0;
             if (gamma != gamma_lu) {
-              const double cf = 2.0 / (1.0 + gamma / gamma_lu);
+              const double cf = div_ool(2.0, 1.0 + div_ool(gamma, gamma_lu));
               x[0] *= cf;
               x[1] *= cf;
             }
@@ -288,8 +288,8 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             y[1] = z[0][1] + l0 * acor[1];
             const double del = wrms2(x[0], x[1], ewt[0], ewt[1], nv, lane);
             if (!isfinite(del)) break;
-            if (it > 0) crate = fmax(0.3 * crate, del / delp);
-            const double dcon = del * fmin(1.0, crate) * C.errc[q] / 0.1;
+            if (it > 0) crate = fmax(0.3 * crate, div_ool(del, delp));
+            const double dcon = div_ool(del * fmin(1.0, crate) * C.errc[q], 0.1);
             if (dcon <= 1.0) {
               conv_fail = false;
               break;
@@ -337,7 +337,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             qprev = 0;
             continue;
           }
-          double eta = 1.0 / (bdf_pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+          double eta = div_ool(1.0, bdf_pow(6.0 * dsm, div_ool(1.0, q + 1)) + 1e-6);
           eta = fmax(0.1, fmin(0.9, eta));
           if (nef >= 2) eta = fmin(eta, 0.2);
           z_rescale(z, q, eta);
@@ -361,26 +361,30 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         status = ST_NONFINITE;
         break;
       }
-      ewt[0] = h0 ? 1.0 / (rtol * fabs(z[0][0]) + atol) : 0.0;
-      ewt[1] = h1 ? 1.0 / (rtol * fabs(z[0][1]) + atol) : 0.0;
+      {
+        const double e0 = div_ool(1.0, rtol * fabs(z[0][0]) + atol);
+        const double e1 = div_ool(1.0, rtol * fabs(z[0][1]) + atol);
+        ewt[0] = h0 ? e0 : 0.0;
+        ewt[1] = h1 ? e1 : 0.0;
+      }
       if (tcur >= dt) break;
       --qwait;
-      const double eta_q = 1.0 / (bdf_pow(6.0 * dsm, 1.0 / (q + 1)) + 1e-6);
+      const double eta_q = div_ool(1.0, bdf_pow(6.0 * dsm, div_ool(1.0, q + 1)) + 1e-6);
       double eta_m = 0.0, eta_p = 0.0;
       if (qwait <= 0) {
         if (q > 1) {
           const double ddn = C.dnc[q] * wrms2(zget(z, q, 0), zget(z, q, 1), ewt[0], ewt[1], nv, lane);
-          eta_m = 1.0 / (bdf_pow(6.0 * ddn, 1.0 / q) + 1e-6);
+          eta_m = div_ool(1.0, bdf_pow(6.0 * ddn, div_ool(1.0, q)) + 1e-6);
         }
         if (q < kQmax && qprev == q) {
-          double r = h / hprev;  // (h / hprev)^(q + 1)
+          double r = div_ool(h, hprev);  // (h / hprev)^(q + 1)
           {
             const double b = r;
             for (int i = 1; i <= q; ++i) r *= b;
           }
           const double dup =
               C.upc[q] * wrms2(acor[0] - r * acorp[0], acor[1] - r * acorp[1], ewt[0], ewt[1], nv, lane);
-          eta_p = 1.0 / (bdf_pow(10.0 * dup, 1.0 / (q + 2)) + 1e-6);
+          eta_p = div_ool(1.0, bdf_pow(10.0 * dup, div_ool(1.0, q + 2)) + 1e-6);
         }
       }
       double eta = eta_q;
@@ -405,7 +409,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
       qprev = q;
       hprev = h;
       if (newq == q + 1) {
-        const double c = C.L[q][q] / (q + 1);
+        const double c = div_ool(C.L[q][q], q + 1);
         zset(z, q + 1, 0, c * acor[0]);
         zset(z, q + 1, 1, c * acor[1]);
         q = q + 1;
@@ -514,7 +518,8 @@ inline cudaError_t ensure_dynamic_smem(const void* kernel, size_t bytes) {
 }
 
 // The solver kernels of one mechanism (instantiated in the mechanism's generated unit and
-// reached through its operation table).
+// reached through its operation table): two sets, [0] with FP64 rate-constant exponentials and
+// [1] with the mixed form (solver_kernels_for picks by the handle's precision).
 typedef void (*BdfKernelFn)(const BdfLaunch);
 typedef void (*RhsJacFn)(SvDev, const double*, long long, int, double, double*, double*, int);
 struct SolverKernels {
@@ -522,10 +527,20 @@ struct SolverKernels {
   RhsJacFn rhs_jac4;
 };
 
+template <class LX>
+constexpr SolverKernels solver_kernel_set() {
+  return {k_bdf<LX, 2>, k_bdf<LX, 4>, k_bdf<LX, 8>, k_bdf<LX, 8, 2>, k_warp_rhs_jac<LX, 4>};
+}
+
 template <class LY>
 const SolverKernels* solver_kernels() {
-  static const SolverKernels k = {k_bdf<LY, 2>, k_bdf<LY, 4>, k_bdf<LY, 8>, k_bdf<LY, 8, 2>, k_warp_rhs_jac<LY, 4>};
-  return &k;
+  static const SolverKernels k[2] = {solver_kernel_set<SvLX<LY, 0>>(), solver_kernel_set<SvLX<LY, 1>>()};
+  return k;
+}
+
+// The kernel set for a precision flag (SvDev::mixed).
+inline const SolverKernels* solver_kernels_for(const SolverKernels* sets, const int mixed) {
+  return sets + (mixed ? 1 : 0);
 }
 
 static __global__ void k_reset_counters(int* a, int* b) {

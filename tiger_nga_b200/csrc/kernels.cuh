@@ -85,7 +85,7 @@ struct MechOps {
   const double* sv_hd[2];  // hot doubles per literal mode
   const int* sv_hi;        // hot ints
   const int* sv_ci;        // cold ints
-  const SolverKernels* sk;  // the implicit solver's kernels, specialised on this mechanism
+  const SolverKernels* sk;  // the implicit solver's kernels, specialised on this mechanism: [0] FP64, [1] mixed
   // mixture properties: lm 0/1, what = TNG_PROPS_* bits (density alone, or viscosity and/or diffusivity)
   cudaError_t (*props)(int lm, int what, const PropsArgs& a, int sm_count, cudaStream_t st);
 };

@@ -118,7 +118,7 @@ static int ensure_tables(tng_chem* h) {
 
 // occ 2 (with 8 warps): launch bounds for two blocks per SM (registers capped at 128)
 static BdfKernelFn bdf_kernel(const tng_chem* h, int warps, int occ = 1) {
-  const SolverKernels* k = h->ops->sk;
+  const SolverKernels* k = solver_kernels_for(h->ops->sk, h->cfg.precision == TNG_MIXED);
   if (warps == 8 && occ == 2) return k->bdf8_occ2;
   switch (warps) {
     case 2:
@@ -419,7 +419,7 @@ extern "C" int tng_solver_rhs_jac(tng_chem* h, const double* state, int64_t ncel
   if (rc) return rc;
   SolverState* s = h->solver;
   const size_t smem = block_smem(s, 4, 0);
-  const RhsJacFn kern = h->ops->sk->rhs_jac4;
+  const RhsJacFn kern = solver_kernels_for(h->ops->sk, h->cfg.precision == TNG_MIXED)->rhs_jac4;
   cudaError_t e = ensure_dynamic_smem((const void*)kern, smem);
   if (e != cudaSuccess) return cuda_error(e, "solver shared memory");
   const int blocks = (int)std::min<int64_t>((ncells + 3) / 4, 148 * 8);

@@ -39,7 +39,15 @@ struct SvDev {
   const int* __restrict__ hi;     // hot ints
   const int* __restrict__ ci;     // cold ints
   SvLayout L;
-  int mixed;  // rate-constant exponentials on the FP32 special-function unit (see rexp)
+  int mixed;  // rate-constant exponentials on the FP32 special-function unit (selects the kernels)
+};
+
+// A mechanism's layout with the precision of the rate-constant exponentials (kMixed: 0 FP64, 1 the
+// mixed form) as a compile-time constant: the solver's kernels are instantiated on SvLX<LY, 0> and
+// SvLX<LY, 1>, and the host picks by the handle's precision.
+template <class LY, int MIX>
+struct SvLX : LY {
+  static constexpr int kMixed = MIX;
 };
 
 // Table view inside a kernel, specialised on the mechanism's layout LY (generated SvL_<m>: the
@@ -56,7 +64,6 @@ struct SvT {
   const double* __restrict__ hd;
   const int* __restrict__ hi;
   const int* __restrict__ ci;
-  int mixed;
   __device__ __forceinline__ const double* d(int k) const { return hd + LY::hd(k); }
   __device__ __forceinline__ const int* i(int k) const { return hi + LY::hi(k); }
   __device__ __forceinline__ const int* c(int k) const { return ci + LY::ci(k); }
@@ -81,7 +88,6 @@ __device__ __forceinline__ SvT<LY> stage_tables(const SvDev& g, void* smem) {
   t.hd = d;
   t.hi = i;
   t.ci = g.ci;
-  t.mixed = g.mixed;
   return t;
 }
 
@@ -195,6 +201,9 @@ __device__ __forceinline__ int nu_of(const int term) { return (int)(int8_t)(term
 // warps stalled on instruction fetch.
 static __device__ __noinline__ double exp_ool(const double x) { return exp(x); }
 static __device__ __noinline__ double log_ool(const double x) { return log(x); }
+// IEEE division out of line, for the integrator's step control: inlined, each of its two dozen
+// divisions carried its own reciprocal sequence (the quotient is correctly rounded either way)
+static __device__ __noinline__ double div_ool(const double a, const double b) { return a / b; }
 
 // exp in mixed precision: 2^x split into an exact power of two (FP64 scaling) and a fraction in
 // [0, 1) evaluated by the FP32 ex2 unit, relative error about 3e-7.
@@ -205,12 +214,16 @@ static __device__ __noinline__ double exp_mixed_ool(const double e) {
   return ldexp((double)tng_ex2f((float)(x - n)), (int)fmin(n, 1100.0));
 }
 
-// exp of a rate-constant exponent in the handle's precision (FP64, or the mixed form above). The
-// exponent itself (ln A + n ln T - E/RT, where the reverse rates' cancellations sit) is always
-// formed in FP64.
+// exp of a rate-constant exponent in the kernel's precision (FP64, or the mixed form above),
+// fixed at compile time by the layout (SvLX): a kernel carries the code of one form only, which
+// keeps the other out of its instruction cache. The exponent itself (ln A + n ln T - E/RT, where
+// the reverse rates' cancellations sit) is always formed in FP64.
 template <class LY>
-__device__ __forceinline__ double rexp(const SvT<LY>& t, const double e) {
-  return t.mixed ? exp_mixed_ool(e) : exp_ool(e);
+__device__ __forceinline__ double rexp(const SvT<LY>&, const double e) {
+  if constexpr (LY::kMixed)
+    return exp_mixed_ool(e);
+  else
+    return exp_ool(e);
 }
 
 // Per-cell thermochemical state shared by the rate and Jacobian evaluations.
@@ -241,9 +254,12 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
   __syncwarp();
   const double prt = p * c.invRT;  // [M] of the ideal gas, for a third-body sum that is zero
   const double* eff = t.d(HD_EFF);
+  // (the loops of the cell preparation stay rolled: fully unrolled they made up a third of the
+  // right-hand side's code)
   for (int m = lane; m < nm; m += 32) {
     const double* e = eff + m * eff_stride(ns);
     double acc = 0.0;
+#pragma unroll 4
     for (int j = 0; j < ns; ++j) acc = fma(e[j], w.C[j], acc);
     w.Ms[m] = acc;
     w.lcm[m] = log_ool(acc > 0.0 ? acc : prt);
@@ -253,7 +269,7 @@ __device__ __forceinline__ CellPrep prepare(const SvT<LY>& t, const WarpMem& w, 
   for (int f = lane; f < nfc; f += 32) {
     const int forms = fcf[f];
     double v = 0.0;
-#pragma unroll
+#pragma unroll 1
     for (int q = 0; q < 3; ++q) {
       const int form = (forms >> (4 * q)) & 15;
       if (form == 15) break;

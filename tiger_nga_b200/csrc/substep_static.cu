@@ -178,7 +178,7 @@ extern "C" int tng_substep_batch_static(tng_chem* h, double* state, int64_t ncel
   a.rs = (nv % 2 == 0) ? nv + 1 : nv;
   a.smem_warp = (warp_mem_doubles(L, a.rs) + 3) & ~3;
   const size_t smem = ((size_t)hot_smem_doubles(L) + (size_t)warps * a.smem_warp) * sizeof(double);
-  const SolverKernels* sk = o->sk;
+  const SolverKernels* sk = solver_kernels_for(o->sk, a.tab.mixed);
   const BdfKernelFn kern = warps == 2 ? sk->bdf2 : warps == 4 ? sk->bdf4 : sk->bdf8;
   e = ensure_dynamic_smem((const void*)kern, smem);
   if (e != cudaSuccess) return cuda_error(e, "tng_substep_batch_static: shared memory");
