@@ -259,6 +259,8 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         }
         if (!conv_fail) {
           double delp = 0.0;
+          // correction scale for a factorisation made at another gamma (fixed over the attempt)
+          const double cf = gamma != gamma_lu ? div_ool(2.0, 1.0 + div_ool(gamma, gamma_lu)) : 1.0;
           acor[0] = acor[1] = 0.0;
           y[0] = z[0][0];
           y[1] = z[0][1];
@@ -278,7 +280,6 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             if (!h0) x[0] = 0.0;
             if (!h1) x[1] = 0.0;
             if (gamma != gamma_lu) {
-              const double cf = div_ool(2.0, 1.0 + div_ool(gamma, gamma_lu));
               x[0] *= cf;
               x[1] *= cf;
             }

@@ -565,23 +565,32 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
     const int* gm = t.c(CI_G_M);
     const double* eff = t.d(HD_EFF);
     // the pairs are sorted by row: each row's contributions are summed in a register and added
-    // to the matrix once (no read-modify-write chain through shared memory per pair); the loops
-    // stay rolled (fully unrolled over the pairs they were a sixth of the solver's code)
-#pragma unroll 1
-    for (int j = lane; j < ns; j += 32) {
+    // to the matrix once (no read-modify-write chain through shared memory per pair); the loop
+    // stays rolled (fully unrolled over the pairs it was a sixth of the solver's code). One pass
+    // over the pairs serves all columns: lane j takes column j and, when there are more than 32
+    // species, column j + 32 with a second accumulator, so the pairs' loads and row tests are not
+    // repeated for a second round of a few columns.
+    if constexpr (ng > 0) {
+      const int j0 = lane, j1 = lane + 32;
+      const bool c0 = j0 < ns, c1 = j1 < ns;
       int cur = gi[0];
-      double acc = 0.0;
+      double acc0 = 0.0, acc1 = 0.0;
 #pragma unroll 4
       for (int g = 0; g < ng; ++g) {
         const int row = gi[g];
         if (row != cur) {
-          w.mat[cur * rs + j] += acc;
-          acc = 0.0;
+          if (c0) w.mat[cur * rs + j0] += acc0;
+          if (c1) w.mat[cur * rs + j1] += acc1;
+          acc0 = 0.0, acc1 = 0.0;
           cur = row;
         }
-        acc = fma(w.G[g], eff[gm[g] * eff_stride(ns) + j], acc);
+        const double gv = w.G[g];
+        const double* e = eff + gm[g] * eff_stride(ns);
+        if (c0) acc0 = fma(gv, e[j0], acc0);
+        if (c1) acc1 = fma(gv, e[j1], acc1);
       }
-      if (ng > 0) w.mat[cur * rs + j] += acc;
+      if (c0) w.mat[cur * rs + j0] += acc0;
+      if (c1) w.mat[cur * rs + j1] += acc1;
     }
   }
   __syncwarp();
@@ -631,22 +640,45 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
   const double fT = __shfl_sync(kFull, ns < 32 ? f0 : f1, ns & 31);
   __syncwarp();
   const double dTdu = -T / rho;
-  for (int j = lane; j < ns; j += 32) {
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // four independent chains
+  {
+    // one pass over the species rows for all columns (lane j: column j, and column j + 32 when
+    // there are more than 32 species), four independent chains per column
+    const int j0 = lane, j1 = lane + 32;
+    const bool c0 = j0 < ns, c1 = j1 < ns;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
     int k = 0;
 #pragma unroll 1
     for (; k + 3 < ns; k += 4) {
-      s0 = fma(w.hb[k], w.mat[k * rs + j], s0);
-      s1 = fma(w.hb[k + 1], w.mat[(k + 1) * rs + j], s1);
-      s2 = fma(w.hb[k + 2], w.mat[(k + 2) * rs + j], s2);
-      s3 = fma(w.hb[k + 3], w.mat[(k + 3) * rs + j], s3);
+      const double h0 = w.hb[k], h1 = w.hb[k + 1], h2 = w.hb[k + 2], h3 = w.hb[k + 3];
+      if (c0) {
+        s0 = fma(h0, w.mat[k * rs + j0], s0);
+        s1 = fma(h1, w.mat[(k + 1) * rs + j0], s1);
+        s2 = fma(h2, w.mat[(k + 2) * rs + j0], s2);
+        s3 = fma(h3, w.mat[(k + 3) * rs + j0], s3);
+      }
+      if (c1) {
+        t0 = fma(h0, w.mat[k * rs + j1], t0);
+        t1 = fma(h1, w.mat[(k + 1) * rs + j1], t1);
+        t2 = fma(h2, w.mat[(k + 2) * rs + j1], t2);
+        t3 = fma(h3, w.mat[(k + 3) * rs + j1], t3);
+      }
     }
 #pragma unroll
-    for (; k < ns; ++k) s0 = fma(w.hb[k], w.mat[k * rs + j], s0);
-    double s = (s0 + s1) + (s2 + s3);
-    s += dTdu * scp;
-    const double dcpm = (w.cb[j] - cpm) / rho + dTdu * ydcp;
-    w.mat[ns * rs + j] = -(s + fT * dcpm) / cpm;
+    for (; k < ns; ++k) {
+      if (c0) s0 = fma(w.hb[k], w.mat[k * rs + j0], s0);
+      if (c1) t0 = fma(w.hb[k], w.mat[k * rs + j1], t0);
+    }
+    const double sum0 = (s0 + s1) + (s2 + s3), sum1 = (t0 + t1) + (t2 + t3);
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      const int j = h == 0 ? j0 : j1;
+      if (j < ns) {
+        double s = h == 0 ? sum0 : sum1;
+        s += dTdu * scp;
+        const double dcpm = (w.cb[j] - cpm) / rho + dTdu * ydcp;
+        w.mat[ns * rs + j] = -(s + fT * dcpm) / cpm;
+      }
+    }
   }
   __syncwarp();
 }
