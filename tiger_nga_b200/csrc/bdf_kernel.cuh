@@ -8,6 +8,9 @@ namespace tng {
 struct BdfCoef {
   double L[kQmax + 2][kQmax + 2];
   double errc[kQmax + 2], dnc[kQmax + 2], upc[kQmax + 2];
+  // grow[e]: (2/3)^e (1 + 1e-9). For x > grow[e], x^(1/e) > 2/3 with a margin far above the
+  // rounding of the power, so the step-size candidate 1 / (x^(1/e) + 1e-6) is below 1.5
+  double grow[kQmax + 3];
 };
 
 struct BdfLaunch {
@@ -370,12 +373,15 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
       }
       if (tcur >= dt) break;
       --qwait;
-      const double eta_q = div_ool(1.0, bdf_pow(6.0 * dsm, div_ool(1.0, q + 1)) + 1e-6);
+      // A candidate below 1.5 never decides the outcome (a larger one wins, or all are below 1.5
+      // and the step is kept), so its power is skipped where the argument shows it is below 1.5.
+      const double eta_q =
+          6.0 * dsm > C.grow[q + 1] ? 0.0 : div_ool(1.0, bdf_pow(6.0 * dsm, div_ool(1.0, q + 1)) + 1e-6);
       double eta_m = 0.0, eta_p = 0.0;
       if (qwait <= 0) {
         if (q > 1) {
           const double ddn = C.dnc[q] * wrms2(zget(z, q, 0), zget(z, q, 1), ewt[0], ewt[1], nv, lane);
-          eta_m = div_ool(1.0, bdf_pow(6.0 * ddn, div_ool(1.0, q)) + 1e-6);
+          eta_m = 6.0 * ddn > C.grow[q] ? 0.0 : div_ool(1.0, bdf_pow(6.0 * ddn, div_ool(1.0, q)) + 1e-6);
         }
         if (q < kQmax && qprev == q) {
           double r = div_ool(h, hprev);  // (h / hprev)^(q + 1)
@@ -385,7 +391,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
           }
           const double dup =
               C.upc[q] * wrms2(acor[0] - r * acorp[0], acor[1] - r * acorp[1], ewt[0], ewt[1], nv, lane);
-          eta_p = div_ool(1.0, bdf_pow(10.0 * dup, div_ool(1.0, q + 2)) + 1e-6);
+          eta_p = 10.0 * dup > C.grow[q + 2] ? 0.0 : div_ool(1.0, bdf_pow(10.0 * dup, div_ool(1.0, q + 2)) + 1e-6);
         }
       }
       double eta = eta_q;

@@ -30,6 +30,7 @@ BdfCoef make_coef() {
     c.dnc[q] = q > 1 ? c.L[q - 1][0] / q * fact : 0.0;
     c.upc[q] = c.L[q + 1][0] / (q + 2) * fact * c.L[q][q];
   }
+  for (int e = 1; e <= kQmax + 2; ++e) c.grow[e] = std::pow(2.0 / 3.0, e) * (1.0 + 1e-9);
   return c;
 }
 

@@ -147,14 +147,13 @@ struct WarpMem {
   double* cb;   // 64 heat capacities (Jacobian), then the pivot reciprocals of the LU
   double* pr;   // nfo: Pr of the falloff slots (from the rate pass the Jacobian follows)
   double* cp;   // 8: the cell's CellPrep from the last rate pass
-  int* piv;     // 64 pivots
   int* perm;    // 64: the composed row permutation of the LU
 };
 
 __host__ __device__ inline int warp_mem_doubles(const SvLayout& L, int rs) {
   const int nv = L.size[SZ_NV];
   return nv * rs + L.size[SZ_NSLOT] + 64 + 2 * L.size[SZ_NM] + 3 * L.size[SZ_NFC] + L.size[SZ_NCDCHUNK] +
-         L.size[SZ_NGPAIR] + 3 * 64 + L.size[SZ_NFO] + 8 + 64 /* pivots and permutation as ints */ + 8;
+         L.size[SZ_NGPAIR] + 3 * 64 + L.size[SZ_NFO] + 8 + 32 /* the permutation as ints */ + 8;
 }
 
 template <class LY>
@@ -175,8 +174,7 @@ __device__ __forceinline__ WarpMem warp_mem(double* base) {
   w.cb = p; p += 64;
   w.pr = p; p += T::NFO;
   w.cp = p; p += 8;
-  w.piv = reinterpret_cast<int*>(p);
-  w.perm = w.piv + 64;
+  w.perm = reinterpret_cast<int*>(p);
   return w;
 }
 
@@ -689,13 +687,18 @@ __device__ __forceinline__ void jac_warp(const SvT<LY>& t, const WarpMem& w, con
 //    64-bit pattern of |a| (a non-negative double orders like its bit pattern; NaN counts as 0)
 //    instead of five rounds of shuffles;
 //  * each lane keeps the pivot-row entries of its columns in registers for the trailing update,
-//    so an update is one load and one store (4 x 8 lane tiles, rows walked at run time).
-// Returns nonzero if a pivot is zero or not finite.
+//    so an update is one load and one store (4 x 8 lane tiles, rows walked at run time);
+//  * the composed row permutation ((P b)[i] = b[perm[i]]) is kept up to date at each row exchange
+//    and the pivots' reciprocals (dinv) are stored as they are formed, so that a solve runs in
+//    registers with no pass over the factors afterwards.
+// Returns nonzero if a pivot is zero or not finite (the factors are then not used).
 template <int N, int RS>
-__device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const int lane) {
+__device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* perm, double* dinv, const int lane) {
   constexpr int NC = (N + 7) / 8;  // columns of a lane (8 column groups)
   int sing = 0;
   const int lr = lane >> 3, lc = lane & 7;
+  for (int i = lane; i < N; i += 32) perm[i] = i;
+  __syncwarp();
 #pragma unroll 1
   for (int k = 0; k < N; ++k) {
     unsigned long long key = 0ULL;
@@ -714,13 +717,18 @@ __device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const
     const unsigned mlo = __reduce_max_sync(kFull, (bi < N && khi == mhi) ? klo : 0u);
     bi = (int)__reduce_min_sync(kFull, (bi < N && khi == mhi && klo == mlo) ? (unsigned)bi : 0xffffffffu);
     if (bi >= N) bi = k;  // no row (cannot happen for k < N)
-    if (lane == 0) piv[k] = bi;
-    if (bi != k)
+    if (bi != k) {
+      if (lane == 0) {
+        const int t = perm[k];
+        perm[k] = perm[bi];
+        perm[bi] = t;
+      }
       for (int j = lane; j < N; j += 32) {
         const double tmp = a[k * RS + j];
         a[k * RS + j] = a[bi * RS + j];
         a[bi * RS + j] = tmp;
       }
+    }
     __syncwarp();
     const double d = a[k * RS + k];
     if (d == 0.0 || !isfinite(d)) {
@@ -728,6 +736,7 @@ __device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const
       continue;
     }
     const double rd = 1.0 / d;
+    if (lane == 0) dinv[k] = rd;
     for (int i = k + 1 + lane; i < N; i += 32) a[i * RS + k] *= rd;
     double u[NC];
 #pragma unroll
@@ -749,25 +758,6 @@ __device__ __forceinline__ int lu_warp_t(double* __restrict__ a, int* piv, const
   return sing;
 }
 
-// After the factorisation: the composed permutation ((P b)[i] = b[perm[i]]) and the reciprocals of the
-// pivots, so that a solve runs in registers.
-__device__ __forceinline__ void lu_finish(const double* a, const int n, const int rs, const int* piv, int* perm,
-                                          double* dinv, const int lane) {
-  if (lane == 0) {
-#pragma unroll 1
-    for (int i = 0; i < n; ++i) perm[i] = i;
-#pragma unroll 1
-    for (int k = 0; k < n; ++k) {
-      const int p = piv[k];
-      const int t = perm[k];
-      perm[k] = perm[p];
-      perm[p] = t;
-    }
-  }
-  for (int i = lane; i < n; i += 32) dinv[i] = 1.0 / a[i * rs + i];
-  __syncwarp();
-}
-
 // Out-of-line Jacobian and factorisation (one copy each, as rhs_call).
 template <class LY>
 static __device__ __noinline__ void jac_call(const SvT<LY> t, double* wb, const double y0, const double y1,
@@ -779,9 +769,7 @@ template <class LY>
 static __device__ __noinline__ int lu_call(double* wb, const int lane) {
   using T = SvT<LY>;
   const WarpMem w = warp_mem<LY>(wb);
-  const int sing = lu_warp_t<T::NV, T::RS>(w.mat, w.piv, lane);
-  lu_finish(w.mat, T::NV, T::RS, w.piv, w.perm, w.cb, lane);
-  return sing;
+  return lu_warp_t<T::NV, T::RS>(w.mat, w.perm, w.cb, lane);
 }
 
 // Solve (LU) x = b with b and x two entries per lane in registers: permutation by one gather,
