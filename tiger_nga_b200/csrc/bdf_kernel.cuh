@@ -36,6 +36,23 @@ __device__ __forceinline__ bool warp_all_finite(const double v0, const double v1
 
 #define TNG_ZLOOP(j) _Pragma("unroll") for (int j = 0; j <= kQmax + 1; ++j)
 
+// The Newton loop's two threshold tests, decided without their division unless the operands lie
+// within a relative 1e-12 of the threshold (the rounding of the quotient is far smaller, so the
+// outcome is that of the test on the rounded quotient; NaN operands take the division):
+//  * |gamma / gamma_lu - 1| > dgmax (gamma_lu > 0: a factorisation exists when this is asked);
+__device__ __forceinline__ bool gamma_moved(const double gamma, const double gamma_lu, const double dgmax) {
+  const double up = gamma_lu * (1.0 + dgmax), dn = gamma_lu * (1.0 - dgmax);
+  if (gamma > up * (1.0 + 1e-12) || gamma < dn * (1.0 - 1e-12)) return true;
+  if (gamma < up * (1.0 - 1e-12) && gamma > dn * (1.0 + 1e-12)) return false;
+  return fabs(div_ool(gamma, gamma_lu) - 1.0) > dgmax;
+}
+//  * the convergence test x / 0.1 <= 1.
+__device__ __forceinline__ bool below_tenth(const double x) {
+  if (x < 0.1 * (1.0 - 1e-12)) return true;
+  if (x > 0.1 * (1.0 + 1e-12)) return false;
+  return div_ool(x, 0.1) <= 1.0;
+}
+
 // x^y of the step-size and order selection (x >= 0, 0 < y < 1), one out-of-line copy, as
 // exp(y ln x) through the solver's own exp and log: these are step-size heuristics, and the
 // library pow (an extended-precision logarithm) cost 3 % of the solver's time
@@ -240,7 +257,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
         const double gamma = h * l0;
         bool conv_fail = false;
         bool jcur = false;
-        if (need_j || nst >= nst_lu + msbp || fabs(div_ool(gamma, gamma_lu) - 1.0) > dgmax) {
+        if (need_j || nst >= nst_lu + msbp || gamma_moved(gamma, gamma_lu, dgmax)) {
           {
             const double2 r = rhs_call(t, w.mat, z[0][0], z[0][1], p, lane, 1);  // keeps the rate constants
             f[0] = r.x, f[1] = r.y;
@@ -293,8 +310,7 @@ __device__ __forceinline__ bool bdf_cell(const BdfLaunch& P, const BdfCoef& C, c
             const double del = wrms2(x[0], x[1], ewt[0], ewt[1], nv, lane);
             if (!isfinite(del)) break;
             if (it > 0) crate = fmax(0.3 * crate, div_ool(del, delp));
-            const double dcon = div_ool(del * fmin(1.0, crate) * C.errc[q], 0.1);
-            if (dcon <= 1.0) {
+            if (below_tenth(del * fmin(1.0, crate) * C.errc[q])) {
               conv_fail = false;
               break;
             }
