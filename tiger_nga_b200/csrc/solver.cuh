@@ -777,65 +777,40 @@ static __device__ __noinline__ int lu_call(double* wb, const int lane) {
 // substitution runs in two parts, over the pivots held in b0 (k < 32) and in b1 (k >= 32): the
 // rows a pivot updates are then known per part (in the forward pass the pivots k >= 32 touch
 // only rows of b1, in the backward pass the pivots k < 32 only rows of b0), and no part pays
-// for the other's predicated-off loads and FMAs. The loops are software-pipelined: the matrix
-// entries (and pivot reciprocal) of the next column are read before this column's shuffle and
-// FMAs, so the chain per column is the shuffle and the FMA alone. The arithmetic per entry is
-// unchanged.
+// for the other's predicated-off loads and FMAs. The arithmetic per entry is unchanged.
 __device__ __forceinline__ void lu_solve_reg(const double* a, const int n, const int rs, const int* perm,
                                              const double* dinv, double* vb, double& x0, double& x1, const int lane) {
   const int i0 = lane, i1 = lane + 32;
-  const bool r0 = i0 < n, r1 = i1 < n;
-  if (r0) vb[i0] = x0;
-  if (r1) vb[i1] = x1;
+  if (i0 < n) vb[i0] = x0;
+  if (i1 < n) vb[i1] = x1;
   __syncwarp();
-  double b0 = r0 ? vb[perm[i0]] : 0.0;
-  double b1 = r1 ? vb[perm[i1]] : 0.0;
+  double b0 = i0 < n ? vb[perm[i0]] : 0.0;
+  double b1 = i1 < n ? vb[perm[i1]] : 0.0;
   __syncwarp();
-  const double* a0 = a + i0 * rs;  // this lane's rows
-  const double* a1 = a + i1 * rs;
   const int nlo = n - 1 < 32 ? n - 1 : 32;  // forward pivots held in b0
-  double p0 = r0 ? a0[0] : 0.0, p1 = r1 ? a1[0] : 0.0;  // column k of the two rows
 #pragma unroll 1
   for (int k = 0; k < nlo; ++k) {
-    const double q0 = r0 ? a0[k + 1] : 0.0, q1 = r1 ? a1[k + 1] : 0.0;
     const double bk = __shfl_sync(kFull, b0, k);
-    if (i0 > k && r0) b0 = fma(-p0, bk, b0);
-    if (r1) b1 = fma(-p1, bk, b1);
-    p0 = q0, p1 = q1;
+    if (i0 > k && i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
 #pragma unroll 1
-  for (int k = 32; k < n - 1; ++k) {  // p1 holds column k
-    const double q1 = r1 ? a1[k + 1] : 0.0;
+  for (int k = 32; k < n - 1; ++k) {
     const double bk = __shfl_sync(kFull, b1, k - 32);
-    if (i1 > k && r1) b1 = fma(-p1, bk, b1);
-    p1 = q1;
+    if (i1 > k && i1 < n) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
-  if (n - 1 >= 32) {
-    int k = n - 1;
-    p0 = r0 ? a0[k] : 0.0, p1 = r1 ? a1[k] : 0.0;
-    double dk = dinv[k];
 #pragma unroll 1
-    for (; k >= 32; --k) {
-      const double q0 = r0 ? a0[k - 1] : 0.0, q1 = r1 ? a1[k - 1] : 0.0, dq = dinv[k - 1];
-      const double bk = __shfl_sync(kFull, b1, k - 32) * dk;
-      if (i1 == k) b1 = bk;
-      if (r0) b0 = fma(-p0, bk, b0);
-      if (i1 < k) b1 = fma(-p1, bk, b1);
-      p0 = q0, p1 = q1, dk = dq;
-    }
+  for (int k = n - 1; k >= 32; --k) {
+    const double bk = __shfl_sync(kFull, b1, k - 32) * dinv[k];
+    if (i1 == k) b1 = bk;
+    if (i0 < n) b0 = fma(-a[i0 * rs + k], bk, b0);
+    if (i1 < k) b1 = fma(-a[i1 * rs + k], bk, b1);
   }
-  {
-    int k = n - 1 < 31 ? n - 1 : 31;
-    p0 = r0 ? a0[k] : 0.0;
-    double dk = dinv[k];
 #pragma unroll 1
-    for (; k >= 0; --k) {
-      const double q0 = (r0 && k > 0) ? a0[k - 1] : 0.0, dq = k > 0 ? dinv[k - 1] : 0.0;
-      const double bk = __shfl_sync(kFull, b0, k) * dk;
-      if (i0 == k) b0 = bk;
-      if (i0 < k) b0 = fma(-p0, bk, b0);
-      p0 = q0, dk = dq;
-    }
+  for (int k = (n - 1 < 31 ? n - 1 : 31); k >= 0; --k) {
+    const double bk = __shfl_sync(kFull, b0, k) * dinv[k];
+    if (i0 == k) b0 = bk;
+    if (i0 < k) b0 = fma(-a[i0 * rs + k], bk, b0);
   }
   x0 = b0;
   x1 = b1;
