@@ -312,13 +312,19 @@ __device__ __forceinline__ double falloff_const(const SvT<LY>& t, const WarpMem&
 // Rate constant of a plain (Arrhenius or constant) slot: the table holds (ln A, E, n) with zeros
 // for absent terms, so the FMA chain of expo() gives the same exponent; constant slots hold A
 // itself. The constant slots come last in processing order, so the rounds of 32 slots that hold
-// only constants skip the exponential (one round per mechanism mixes the two kinds).
+// only constants skip the exponential (one round per mechanism mixes the two kinds). This loop
+// evaluates most of the right-hand side's exponentials, and its FP64 exp is the one inlined copy
+// (the call and the registers it keeps live measured 3.5 % of the solve).
 template <class LY>
 __device__ __forceinline__ double plain_const(const SvT<LY>& t, const CellPrep& c, const int p, const int w0) {
   const double* sd = t.d(HD_SLOT) + kSlotRec * (p - SvT<LY>::NFO);
   const double a = sd[0];
   if (w0 & 8) return a;
-  return rexp(t, fma(sd[2], c.LT, fma(sd[1], c.invRT, a)));
+  const double e = fma(sd[2], c.LT, fma(sd[1], c.invRT, a));
+  if constexpr (LY::kMixed)
+    return rexp(t, e);
+  else
+    return exp(e);
 }
 
 // The cell preparation and the slot loops of the right-hand side, one out-of-line copy (the
