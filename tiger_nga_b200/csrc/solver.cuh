@@ -18,7 +18,13 @@
 //    for the trailing update);
 //  * a persistent grid steals cells from a queue; a cell that exhausts the pass's step budget
 //    saves its Nordsieck history and goes to the next pass's queue (recompaction), so a pass
-//    never runs longer than the budget allows and the host loop over passes is a CUDA graph.
+//    never runs longer than the budget allows and the host loop over passes is a CUDA graph;
+//  * at eight warps per SM (two per scheduler) the kernel is bound by instruction supply and
+//    latency, not by a pipe: the tables' records have odd strides (conflict-free lane-parallel
+//    reads), the exponential's precision is fixed per kernel (one form in its code), the walks
+//    are software-pipelined, transcendentals and the step control's divisions are out of line
+//    except the plain-slot exponential, and the step control skips work whose outcome its
+//    operands already decide. Each of these was kept on a measured, bit-identical A/B.
 // No wait in this kernel depends on another warp or block: work is claimed with atomics only.
 #pragma once
 #include <cuda_runtime.h>
